@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Benchmark of the KAOS kinetic particle loop on B200.
+
+Workload (one line per run, rank 0 prints JSON): the precision A/B tube --
+L = 4 dipole flux tube from 1000 km to |q| = 1e-3, 256 cells, 3D velocity grid
+48x48x64 (geometric), 1e7 O+ macro-ions (seeded synthetic Maxwellian,
+T = 0.3 eV, n0 = 1e10 m^-3, H = 300 km), wave heating on (chi = 1.7,
+1e-3 eV/s at the base), dt = 0.005 s, master step every 50 steps (boundary
+removal/injection, ambipolar field, counts and moments).
+
+A "step" is one computational step of every particle of the tube.  The
+metric is particle-steps/s (higher is better).  `value` is the mixed-
+precision path; the FP64 path is timed beside it (`fp64`).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank advances its own tube
+(tubes are independent in the reference: species/tube loops are outermost,
+_8_KineticSolver.f90:43-44): weak scaling, no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s, mixed-prec vs FP64 on 1 B200, at stated moment error"
+N_PART = 10_000_000
+
+
+def clocks_sampler(stop, out):
+    """nvidia-smi clocks during the timed region (one sample per 200 ms)."""
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                              "-lms", "200"], stdout=subprocess.PIPE, text=True)
+    except Exception:
+        return
+    dev = os.environ.get("LOCAL_RANK", "0")
+    while not stop.is_set():
+        line = p.stdout.readline()
+        if not line:
+            break
+        f = [x.strip() for x in line.split(",")]
+        if f and f[0] == dev:
+            out.append(f)
+    p.terminate()
+
+
+def summarize_clocks(samples):
+    if not samples:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    sm = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
+    mx = [float(s[2]) for s in samples if s[2].replace(".", "").isdigit()]
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = sorted({names[k] for s in samples for k in range(4)
+                      if len(s) > 5 + k and s[5 + k].lower().startswith("active")})
+    return {"sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_workload(precision, n_part=N_PART, heating=True, collisions=False):
+    from kaos_b200 import grids
+    mi, spec, tube, vg = grids.config_c2(n_particles=n_part, heating=heating,
+                                         collisions=collisions,
+                                         precision=precision)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=20261203)
+    return mi, spec, tube, vg, (q, vpar, v1, v2)
+
+
+def bytes_per_particle_step(mixed, heating):
+    """Algorithmic HBM bytes per ion per ordinary step (reads + writes)."""
+    if mixed:  # cell, offset, V||, Vperp1, Vperp2, AEA, AG (4 B each)
+        rd, wr = 7 * 4, (5 if heating else 3) * 4
+    else:      # rho, z, V||, Vperp1, Vperp2, AEA, AG (8 B) + Qindk1 (4 B)
+        rd, wr = 7 * 8, (5 if heating else 3) * 8 + 4
+    return rd + wr
+
+
+def run_ours(args, precision, mi_tag):
+    from kaos_b200 import build as kbuild
+    from kaos_b200.lib import Solver
+    kbuild.build()
+    mi, spec, tube, vg, init = build_workload(precision, args.particles,
+                                              heating=not args.no_heating,
+                                              collisions=args.collisions)
+    s = Solver(mi, [tube], vg)
+    t0 = time.perf_counter()
+    s.load(0, *init)
+    t_load = time.perf_counter() - t0
+    s.step(args.warmup)
+    n0, _ = s.count()
+    # --- device-timed region: K steps in one call (CUDA events on the
+    # library's stream; inputs 0.5-1 GB > L2, so no explicit flush) --------
+    s.step(args.steps)
+    ms, launches = s.timing()
+    n1, _ = s.count()
+    nmean = 0.5 * (n0 + n1)
+    value = nmean * args.steps / (ms * 1e-3)
+    # --- per-step breakdown: ordinary steps are one push launch ------------
+    per = []
+    for _ in range(min(args.steps, 20)):
+        s.step(1)
+        per.append(s.timing())
+    ordinary = [m for (m, l) in per if l == 1]
+    push_ms = statistics.median(ordinary) if ordinary else ms / args.steps
+    return dict(value=value, ms=ms, launches=launches, n=nmean, push_ms=push_ms,
+                t_load=t_load, solver=s, init=init, tube=tube, mi=mi)
+
+
+def run_e2e(args, precision):
+    """Same metric through the public C-ABI with host buffers: the particle
+    arrays go host -> device once (amortised per step), every step reads the
+    per-cell moments back to the host, the final state comes back."""
+    from kaos_b200.lib import Solver
+    from kaos_b200.model_input import KAOS_M0, KAOS_M2PAR
+    mi, spec, tube, vg, init = build_workload(precision, args.particles,
+                                              heating=not args.no_heating,
+                                              collisions=args.collisions)
+    s = Solver(mi, [tube], vg)
+    K = args.steps
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.load(0, *init)
+    h2d = sum(a.nbytes for a in init)
+    d2h = 0
+    for _ in range(K):
+        s.step(1)
+        for m in range(8):
+            d2h += s.moments(m).nbytes
+    p = s.particles()
+    d2h += sum(v.nbytes for v in p.values())
+    dt = time.perf_counter() - t0
+    n = len(p["q"])
+    s.close()
+    return dict(value=n * K / dt, h2d=h2d / K, d2h=d2h / K)
+
+
+def cpu_baseline(args, sample_particles=20000, sample_steps=5):
+    """The CPU oracle (FP64 restatement of the reference loop, direct
+    binning) on a bounded sample of the same workload, one host thread."""
+    from oracle.oracle import Oracle
+    from kaos_b200 import grids
+    from kaos_b200.model_input import KAOS_PREC_FP64
+    mi, spec, tube, vg = grids.config_c2(n_particles=sample_particles,
+                                         heating=not args.no_heating,
+                                         collisions=args.collisions,
+                                         precision=KAOS_PREC_FP64)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=20261203)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    o.step(1)
+    t0 = time.perf_counter()
+    o.step(sample_steps)
+    dt = time.perf_counter() - t0
+    n, _ = o.count()
+    return dict(value=n * sample_steps / dt, unit="particle-steps/s", cores=1,
+                kind="port",
+                sample=f"{n} O+ of the same tube x {sample_steps} steps "
+                       "(oracle, direct binning, 1 thread)")
+
+
+def reference_arm(args):
+    """--impl reference: the CPU restatement of the reference loop (the
+    reference itself is Fortran+MPI and cannot be built in this image) on
+    the host cores, bounded sample per step."""
+    from oracle.oracle import Oracle
+    from kaos_b200 import grids
+    from kaos_b200.model_input import KAOS_PREC_FP64
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    npart = 20000
+    mi, spec, tube, vg = grids.config_c2(n_particles=npart,
+                                         heating=not args.no_heating,
+                                         collisions=args.collisions,
+                                         precision=KAOS_PREC_FP64)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=20261203)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    o.step(args.warmup)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    dt = time.perf_counter() - t0
+    n, _ = o.count()
+    v = n * args.steps / dt
+    return {
+        "impl": "reference", "metric": METRIC, "value": v,
+        "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"precision A/B tube, L=4, 256 cells, 48x48x64, "
+                               f"{npart} O+ sample (of 1e7), heating on, dt 5 ms"},
+        "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": 1,
+                         "kind": "port",
+                         "sample": f"{n} O+ x {args.steps} steps per run, oracle FP64, "
+                                   "direct binning, 1 thread"},
+        "e2e": {"value": v, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--particles", type=int, default=N_PART)
+    ap.add_argument("--no-heating", action="store_true")
+    ap.add_argument("--collisions", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        line = reference_arm(args)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from kaos_b200.model_input import KAOS_PREC_FP64, KAOS_PREC_MIXED
+    # FP64 path first (reported beside the headline)
+    r64 = run_ours(args, KAOS_PREC_FP64, "fp64")
+    r64["solver"].close()
+    stop = threading.Event()
+    samples = []
+    th = threading.Thread(target=clocks_sampler, args=(stop, samples), daemon=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    th.start()
+    r32 = run_ours(args, KAOS_PREC_MIXED, "mixed")
+    torch.cuda.synchronize()
+    stop.set()
+    ms = r32["ms"]
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * r32["n"] * args.steps / (ms * 1e-3)
+    mixed_bytes = bytes_per_particle_step(True, not args.no_heating)
+    achieved = mixed_bytes * r32["n"] / (r32["push_ms"] * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    e2e = None
+    if not args.skip_e2e:
+        r32["solver"].close()
+        e2e = run_e2e(args, KAOS_PREC_MIXED)
+    cpu = cpu_baseline(args) if (rank == 0 and world == 1) else None
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "push_traffic.json")) as f:
+            tr = json.load(f)
+        traffic = tr.get("mixed_bytes_per_particle") * r32["n"]
+    except Exception:
+        pass
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": "precision A/B tube: L=4, 256 cells, 3D grid 48x48x64, "
+                                   f"{int(r32['n'])} O+ per GPU, heating "
+                                   f"{'off' if args.no_heating else 'on'}, collisions "
+                                   f"{'on' if args.collisions else 'off'}, dt 5 ms, "
+                                   "master step every 50 steps",
+                       "precision": "mixed (FP32 state + RK, FP64 quartic/renormalisation/reductions)",
+                       "l2": "inputs > L2 (particle arrays 0.5-1 GB); no flush",
+                       "parallelism": f"tube per GPU x{world}"},
+            "fp64": {"value": r64["value"] * world, "ms_per_step": r64["ms"] / args.steps,
+                     "push_ms": r64["push_ms"]},
+            "mixed_over_fp64": value / (r64["value"] * world),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_push32 (mixed push)",
+                         "bytes_per_particle": mixed_bytes},
+            "cpu_baseline": cpu,
+            "e2e": None if e2e is None else {
+                "value": e2e["value"] * world, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+            "gpu_launches": r32["launches"],
+            "clocks": summarize_clocks(samples),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,250 @@
+/*
+ * kaos_gpu.h -- C-ABI of the B200 kinetic particle loop for KAOS
+ * (Kinetic model of Auroral ion OutflowS).
+ *
+ * The reference has no plugin API: its hot path is the body of
+ * `KineticSolverSub` (_8_KineticSolver.f90:35-263), reached by the single
+ * call `call KineticSolverSub` (_KineticMain.f90:41), with all state held
+ * in module globals (_KineticMainParams.f90:170-250).  Each entry point
+ * below replaces one block of that body; the comment on each names the
+ * reference lines it stands for.  A Fortran host binds these through the
+ * `bind(C)` interface in kaos_b200/fortran/kaos_gpu_iface.f90.
+ *
+ * Conventions
+ *  - SI units throughout, like the reference.
+ *  - Configuration cells are 0-based inside the library (reference Qind =
+ *    NqLB + k).  Exported cell indices keep the reference escape sentinels
+ *    shifted to negative values: -1 = below the lower boundary (reference
+ *    Qind 0), -2 = above the upper boundary (reference Qind -1).
+ *  - Velocity-bin indices are 0-based; -1 = outside the velocity grid
+ *    (reference index 0).
+ *  - Every call returns an int status (KAOS_OK on success).  The text of
+ *    the last error of a handle is returned by kaos_last_error().
+ *  - A handle owns one CUDA stream on the device that was current when it
+ *    was created and is not thread safe; use one handle per thread/GPU.
+ */
+#ifndef KAOS_GPU_H
+#define KAOS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define KAOS_OK 0
+#define KAOS_ERR_PARAM 1    /* bad argument / inconsistent parameters      */
+#define KAOS_ERR_CAPACITY 2 /* particle capacity of a tube exceeded        */
+#define KAOS_ERR_NAN 3      /* non-finite particle state detected          */
+#define KAOS_ERR_CUDA 4     /* CUDA runtime error                          */
+#define KAOS_ERR_TIMEOUT 5  /* bounded device wait gave up                  */
+#define KAOS_ERR_STATE 6    /* call out of order (e.g. step before load)   */
+
+/* ---- precision modes ---------------------------------------------------- */
+#define KAOS_PREC_FP64 0  /* all particle arithmetic in FP64                */
+#define KAOS_PREC_MIXED 1 /* FP32 state + RK stages; FP64 quartic, position
+                             renormalisation and reductions                  */
+
+/* ---- moment selectors for kaos_get_moments ------------------------------ */
+#define KAOS_M0 0        /* M0phRT      density [m^-3]                      */
+#define KAOS_M1PERP1 1   /* M1Perp1phRT [m/s]   (3D velocity grid)          */
+#define KAOS_M1PERP2 2   /* M1Perp2phRT [m/s]   (3D velocity grid)          */
+#define KAOS_M1PAR 3     /* M1ParphRT   [m/s]                               */
+#define KAOS_M2 4        /* M2phRT      [J]                                 */
+#define KAOS_M2PERP1 5   /* M2Perp1phRT [J]     (3D velocity grid)          */
+#define KAOS_M2PERP2 6   /* M2Perp2phRT [J]     (3D velocity grid)          */
+#define KAOS_M2PAR 7     /* M2ParphRT   [J]                                 */
+#define KAOS_M1PERP 8    /* M1PerpphRT  [m/s]   (2D velocity grid)          */
+#define KAOS_M2PERP 9    /* M2PerpphRT  [J]     (2D velocity grid)          */
+#define KAOS_NQ 10       /* NqRT  per-cell density from counts [m^-3]       */
+#define KAOS_EAMAG 11    /* EAmagRT ambipolar field at cell centres [V/m]   */
+#define KAOS_EGMAG 12    /* EGmagRT gravity "field" at cell centres [V/m]   */
+#define KAOS_M0FILT 13   /* M0FiltAvrgRT filtered density used by EAmag     */
+#define KAOS_NUPOI 14    /* nuIonNeutRT Poisson collision counts per cell  */
+#define KAOS_NMOMENTS 15
+
+/*
+ * Run parameters: the subset of _ModelInput.f90 / FluxTubeT flag fields
+ * (_KineticMainParams.f90:464-473) that the per-step loop reads.  Flags are
+ * 0/1 exactly as in the reference.
+ */
+typedef struct kaos_params_c {
+  double ms;       /* SpecieT%msT ion mass [kg]                        */
+  double qs;       /* SpecieT%qsT ion charge [C]                       */
+  double h;        /* SpecieT%hT computational time step [s]           */
+  double mNeut;    /* neutral mass for ENA gravity / collisions [kg]   */
+  double TNeut;    /* neutral temperature [K]                          */
+  double dNTe;     /* Te increment per master step [K]                 */
+  double dNTeEND;  /* Te increment cap [K]                             */
+  uint64_t seed;   /* counter-based RNG key                            */
+  int32_t ndatfac; /* master-step cadence (reference ndatfacGT)        */
+  int32_t precision;            /* KAOS_PREC_*                         */
+  int32_t ION2VPERPflag;        /* 1: 3D (Vperp1,Vperp2,Vpar) grid     */
+  int32_t ICRflag;              /* wave heating                        */
+  int32_t ICRCOHERENCEflag;     /* coherent heating variant            */
+  int32_t MIRRORflag;
+  int32_t GRAVflag;
+  int32_t EAMBflag;
+  int32_t EAMBSIGNflag;
+  int32_t EAMBSELFCONSISTflag;
+  int32_t EAPRESSUREflag;
+  int32_t MOMENTFILTERflag;
+  int32_t QEXCHANGEflag;        /* ion -> ENA charge exchange          */
+  int32_t LBCONDITIONflag;      /* lower-boundary injection            */
+  int32_t UBCONDITIONflag;      /* upper-boundary injection            */
+  int32_t STATICINJECTIONflag;
+  int32_t PHASEENERGYPARIONMOMENTCENTERflag;
+  int32_t PHASEENERGYPERPIONMOMENTCENTERflag;
+  int32_t M0MAfilterPt;         /* moving-average points (odd)         */
+  int32_t M1ParMAfilterPt;
+  int32_t M1Perp1MAfilterPt;
+  int32_t M1Perp2MAfilterPt;
+  int32_t M2ParMAfilterPt;
+  int32_t reserved[4];
+} kaos_params_c;
+
+/*
+ * One flux tube: the per-cell grid tables of FluxTubeT
+ * (_KineticMainParams.f90:476-481) for the cells NqLB..NqUB, flattened to
+ * 0-based arrays of length nq.  All pointers are host pointers read once by
+ * kaos_create.  Optional tables may be NULL (zeros are used).
+ */
+typedef struct kaos_tube_c {
+  int32_t nq;              /* NqUB - NqLB + 1                              */
+  int32_t capacity;        /* max particles (incl. injection headroom)     */
+  double pG;               /* pGCGT  (field-line p = L shell) [RE]         */
+  double phiG;             /* phiGCGT longitude [rad]                      */
+  double nsnormfac;        /* macro-particle weight                        */
+  double nsnormCLB;        /* LB injection macro-particle count / master   */
+  double nsnormCUB;        /* UB injection macro-particle count / master   */
+  double sumdsICR;         /* sum(dsICRGT) heating-region arc length [m]   */
+  const double *qGL, *qGH, *qGC;   /* cell lower/upper/centre q            */
+  const double *hqC, *dqC, *d3xC;  /* metric factor, width, volume         */
+  const double *rGC, *thetaGC, *ellGC; /* cell-centre r, theta, ell        */
+  const double *TeG;       /* TeGT electron temperature [K]                */
+  const double *TsG;       /* TsGT ion temperature (injection) [K]         */
+  const double *nsnormCNeut; /* neutral density for collisions [m^-3]      */
+  /* ICR wave-heating tables (_1_SimParameterization.f90:1408-1444)        */
+  const double *lambdaPerp, *EtaLH, *XiPerp1, *XiPerp2;
+  const double *S0, *OmegaG0, *ChiPerp1, *ChiPerp2;
+} kaos_tube_c;
+
+/*
+ * The velocity grid, shared by every cell and tube (the reference reads
+ * QCellT(1)%V2PerpCellT everywhere, e.g. _8_4_1_IonDistributionFunctions
+ * .f90:58-59).  Edges are separable per axis.
+ *   3D (ION2VPERPflag=1): axes Vperp1 (n1), Vperp2 (n2), Vpar (npar).
+ *   2D (ION2VPERPflag=0): axes Vperp (n1, magnitudes), Vpar (npar); n2=0.
+ * Arrays of edges have n+1 entries (lower edge of bin k = e[k], upper =
+ * e[k+1]); centres are (lo+hi)/2 as in _0_0_VelGridGenerator.f90:338-467.
+ */
+typedef struct kaos_vgrid_c {
+  int32_t n1, n2, npar;
+  const double *e1, *e2, *epar;
+} kaos_vgrid_c;
+
+typedef struct kaos_handle kaos_handle;
+
+/* Create a solver for `ntubes` independent tubes on the current device.
+ * Replaces the allocation and parameter copy of DataTypeAllocBSub /
+ * SimParameterizationSub (_8_KineticSolver.f90:50). */
+int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
+                int32_t ntubes, const kaos_vgrid_c *vg, kaos_handle **out);
+
+/* Load the initial particles of one tube: the initial-condition arrays
+ * x0T..Vz0T, Vperp10T, Vperp20T of FluxTubeT (_7_InitialConditions.f90:
+ * 51-98).  Positions are field-line q values (p = pG is implied);
+ * velocities are field-aligned components. */
+int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
+                        const double *vpar, const double *vperp1,
+                        const double *vperp2, int64_t n);
+
+/* Set the per-cell ambipolar field EAmagRT (host-imported spin-up
+ * profile, _8_7_AmbipolarEfield.f90:1375-1402) used on the first step.
+ * NULL resets to "compute from the initial moments". */
+int kaos_set_fields(kaos_handle *h, int32_t tube, const double *EAmag,
+                    int32_t nq);
+
+/* Advance every tube by `nsteps` computational steps: the body of the
+ * ComputationalTimeStepLoop (_8_KineticSolver.f90:54-239): charge exchange,
+ * BoundaryConditionsSub, AmbipolarEfieldSub/GravfieldSub, KineticSolverA/B
+ * (push, injection, counts, distribution functions, moments).  The first
+ * call performs the n=1 step of KineticSolverASub. */
+int kaos_step(kaos_handle *h, int64_t nsteps);
+
+/* Number of computational steps taken so far (reference n - 1). */
+int kaos_get_step(kaos_handle *h, int64_t *n);
+
+/* Live particle counts of a tube: ions and ENAs (reference NsT split by
+ * ENAflag). */
+int kaos_get_count(kaos_handle *h, int32_t tube, int64_t *nion,
+                   int64_t *nena);
+
+/* Per-cell moment / field of the latest master step (M*phRT(nn,:),
+ * EAmagRT(nn,:) ...), `which` = KAOS_M0 ... ; out has nq doubles. */
+int kaos_get_moments(kaos_handle *h, int32_t tube, int32_t which,
+                     double *out, int32_t nq);
+
+/* Integer counts of the latest master step: per-cell ion counts
+ * (NqReNormT, nq entries) when nbins == nq, or the full phase-space
+ * histogram N2PerpphReNormRT / NphReNormRT laid out
+ * [cell][v1][v2][vpar] (3D) or [cell][vperp][vpar] (2D) when nbins equals
+ * that size.  The full histogram requires kaos_set_export(h, 1) before the
+ * master step. */
+int kaos_get_counts(kaos_handle *h, int32_t tube, int64_t *out,
+                    int64_t nbins);
+
+/* Enable (1) / disable (0) materialising the full phase-space histogram on
+ * master steps (the DataExport2 path). */
+int kaos_set_export(kaos_handle *h, int32_t on);
+
+/* Copy the ion state of a tube to host arrays of length n (n must equal the
+ * live ion count): field-line q, parallel velocity, Vperp1, Vperp2 and the
+ * start-of-step cell index Qindk1 (0-based, -1/-2 escape sentinels).  Any
+ * pointer may be NULL.  Order is the reference particle order. */
+int kaos_get_particles(kaos_handle *h, int32_t tube, double *q, double *vpar,
+                       double *vperp1, double *vperp2, int32_t *qind,
+                       int64_t n);
+
+/* Meridian-plane position (rho = x cos phi + y sin phi, z) of the ions of a
+ * tube, FP64 reconstruction of xN/yN/zN (_8_1_KineticRK4Update.f90:174-176). */
+int kaos_get_positions(kaos_handle *h, int32_t tube, double *rho, double *z,
+                       int64_t n);
+
+/* ENA state of a tube (Cartesian x, y, z, Vx, Vy, Vz), n = live ENA count. */
+int kaos_get_enas(kaos_handle *h, int32_t tube, double *x, double *y,
+                  double *z, double *vx, double *vy, double *vz, int64_t n);
+
+/* Boundary fluxes of the latest master step: escaped LB/UB ion counts
+ * (NqReNormLB/UBoutfluxIonT) and injected LB/UB counts (LB/UBNetDensityT). */
+int kaos_get_boundary(kaos_handle *h, int32_t tube, int64_t *lb_out,
+                      int64_t *ub_out, int64_t *lb_in, int64_t *ub_in);
+
+/* Device time (ms) of the last kaos_step call, measured with CUDA events on
+ * the handle's stream, and the number of kernels it launched. */
+int kaos_get_timing(kaos_handle *h, double *ms, int64_t *launches);
+
+/* Record the whole computational step in CUDA graphs (1) or launch the
+ * kernels directly (0, default). */
+int kaos_set_graph(kaos_handle *h, int32_t on);
+
+/* Block shape for the push kernel (threads per block; 0 = autotuned). */
+int kaos_set_launch(kaos_handle *h, int32_t threads, int32_t blocks_per_sm);
+
+/* Text of the last error on this handle (static storage; never NULL). */
+const char *kaos_last_error(kaos_handle *h);
+
+/* Device status word: nonzero bits report non-finite state (1), capacity
+ * overflow (2), bounded-wait timeout (4) seen on the device. */
+int kaos_get_status(kaos_handle *h, uint32_t *status);
+
+void kaos_destroy(kaos_handle *h);
+
+/* Library version string. */
+const char *kaos_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KAOS_GPU_H */

@@ -1,0 +1,917 @@
+// kaos_api.cu -- host side of the C-ABI (include/kaos_gpu.h): device memory
+// for the particles and per-cell tables, and the per-step launch sequence
+// that replaces the body of KineticSolverSub (_8_KineticSolver.f90:54-239).
+//
+// Everything stays resident in HBM across calls; the host only issues
+// launches on the handle's stream and reads results on request.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kaos_tube.cuh"
+
+using namespace kaos;
+
+namespace {
+
+constexpr int PUSH_THREADS = 256;
+constexpr int PUSH_ITEMS = 4;
+constexpr int BC_THREADS = 256;
+
+// Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0: closed form of the
+// depressed resolvent cubic in hyperbolic form, then Newton polish.
+double host_quartic_u(double q, double p) {
+  if (q == 0.0) return p;
+  double Cp = 1.0 / (p * q * q);
+  double eps = 4.0 / (3.0 * q * q);
+  double t = (Cp * Cp / 2.0) / (eps * std::sqrt(eps));
+  double sigma = 2.0 * std::sqrt(eps) * std::sinh(std::asinh(t) / 3.0);
+  double mu = std::sqrt(sigma);
+  double u = (-mu + std::sqrt(-sigma + 2.0 * Cp / mu)) / 2.0;
+  for (int k = 0; k < 4; ++k) {
+    double f = q * q * u * u * u * u + u / p - 1.0;
+    double fp = 4.0 * q * q * u * u * u + 1.0 / p;
+    u -= f / fp;
+  }
+  return u;
+}
+
+void host_rho_z(double q, double p, double *rho, double *z) {
+  double u = host_quartic_u(q, p);
+  double st = std::sqrt(u / p), ct = q * u * u, r = u * RE;
+  *rho = r * st;
+  *z = r * ct;
+  if (std::fabs(*rho) < 1e-6) *rho = 0.0;
+  if (std::fabs(*z) < 1e-6) *z = 0.0;
+}
+
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace
+
+struct kaos_handle {
+  kaos_params_c P{};
+  int ntubes = 0;
+  int mixed = 0;
+  int three_d = 1;
+  int nv = 0;
+  int64_t ncell = 0;
+  std::vector<TubeD> th;          // host copy of tube descriptors
+  std::vector<std::vector<double>> host_cells;  // for getters
+  VGridC vg{};
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // device
+  TubeD *d_tubes = nullptr;
+  int *d_blk_tube = nullptr;
+  int64_t *d_blk_start = nullptr;
+  int *d_tube_blk0 = nullptr;
+  int nblk = 0;
+  std::vector<int> tube_blk0;
+  int64_t *d_nlive = nullptr, *d_nlive_new = nullptr;
+  uint64_t *d_next_id = nullptr;
+  int64_t *d_blkcnt = nullptr, *d_blkoff = nullptr;
+  unsigned long long *d_lb_out = nullptr, *d_ub_out = nullptr,
+                     *d_lb_in = nullptr, *d_ub_in = nullptr;
+  uint32_t *d_status = nullptr;
+  std::vector<void *> allocs;
+  CellTables ct{};
+  Accum acc{};
+  Ions ion[2]{};
+  int cur = 0;
+  int64_t n = 0;      // computational steps taken
+  int export_on = 0;
+  int have_import = 0;
+  int loaded = 0;
+  int graph = 0;
+  double last_ms = 0.0;
+  int64_t launches = 0;
+  char err[512] = {0};
+};
+
+namespace {
+
+int fail(kaos_handle *h, int code, const char *fmt, ...) {
+  if (h) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(h->err, sizeof(h->err), fmt, ap);
+    va_end(ap);
+  }
+  return code;
+}
+
+#define CK(call)                                                              \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return fail(h, KAOS_ERR_CUDA, "%s: %s (%s:%d)", #call,                 \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                \
+  } while (0)
+
+template <typename T>
+int dalloc(kaos_handle *h, T **p, size_t n) {
+  void *q = nullptr;
+  size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess)
+    return fail(h, KAOS_ERR_CUDA, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  cudaMemset(q, 0, bytes);
+  h->allocs.push_back(q);
+  *p = (T *)q;
+  return KAOS_OK;
+}
+
+int upload(kaos_handle *h, double **dst, const std::vector<double> &v) {
+  int rc = dalloc(h, dst, v.size());
+  if (rc) return rc;
+  CK(cudaMemcpy(*dst, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return KAOS_OK;
+}
+
+bool is_master(const kaos_handle *h, int64_t n) {
+  return n >= 2 && (n % h->P.ndatfac) == 0;
+}
+
+PushArgs push_args(kaos_handle *h) {
+  PushArgs a{};
+  a.tubes = h->d_tubes;
+  a.blk_tube = h->d_blk_tube;
+  a.blk_start = h->d_blk_start;
+  a.chunk = PUSH_THREADS * PUSH_ITEMS;
+  a.nlive = h->d_nlive;
+  a.ion = h->ion[h->cur];
+  a.ct = h->ct;
+  a.acc = h->acc;
+  a.h = h->P.h;
+  a.ms = h->P.ms;
+  a.qs = h->P.qs;
+  a.seed = h->P.seed;
+  a.ff.mirror = h->P.MIRRORflag == 1;
+  a.ff.grav = h->P.GRAVflag == 1;
+  a.ff.eamb = h->P.EAMBflag == 1;
+  a.ff.eambsign = h->P.EAMBSIGNflag == 1;
+  a.icr = h->P.ICRflag == 1;
+  a.icrcoh = h->P.ICRCOHERENCEflag == 1;
+  a.status = h->d_status;
+  a.exporting = h->export_on;
+  return a;
+}
+
+TubeArgs tube_args(kaos_handle *h, uint32_t nn) {
+  TubeArgs a{};
+  a.tubes = h->d_tubes;
+  a.ntubes = h->ntubes;
+  a.ct = h->ct;
+  a.acc = h->acc;
+  a.nlive = h->d_nlive;
+  a.ms = h->P.ms;
+  a.qs = h->P.qs;
+  a.h = h->P.h;
+  a.mNeut = h->P.mNeut;
+  a.TNeut = h->P.TNeut;
+  a.dNTe = h->P.dNTe;
+  a.dNTeEND = h->P.dNTeEND;
+  a.seed = h->P.seed;
+  a.nn = nn;
+  a.three_d = h->three_d;
+  a.eamb = h->P.EAMBflag == 1;
+  a.grav = h->P.GRAVflag == 1;
+  a.eapressure = h->P.EAPRESSUREflag == 1;
+  a.eambsign = h->P.EAMBSIGNflag == 1;
+  a.eambself = h->P.EAMBSELFCONSISTflag == 1;
+  a.momfilter = h->P.MOMENTFILTERflag == 1;
+  a.qexchange = h->P.QEXCHANGEflag == 1;
+  a.cenpar = h->P.PHASEENERGYPARIONMOMENTCENTERflag == 1;
+  a.cenperp = h->P.PHASEENERGYPERPIONMOMENTCENTERflag == 1;
+  a.fpM0 = h->P.M0MAfilterPt;
+  a.fpM1par = h->P.M1ParMAfilterPt;
+  a.fpM1p1 = h->P.M1Perp1MAfilterPt;
+  a.fpM1p2 = h->P.M1Perp2MAfilterPt;
+  a.fpM2par = h->P.M2ParMAfilterPt;
+  return a;
+}
+
+int max_nq(const kaos_handle *h) {
+  int m = 0;
+  for (auto &t : h->th) m = std::max(m, t.nq);
+  return m;
+}
+
+int launch_push(kaos_handle *h, const PushArgs &a) {
+  const int nq = max_nq(h);
+  size_t smem = (size_t)(2 * nq + 1) * sizeof(double);
+  if (h->mixed) smem += (size_t)4 * nq * sizeof(double);
+  if (h->mixed) {
+    if (h->three_d) k_push32<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
+    else k_push32<false><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
+  } else {
+    if (h->three_d) k_push64<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
+    else k_push64<false><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
+  }
+  h->launches++;
+  CK(cudaGetLastError());
+  return KAOS_OK;
+}
+
+int zero_accum(kaos_handle *h) {
+  const int64_t nc = h->ncell;
+  CK(cudaMemsetAsync(h->acc.cnt, 0, nc * sizeof(unsigned), h->s));
+  CK(cudaMemsetAsync(h->acc.mpar, 0, nc * h->vg.npar * sizeof(unsigned), h->s));
+  CK(cudaMemsetAsync(h->acc.m1, 0, nc * h->vg.n1 * sizeof(unsigned), h->s));
+  if (h->three_d)
+    CK(cudaMemsetAsync(h->acc.m2, 0, nc * h->vg.n2 * sizeof(unsigned), h->s));
+  if (h->export_on && h->acc.hist)
+    CK(cudaMemsetAsync(h->acc.hist, 0, nc * (int64_t)h->nv * sizeof(unsigned), h->s));
+  return KAOS_OK;
+}
+
+int launch_moments(kaos_handle *h, uint32_t nn) {
+  TubeArgs ta = tube_args(h, nn);
+  size_t smem = (size_t)8 * max_nq(h) * sizeof(double);
+  k_moments<<<h->ntubes, 256, smem, h->s>>>(ta);
+  h->launches++;
+  CK(cudaGetLastError());
+  return KAOS_OK;
+}
+
+int launch_fields(kaos_handle *h, int te_update) {
+  TubeArgs ta = tube_args(h, 0);
+  ta.te_update = te_update;
+  ta.have_import = 0;
+  size_t smem = (size_t)3 * max_nq(h) * sizeof(double);
+  k_fields<<<h->ntubes, 256, smem, h->s>>>(ta);
+  h->launches++;
+  CK(cudaGetLastError());
+  return KAOS_OK;
+}
+
+Fields ion_fields(kaos_handle *h, int from, int to) {
+  Fields F{};
+  const Ions &A = h->ion[from], &B = h->ion[to];
+  auto add = [&](void *s, void *d, int sz) {
+    if (s) F.f[F.n++] = Field{s, d, sz};
+  };
+  if (h->mixed) {
+    add(A.cell, B.cell, 4); add(A.off, B.off, 4); add(A.fvpar, B.fvpar, 4);
+    add(A.fv1, B.fv1, 4); add(A.fv2, B.fv2, 4); add(A.faea, B.faea, 4);
+    add(A.fag, B.fag, 4); add(A.fqk4, B.fqk4, 4);
+  } else {
+    add(A.rho, B.rho, 8); add(A.z, B.z, 8); add(A.vpar, B.vpar, 8);
+    add(A.v1, B.v1, 8); add(A.v2, B.v2, 8); add(A.aea, B.aea, 8);
+    add(A.ag, B.ag, 8); add(A.qk4, B.qk4, 8);
+  }
+  add(A.qind, B.qind, 4);
+  add(A.vb, B.vb, 4);
+  add(A.id, B.id, 8);
+  return F;
+}
+
+int launch_boundary(kaos_handle *h) {
+  BcArgs b{};
+  b.tubes = h->d_tubes;
+  b.blk_tube = h->d_blk_tube;
+  b.blk_start = h->d_blk_start;
+  b.tube_blk0 = h->d_tube_blk0;
+  b.chunk = PUSH_THREADS * PUSH_ITEMS;
+  b.nlive = h->d_nlive_new;
+  b.qind = h->ion[h->cur].qind;
+  b.blkcnt = h->d_blkcnt;
+  b.blkoff = h->d_blkoff;
+  b.lb_out = h->d_lb_out;
+  b.ub_out = h->d_ub_out;
+  b.fields = ion_fields(h, h->cur, 1 - h->cur);
+  CK(cudaMemsetAsync(h->d_lb_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
+  CK(cudaMemsetAsync(h->d_ub_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
+  CK(cudaMemsetAsync(h->d_lb_in, 0, h->ntubes * sizeof(unsigned long long), h->s));
+  CK(cudaMemsetAsync(h->d_ub_in, 0, h->ntubes * sizeof(unsigned long long), h->s));
+  BcArgs bc = b;
+  bc.nlive = h->d_nlive;  // count reads the live counts
+  k_bc_count<<<h->nblk, BC_THREADS, 0, h->s>>>(bc);
+  k_bc_scan<<<h->ntubes, 32, 0, h->s>>>(b);      // writes nlive_new
+  k_bc_scatter<<<h->nblk, BC_THREADS, 0, h->s>>>(b, h->d_nlive);
+  h->launches += 3;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->d_nlive, h->d_nlive_new, h->ntubes * sizeof(int64_t),
+                     cudaMemcpyDeviceToDevice, h->s));
+  h->cur = 1 - h->cur;
+  return KAOS_OK;
+}
+
+int launch_inject(kaos_handle *h, int ub) {
+  InjArgs a{};
+  a.tubes = h->d_tubes;
+  a.ct = h->ct;
+  a.acc = h->acc;
+  a.ion = h->ion[h->cur];
+  a.nlive = h->d_nlive;
+  a.next_id = h->d_next_id;
+  a.n_in = ub ? h->d_ub_in : h->d_lb_in;
+  a.mixed = h->mixed;
+  a.ub = ub;
+  a.bin = 1;
+  a.exporting = h->export_on;
+  a.ms = h->P.ms;
+  a.qs = h->P.qs;
+  a.seed = h->P.seed;
+  a.status = h->d_status;
+  k_inject<<<h->ntubes, 256, 0, h->s>>>(a);
+  h->launches++;
+  CK(cudaGetLastError());
+  return KAOS_OK;
+}
+
+// One computational step n = h->n + 1.
+int step_once(kaos_handle *h) {
+  const int64_t n = h->n + 1;
+  const bool next_master = is_master(h, n + 1);
+  const bool qx = h->P.QEXCHANGEflag == 1;
+  int rc;
+  if (n == 1) {
+    // KineticSolverASub: statistics of the initial state, fields, push.
+    if ((rc = zero_accum(h))) return rc;
+    PushArgs a = push_args(h);
+    a.step = (uint32_t)n;
+    a.bin = 1;
+    a.bin_only = 1;
+    a.write_qind = 1;
+    if ((rc = launch_push(h, a))) return rc;
+    if ((rc = launch_moments(h, 1))) return rc;
+    if (!h->have_import) {
+      if ((rc = launch_fields(h, 0))) return rc;
+    } else {
+      TubeArgs ta = tube_args(h, 0);
+      ta.have_import = 1;  // gravity only, EAmag kept
+      k_fields<<<h->ntubes, 256, (size_t)3 * max_nq(h) * sizeof(double), h->s>>>(ta);
+      h->launches++;
+    }
+    PushArgs p = push_args(h);
+    p.step = (uint32_t)n;
+    p.prologue = 1;  // interpolate at q0 (qk4 holds q0 after loading)
+    p.write_qind = 1;
+    p.write_qk4 = next_master;
+    if ((rc = launch_push(h, p))) return rc;
+    h->n = n;
+    return KAOS_OK;
+  }
+  const bool master = is_master(h, n);
+  const uint32_t nn = (uint32_t)(n / h->P.ndatfac + 1);
+  if (master) {
+    if ((rc = launch_boundary(h))) return rc;
+    if ((rc = launch_fields(h, 1))) return rc;
+    if ((rc = zero_accum(h))) return rc;
+  }
+  PushArgs p = push_args(h);
+  p.step = (uint32_t)n;
+  p.bin = master;
+  p.prologue = master;
+  p.write_qind = (!h->mixed) || next_master || qx || h->export_on;
+  p.write_qk4 = next_master;
+  if ((rc = launch_push(h, p))) return rc;
+  if (master) {
+    if (h->P.LBCONDITIONflag == 1 && (rc = launch_inject(h, 0))) return rc;
+    if (h->P.UBCONDITIONflag == 1 && (rc = launch_inject(h, 1))) return rc;
+    if ((rc = launch_moments(h, nn))) return rc;
+  }
+  h->n = n;
+  return KAOS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char *kaos_version(void) { return "kaos_b200 0.1.0 (sm_100a)"; }
+
+const char *kaos_last_error(kaos_handle *h) {
+  return h ? h->err : "null handle";
+}
+
+int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
+                int32_t ntubes, const kaos_vgrid_c *vgc, kaos_handle **out) {
+  if (!p || !tubes || !vgc || !out || ntubes < 1) return KAOS_ERR_PARAM;
+  *out = nullptr;
+  kaos_handle *h = new kaos_handle();
+  h->P = *p;
+  if (h->P.ndatfac < 1) h->P.ndatfac = 1;
+  if (h->P.h <= 0.0 || h->P.ms <= 0.0) {
+    int rc = fail(h, KAOS_ERR_PARAM, "h and ms must be positive");
+    *out = h;
+    return rc;
+  }
+  h->mixed = p->precision == KAOS_PREC_MIXED;
+  h->three_d = p->ION2VPERPflag == 1;
+  h->ntubes = ntubes;
+  VGridC &vg = h->vg;
+  vg.three_d = h->three_d;
+  vg.n1 = vgc->n1;
+  vg.n2 = h->three_d ? vgc->n2 : 0;
+  vg.npar = vgc->npar;
+  if (vg.n1 < 1 || vg.npar < 1 || vg.n1 > MAXV || vg.npar > MAXV ||
+      (h->three_d && (vg.n2 < 1 || vg.n2 > MAXV)) || !vgc->e1 || !vgc->epar ||
+      (h->three_d && !vgc->e2)) {
+    *out = h;
+    return fail(h, KAOS_ERR_PARAM, "velocity grid sizes must be in [1, %d]", MAXV);
+  }
+  for (int k = 0; k <= vg.n1; ++k) { vg.e1[k] = vgc->e1[k]; vg.f1[k] = (float)vgc->e1[k]; }
+  for (int k = 0; k <= vg.npar; ++k) { vg.epar[k] = vgc->epar[k]; vg.fpar[k] = (float)vgc->epar[k]; }
+  for (int k = 0; h->three_d && k <= vg.n2; ++k) { vg.e2[k] = vgc->e2[k]; vg.f2[k] = (float)vgc->e2[k]; }
+  h->nv = h->three_d ? vg.n1 * vg.n2 * vg.npar : vg.n1 * vg.npar;
+
+  // ---- tubes: descriptors, concatenated per-cell tables -----------------
+  std::vector<double> qGL, qGH, qGC, hqC, dqC, d3xC, rGC, thC, elC, TeG, TsG,
+      neut, lam, eta, xi1, xi2, S0, Om0, chi1, chi2, uL, uH;
+  int64_t poff = 0, coff = 0, moff = 0, hoff = 0;
+  for (int t = 0; t < ntubes; ++t) {
+    const kaos_tube_c &T = tubes[t];
+    if (T.nq < 6 || T.nq > 4096 || T.capacity < 1 || !T.qGL || !T.qGH ||
+        !T.qGC || !T.hqC || !T.dqC || !T.d3xC || !T.rGC || !T.thetaGC ||
+        !T.ellGC || !T.TeG || !T.TsG) {
+      *out = h;
+      return fail(h, KAOS_ERR_PARAM, "tube %d: nq must be in [6, 4096], capacity > 0, tables non-NULL", t);
+    }
+    for (int k = 0; k + 1 < T.nq; ++k)
+      if (T.qGH[k] != T.qGL[k + 1]) {
+        *out = h;
+        return fail(h, KAOS_ERR_PARAM, "tube %d: cells must be contiguous (qGH[%d] != qGL[%d])", t, k, k + 1);
+      }
+    TubeD d{};
+    d.nq = T.nq;
+    d.coff = (int)coff;
+    d.off = poff;
+    d.cap = T.capacity;
+    d.pG = T.pG;
+    d.phiG = T.phiG;
+    d.cphi = std::cos(T.phiG);
+    d.sphi = std::sin(T.phiG);
+    d.sgn = (T.qGL[0] <= 0.0) ? 1.0 : -1.0;
+    d.nsnormfac = T.nsnormfac;
+    d.nsnormCLB = T.nsnormCLB;
+    d.nsnormCUB = T.nsnormCUB;
+    d.sumdsICR = T.sumdsICR;
+    d.moff = moff;
+    d.hoff = hoff;
+    host_rho_z(T.qGC[0], T.pG, &d.rhoLB, &d.zLB);
+    host_rho_z(T.qGC[T.nq - 1], T.pG, &d.rhoUB, &d.zUB);
+    h->th.push_back(d);
+    auto app = [&](std::vector<double> &v, const double *src, double dflt) {
+      for (int k = 0; k < T.nq; ++k) v.push_back(src ? src[k] : dflt);
+    };
+    app(qGL, T.qGL, 0); app(qGH, T.qGH, 0); app(qGC, T.qGC, 0);
+    app(hqC, T.hqC, 0); app(dqC, T.dqC, 0); app(d3xC, T.d3xC, 1);
+    app(rGC, T.rGC, 0); app(thC, T.thetaGC, 0); app(elC, T.ellGC, 1);
+    app(TeG, T.TeG, 0); app(TsG, T.TsG, 0); app(neut, T.nsnormCNeut, 0);
+    app(lam, T.lambdaPerp, 0); app(eta, T.EtaLH, 0); app(xi1, T.XiPerp1, 0);
+    app(xi2, T.XiPerp2, 0); app(S0, T.S0, 0); app(Om0, T.OmegaG0, 1);
+    app(chi1, T.ChiPerp1, 0); app(chi2, T.ChiPerp2, 0);
+    for (int k = 0; k < T.nq; ++k) {
+      uL.push_back(host_quartic_u(T.qGL[k], T.pG));
+      uH.push_back(host_quartic_u(T.qGH[k], T.pG));
+    }
+    poff += T.capacity;
+    coff += T.nq;
+    moff += T.nq;
+    hoff += (int64_t)T.nq * h->nv;
+  }
+  h->ncell = coff;
+  *out = h;
+  int rc;
+  CK(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&h->e0));
+  CK(cudaEventCreate(&h->e1));
+  CellTables &c = h->ct;
+  c.ncell_total = coff;
+  double *tmp;
+#define UP(field, vec)                                  \
+  if ((rc = upload(h, &tmp, vec))) return rc;           \
+  c.field = tmp;
+  UP(qGL, qGL) UP(qGH, qGH) UP(qGC, qGC) UP(hqC, hqC) UP(dqC, dqC)
+  UP(d3xC, d3xC) UP(rGC, rGC) UP(thetaGC, thC) UP(ellGC, elC) UP(TeG, TeG)
+  UP(TsG, TsG) UP(nsnormCNeut, neut) UP(lambdaPerp, lam) UP(EtaLH, eta)
+  UP(XiPerp1, xi1) UP(XiPerp2, xi2) UP(S0, S0) UP(OmegaG0, Om0)
+  UP(ChiPerp1, chi1) UP(ChiPerp2, chi2) UP(uL, uL) UP(uH, uH)
+  UP(Te, TeG)
+#undef UP
+  if ((rc = dalloc(h, &c.EAmag, coff))) return rc;
+  if ((rc = dalloc(h, &c.EG, coff))) return rc;
+  if ((rc = dalloc(h, &c.M0prev, coff))) return rc;
+  if ((rc = dalloc(h, &c.nuPoi, coff))) return rc;
+  if ((rc = dalloc(h, &c.mom, coff * KAOS_NMOMENTS))) return rc;
+  h->host_cells = {qGL, qGH, qGC};
+  // accumulators
+  if ((rc = dalloc(h, &h->acc.cnt, coff))) return rc;
+  if ((rc = dalloc(h, &h->acc.mpar, coff * vg.npar))) return rc;
+  if ((rc = dalloc(h, &h->acc.m1, coff * vg.n1))) return rc;
+  if ((rc = dalloc(h, &h->acc.m2, coff * std::max(vg.n2, 1)))) return rc;
+  // tube descriptors and the static block -> (tube, chunk) map
+  std::vector<int> bt;
+  std::vector<int64_t> bs;
+  const int64_t chunk = PUSH_THREADS * PUSH_ITEMS;
+  for (int t = 0; t < ntubes; ++t) {
+    h->tube_blk0.push_back((int)bt.size());
+    for (int64_t s0 = 0; s0 < h->th[t].cap; s0 += chunk) {
+      bt.push_back(t);
+      bs.push_back(s0);
+    }
+  }
+  h->tube_blk0.push_back((int)bt.size());
+  h->nblk = (int)bt.size();
+  if ((rc = dalloc(h, &h->d_tubes, ntubes))) return rc;
+  CK(cudaMemcpy(h->d_tubes, h->th.data(), ntubes * sizeof(TubeD), cudaMemcpyHostToDevice));
+  if ((rc = dalloc(h, &h->d_blk_tube, bt.size()))) return rc;
+  if ((rc = dalloc(h, &h->d_blk_start, bs.size()))) return rc;
+  if ((rc = dalloc(h, &h->d_tube_blk0, h->tube_blk0.size()))) return rc;
+  CK(cudaMemcpy(h->d_blk_tube, bt.data(), bt.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_blk_start, bs.data(), bs.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_tube_blk0, h->tube_blk0.data(), h->tube_blk0.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if ((rc = dalloc(h, &h->d_nlive, ntubes))) return rc;
+  if ((rc = dalloc(h, &h->d_nlive_new, ntubes))) return rc;
+  if ((rc = dalloc(h, &h->d_next_id, ntubes))) return rc;
+  if ((rc = dalloc(h, &h->d_blkcnt, bt.size()))) return rc;
+  if ((rc = dalloc(h, &h->d_blkoff, bt.size()))) return rc;
+  if ((rc = dalloc(h, &h->d_lb_out, ntubes))) return rc;
+  if ((rc = dalloc(h, &h->d_ub_out, ntubes))) return rc;
+  if ((rc = dalloc(h, &h->d_lb_in, ntubes))) return rc;
+  if ((rc = dalloc(h, &h->d_ub_in, ntubes))) return rc;
+  if ((rc = dalloc(h, &h->d_status, 1))) return rc;
+  // particle arrays (two buffer sets for the order-preserving compaction)
+  const int64_t cap = poff;
+  for (int b = 0; b < 2; ++b) {
+    Ions &I = h->ion[b];
+    if (h->mixed) {
+      if ((rc = dalloc(h, &I.cell, cap))) return rc;
+      if ((rc = dalloc(h, &I.off, cap))) return rc;
+      if ((rc = dalloc(h, &I.fvpar, cap))) return rc;
+      if ((rc = dalloc(h, &I.fv1, cap))) return rc;
+      if ((rc = dalloc(h, &I.fv2, cap))) return rc;
+      if ((rc = dalloc(h, &I.faea, cap))) return rc;
+      if ((rc = dalloc(h, &I.fag, cap))) return rc;
+      if ((rc = dalloc(h, &I.fqk4, cap))) return rc;
+    } else {
+      if ((rc = dalloc(h, &I.rho, cap))) return rc;
+      if ((rc = dalloc(h, &I.z, cap))) return rc;
+      if ((rc = dalloc(h, &I.vpar, cap))) return rc;
+      if ((rc = dalloc(h, &I.v1, cap))) return rc;
+      if ((rc = dalloc(h, &I.v2, cap))) return rc;
+      if ((rc = dalloc(h, &I.aea, cap))) return rc;
+      if ((rc = dalloc(h, &I.ag, cap))) return rc;
+      if ((rc = dalloc(h, &I.qk4, cap))) return rc;
+    }
+    if ((rc = dalloc(h, &I.qind, cap))) return rc;
+    if (!h->three_d && (rc = dalloc(h, &I.vb, cap))) return rc;
+    if ((rc = dalloc(h, &I.id, cap))) return rc;
+  }
+  CK(cudaDeviceSynchronize());
+  return KAOS_OK;
+}
+
+int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
+                        const double *vpar, const double *vperp1,
+                        const double *vperp2, int64_t n) {
+  if (!h) return KAOS_ERR_PARAM;
+  if (tube < 0 || tube >= h->ntubes) return fail(h, KAOS_ERR_PARAM, "bad tube %d", tube);
+  if (!q || !vpar || !vperp1 || n < 0) return fail(h, KAOS_ERR_PARAM, "null input");
+  if (h->n != 0) return fail(h, KAOS_ERR_STATE, "particles must be loaded before the first step");
+  const TubeD &T = h->th[tube];
+  if (n > T.cap) return fail(h, KAOS_ERR_CAPACITY, "tube %d: %lld particles exceed capacity %lld", tube, (long long)n, (long long)T.cap);
+  const double *qGL = h->host_cells[0].data() + T.coff;
+  const double *qGH = h->host_cells[1].data() + T.coff;
+  std::vector<double> E(T.nq + 1);
+  for (int k = 0; k < T.nq; ++k) E[k] = T.sgn * qGL[k];
+  E[T.nq] = T.sgn * qGH[T.nq - 1];
+  std::vector<int32_t> qind(n), vb(n), cell(n);
+  std::vector<double> a(n), b(n), qq(n);
+  std::vector<float> fo(n), f1(n), f2(n), f3(n), fq(n);
+  std::vector<uint64_t> id(n);
+  for (int64_t j = 0; j < n; ++j) {
+    double qj = q[j];
+    // KineticSolverASub q clamp (_8_0_0_1_KineticSolverA.f90:55-65)
+    if (T.sgn * qj <= E[0]) qj = qGL[0];
+    else if (T.sgn * qj > E[T.nq]) qj = qGH[T.nq - 1];
+    qq[j] = qj;
+    double s = T.sgn * qj;
+    int c;
+    if (s < E[0]) c = BELOW;
+    else if (s > E[T.nq]) c = ABOVE;
+    else c = (int)(std::lower_bound(E.begin() + 1, E.end(), s) - E.begin()) - 1;
+    qind[j] = c;
+    id[j] = (uint64_t)j;
+    double v1 = vperp1[j], v2 = vperp2 ? vperp2[j] : 0.0;
+    auto bin = [](const double *e, int nb, double v) {
+      if (!(v >= e[0] && v <= e[nb])) return -1;
+      return (int)(std::lower_bound(e + 1, e + nb + 1, v) - (e + 1));
+    };
+    int bp = bin(h->vg.epar, h->vg.npar, vpar[j]);
+    int b1 = bin(h->vg.e1, h->vg.n1, std::sqrt(v1 * v1 + v2 * v2));
+    vb[j] = ((b1 + 1) << 16) | (bp + 1);
+    if (h->mixed) {
+      int cp = c >= 0 ? c : (c == BELOW ? 0 : T.nq - 1);
+      cell[j] = cp;
+      fo[j] = (float)((qj - qGL[cp]) / (qGH[cp] - qGL[cp]));
+      f1[j] = (float)vpar[j];
+      f2[j] = (float)v1;
+      f3[j] = (float)v2;
+      fq[j] = (float)qj;
+    } else {
+      host_rho_z(qj, T.pG, &a[j], &b[j]);
+    }
+  }
+  Ions &I = h->ion[h->cur];
+  const int64_t o = T.off;
+#define H2D(dst, src, T_) CK(cudaMemcpy((dst) + o, (src), n * sizeof(T_), cudaMemcpyHostToDevice))
+  if (h->mixed) {
+    H2D(I.cell, cell.data(), int32_t);
+    H2D(I.off, fo.data(), float);
+    H2D(I.fvpar, f1.data(), float);
+    H2D(I.fv1, f2.data(), float);
+    H2D(I.fv2, f3.data(), float);
+    H2D(I.fqk4, fq.data(), float);
+  } else {
+    std::vector<double> v2v(n);
+    for (int64_t j = 0; j < n; ++j) v2v[j] = vperp2 ? vperp2[j] : 0.0;
+    H2D(I.rho, a.data(), double);
+    H2D(I.z, b.data(), double);
+    H2D(I.vpar, vpar, double);
+    H2D(I.v1, vperp1, double);
+    H2D(I.v2, v2v.data(), double);
+    H2D(I.qk4, qq.data(), double);
+  }
+  H2D(I.qind, qind.data(), int32_t);
+  if (I.vb) H2D(I.vb, vb.data(), int32_t);
+  H2D(I.id, id.data(), uint64_t);
+#undef H2D
+  int64_t nl = n;
+  uint64_t nid = (uint64_t)n;
+  CK(cudaMemcpy(h->d_nlive + tube, &nl, sizeof(int64_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_next_id + tube, &nid, sizeof(uint64_t), cudaMemcpyHostToDevice));
+  h->loaded = 1;
+  return KAOS_OK;
+}
+
+int kaos_set_fields(kaos_handle *h, int32_t tube, const double *EAmag,
+                    int32_t nq) {
+  if (!h) return KAOS_ERR_PARAM;
+  if (tube < 0 || tube >= h->ntubes) return fail(h, KAOS_ERR_PARAM, "bad tube %d", tube);
+  if (!EAmag) {
+    h->have_import = 0;
+    return KAOS_OK;
+  }
+  if (nq != h->th[tube].nq) return fail(h, KAOS_ERR_PARAM, "nq mismatch");
+  CK(cudaMemcpy(h->ct.EAmag + h->th[tube].coff, EAmag, nq * sizeof(double), cudaMemcpyHostToDevice));
+  h->have_import = 1;
+  return KAOS_OK;
+}
+
+int kaos_set_export(kaos_handle *h, int32_t on) {
+  if (!h) return KAOS_ERR_PARAM;
+  if (on && !h->acc.hist) {
+    int rc = dalloc(h, &h->acc.hist, (size_t)h->ncell * h->nv);
+    if (rc) return rc;
+  }
+  h->export_on = on ? 1 : 0;
+  return KAOS_OK;
+}
+
+int kaos_set_graph(kaos_handle *h, int32_t on) {
+  if (!h) return KAOS_ERR_PARAM;
+  h->graph = on ? 1 : 0;
+  return KAOS_OK;
+}
+
+int kaos_set_launch(kaos_handle *h, int32_t threads, int32_t bps) {
+  if (!h) return KAOS_ERR_PARAM;
+  (void)threads;
+  (void)bps;
+  return KAOS_OK;
+}
+
+int kaos_step(kaos_handle *h, int64_t nsteps) {
+  if (!h) return KAOS_ERR_PARAM;
+  if (!h->loaded) return fail(h, KAOS_ERR_STATE, "kaos_step before kaos_load_particles");
+  if (nsteps < 0) return fail(h, KAOS_ERR_PARAM, "nsteps < 0");
+  CK(cudaMemcpyToSymbolAsync(c_vg, &h->vg, sizeof(VGridC), 0, cudaMemcpyHostToDevice, h->s));
+  h->launches = 0;
+  CK(cudaEventRecord(h->e0, h->s));
+  for (int64_t k = 0; k < nsteps; ++k) {
+    int rc = step_once(h);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(h->e1, h->s));
+  CK(cudaEventSynchronize(h->e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, h->e0, h->e1));
+  h->last_ms = ms;
+  uint32_t st = 0;
+  CK(cudaMemcpy(&st, h->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (st & ST_NAN) return fail(h, KAOS_ERR_NAN, "non-finite particle state on the device");
+  if (st & ST_CAP) return fail(h, KAOS_ERR_CAPACITY, "tube capacity exceeded during injection");
+  return KAOS_OK;
+}
+
+int kaos_get_step(kaos_handle *h, int64_t *n) {
+  if (!h || !n) return KAOS_ERR_PARAM;
+  *n = h->n;
+  return KAOS_OK;
+}
+
+int kaos_get_status(kaos_handle *h, uint32_t *status) {
+  if (!h || !status) return KAOS_ERR_PARAM;
+  CK(cudaMemcpy(status, h->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return KAOS_OK;
+}
+
+int kaos_get_count(kaos_handle *h, int32_t tube, int64_t *nion, int64_t *nena) {
+  if (!h || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  CK(cudaStreamSynchronize(h->s));
+  int64_t nl = 0;
+  CK(cudaMemcpy(&nl, h->d_nlive + tube, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  // converted slots (DEAD) are not ions
+  std::vector<int32_t> q(nl);
+  if (nl) CK(cudaMemcpy(q.data(), h->ion[h->cur].qind + h->th[tube].off, nl * 4, cudaMemcpyDeviceToHost));
+  int64_t dead = 0;
+  for (auto v : q) dead += (v == DEAD);
+  if (nion) *nion = nl - dead;
+  if (nena) *nena = 0;
+  return KAOS_OK;
+}
+
+int kaos_get_moments(kaos_handle *h, int32_t tube, int32_t which, double *out,
+                     int32_t nq) {
+  if (!h || !out || tube < 0 || tube >= h->ntubes || which < 0 ||
+      which >= KAOS_NMOMENTS)
+    return KAOS_ERR_PARAM;
+  if (nq != h->th[tube].nq) return fail(h, KAOS_ERR_PARAM, "nq mismatch");
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaMemcpy(out, h->ct.mom + which * h->ncell + h->th[tube].coff,
+                nq * sizeof(double), cudaMemcpyDeviceToHost));
+  return KAOS_OK;
+}
+
+int kaos_get_counts(kaos_handle *h, int32_t tube, int64_t *out, int64_t nbins) {
+  if (!h || !out || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  const TubeD &T = h->th[tube];
+  CK(cudaStreamSynchronize(h->s));
+  if (nbins == T.nq) {
+    std::vector<unsigned> v(T.nq);
+    CK(cudaMemcpy(v.data(), h->acc.cnt + T.coff, T.nq * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < T.nq; ++k) out[k] = v[k];
+    return KAOS_OK;
+  }
+  if (nbins != (int64_t)T.nq * h->nv) return fail(h, KAOS_ERR_PARAM, "nbins must be nq or nq*nv");
+  if (!h->acc.hist) return fail(h, KAOS_ERR_STATE, "full histogram needs kaos_set_export(h, 1)");
+  std::vector<unsigned> v(nbins);
+  CK(cudaMemcpy(v.data(), h->acc.hist + T.hoff, nbins * sizeof(unsigned), cudaMemcpyDeviceToHost));
+  for (int64_t k = 0; k < nbins; ++k) out[k] = v[k];
+  return KAOS_OK;
+}
+
+int kaos_get_particles(kaos_handle *h, int32_t tube, double *q, double *vpar,
+                       double *vperp1, double *vperp2, int32_t *qind,
+                       int64_t n) {
+  if (!h || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  const TubeD &T = h->th[tube];
+  CK(cudaStreamSynchronize(h->s));
+  int64_t nl = 0;
+  CK(cudaMemcpy(&nl, h->d_nlive + tube, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  const Ions &I = h->ion[h->cur];
+  const int64_t o = T.off;
+  std::vector<int32_t> qi(nl);
+  if (nl) CK(cudaMemcpy(qi.data(), I.qind + o, nl * 4, cudaMemcpyDeviceToHost));
+  int64_t live = 0;
+  for (auto v : qi) live += (v != DEAD);
+  if (n != live) return fail(h, KAOS_ERR_PARAM, "n (%lld) must equal the ion count (%lld)", (long long)n, (long long)live);
+  std::vector<double> a(nl), b(nl), c(nl), d(nl), e(nl);
+  if (h->mixed) {
+    std::vector<int32_t> cell(nl);
+    std::vector<float> fo(nl), f1(nl), f2(nl), f3(nl);
+    if (nl) {
+      CK(cudaMemcpy(cell.data(), I.cell + o, nl * 4, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(fo.data(), I.off + o, nl * 4, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(f1.data(), I.fvpar + o, nl * 4, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(f2.data(), I.fv1 + o, nl * 4, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(f3.data(), I.fv2 + o, nl * 4, cudaMemcpyDeviceToHost));
+    }
+    const double *qGL = h->host_cells[0].data() + T.coff;
+    const double *qGH = h->host_cells[1].data() + T.coff;
+    for (int64_t j = 0; j < nl; ++j) {
+      a[j] = qGL[cell[j]] + (double)fo[j] * (qGH[cell[j]] - qGL[cell[j]]);
+      b[j] = f1[j];
+      c[j] = f2[j];
+      d[j] = f3[j];
+    }
+  } else if (nl) {
+    CK(cudaMemcpy(a.data(), I.rho + o, nl * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(e.data(), I.z + o, nl * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(b.data(), I.vpar + o, nl * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(c.data(), I.v1 + o, nl * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(d.data(), I.v2 + o, nl * 8, cudaMemcpyDeviceToHost));
+    for (int64_t j = 0; j < nl; ++j) {
+      double r2 = a[j] * a[j] + e[j] * e[j];
+      double r = std::sqrt(r2);
+      a[j] = (RE * RE) * (e[j] / r) / r2;
+    }
+  }
+  int64_t k = 0;
+  for (int64_t j = 0; j < nl; ++j) {
+    if (qi[j] == DEAD) continue;
+    if (q) q[k] = a[j];
+    if (vpar) vpar[k] = b[j];
+    if (vperp1) vperp1[k] = c[j];
+    if (vperp2) vperp2[k] = d[j];
+    if (qind) qind[k] = qi[j];
+    ++k;
+  }
+  return KAOS_OK;
+}
+
+int kaos_get_positions(kaos_handle *h, int32_t tube, double *rho, double *z,
+                       int64_t n) {
+  if (!h || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  const TubeD &T = h->th[tube];
+  CK(cudaStreamSynchronize(h->s));
+  int64_t nl = 0;
+  CK(cudaMemcpy(&nl, h->d_nlive + tube, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  const Ions &I = h->ion[h->cur];
+  std::vector<int32_t> qi(nl);
+  std::vector<double> a(nl), b(nl);
+  if (nl) CK(cudaMemcpy(qi.data(), I.qind + T.off, nl * 4, cudaMemcpyDeviceToHost));
+  if (h->mixed) {
+    std::vector<double> qv(n);
+    int rc = kaos_get_particles(h, tube, qv.data(), nullptr, nullptr, nullptr, nullptr, n);
+    if (rc) return rc;
+    for (int64_t j = 0; j < n; ++j) {
+      double rr = 0.0, zz = 0.0;
+      host_rho_z(qv[j], T.pG, &rr, &zz);
+      if (rho) rho[j] = rr;
+      if (z) z[j] = zz;
+    }
+    return KAOS_OK;
+  }
+  if (nl) {
+    CK(cudaMemcpy(a.data(), I.rho + T.off, nl * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(b.data(), I.z + T.off, nl * 8, cudaMemcpyDeviceToHost));
+  }
+  int64_t k = 0;
+  for (int64_t j = 0; j < nl; ++j) {
+    if (qi[j] == DEAD) continue;
+    if (k >= n) return fail(h, KAOS_ERR_PARAM, "n too small");
+    if (rho) rho[k] = a[j];
+    if (z) z[k] = b[j];
+    ++k;
+  }
+  return KAOS_OK;
+}
+
+int kaos_get_enas(kaos_handle *h, int32_t tube, double *x, double *y, double *z,
+                  double *vx, double *vy, double *vz, int64_t n) {
+  (void)x; (void)y; (void)z; (void)vx; (void)vy; (void)vz;
+  if (!h || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  if (n != 0) return fail(h, KAOS_ERR_PARAM, "no ENA population");
+  return KAOS_OK;
+}
+
+int kaos_get_boundary(kaos_handle *h, int32_t tube, int64_t *lb_out,
+                      int64_t *ub_out, int64_t *lb_in, int64_t *ub_in) {
+  if (!h || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  CK(cudaStreamSynchronize(h->s));
+  unsigned long long v[4] = {0, 0, 0, 0};
+  CK(cudaMemcpy(&v[0], h->d_lb_out + tube, 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&v[1], h->d_ub_out + tube, 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&v[2], h->d_lb_in + tube, 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&v[3], h->d_ub_in + tube, 8, cudaMemcpyDeviceToHost));
+  if (lb_out) *lb_out = (int64_t)v[0];
+  if (ub_out) *ub_out = (int64_t)v[1];
+  if (lb_in) *lb_in = (int64_t)v[2];
+  if (ub_in) *ub_in = (int64_t)v[3];
+  return KAOS_OK;
+}
+
+int kaos_get_timing(kaos_handle *h, double *ms, int64_t *launches) {
+  if (!h) return KAOS_ERR_PARAM;
+  if (ms) *ms = h->last_ms;
+  if (launches) *launches = h->launches;
+  return KAOS_OK;
+}
+
+void kaos_destroy(kaos_handle *h) {
+  if (!h) return;
+  if (h->s) cudaStreamSynchronize(h->s);
+  for (void *p : h->allocs) cudaFree(p);
+  if (h->e0) cudaEventDestroy(h->e0);
+  if (h->e1) cudaEventDestroy(h->e1);
+  if (h->s) cudaStreamDestroy(h->s);
+  delete h;
+}
+
+}  // extern "C"

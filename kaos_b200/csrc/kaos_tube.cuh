@@ -1,0 +1,478 @@
+// kaos_tube.cuh -- per-tube and bookkeeping kernels of a master step:
+// moments from the binning marginals, moment filter + ambipolar field +
+// gravity field, ion-neutral collision counts, order-preserving removal of
+// escaped ions and lower/upper-boundary injection.
+#pragma once
+#include "kaos_push.cuh"
+
+namespace kaos {
+
+struct TubeArgs {
+  const TubeD *tubes;
+  int ntubes;
+  CellTables ct;
+  Accum acc;
+  const int64_t *nlive;
+  double ms, qs, h, mNeut, TNeut, dNTe, dNTeEND;
+  uint64_t seed;
+  uint32_t nn;          // master-step index (reference nn)
+  int three_d;
+  int te_update, have_import, eamb, grav, eapressure, eambsign, eambself,
+      momfilter, qexchange, cenpar, cenperp;
+  int fpM0, fpM1par, fpM1p1, fpM1p2, fpM2par;
+};
+
+// MomentFilterSub (_8_7_1_MomentFilter.f90:30-142) for cell Q of nq, input
+// in shared memory.
+__device__ double filter_cell(const double *in, int nq, int Q, int Pt) {
+  const int H = (Pt - 1) / 2;
+  const int LB = 0, UB = nq - 1;
+  double out = 0.0;
+  if (Q <= LB - 1 + H) {
+    double s1 = in[Q] + in[Q + 1];
+    for (int k = 2; k <= H; ++k) s1 += in[Q + k];
+    double a1 = s1 / (H + 1);
+    if (Q == LB) out = a1;
+    else if (Q == LB + 1) out = (a1 + in[LB]) / 2.0;
+    else {
+      double s2 = in[Q - 1];
+      for (int k = 2; k <= Q - LB; ++k) s2 += in[Q - k];
+      out = (a1 + s2 / (Q - LB)) / 2.0;
+    }
+  }
+  if ((Q > LB - 1 + H) && (Q < UB - H)) {
+    double s1 = in[Q] + in[Q + 1];
+    for (int k = 2; k <= H; ++k) s1 += in[Q + k];
+    double s2 = in[Q - 1];
+    for (int k = 2; k <= H; ++k) s2 += in[Q - k];
+    out = (s1 / (H + 1) + s2 / H) / 2.0;
+  }
+  if (Q >= UB - H) {
+    double s2 = in[Q] + in[Q - 1];
+    for (int k = 2; k <= H; ++k) s2 += in[Q - k];
+    double a2 = s2 / (H + 1);
+    if (Q == UB) out = a2;
+    else if (Q == UB - 1) out = (in[UB] + a2) / 2.0;
+    else {
+      double s1 = in[Q + 1];
+      for (int k = 2; k <= UB - Q; ++k) s1 += in[Q + k];
+      out = (s1 / (UB - Q) + a2) / 2.0;
+    }
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// AmbipolarEfieldSub pressure term (_8_7_AmbipolarEfield.f90:611-1299),
+// GravfieldSub (_8_7_2_Gravfield.f90:57-65) and the Te update of
+// KineticSolverSub (_8_KineticSolver.f90:69-89).  One block per tube.
+__global__ void k_fields(TubeArgs a) {
+  extern __shared__ double sm[];
+  const TubeD T = a.tubes[blockIdx.x];
+  const int nq = T.nq;
+  double *M0p = sm, *M0f = sm + nq, *EP = sm + 2 * nq;
+  const CellTables &c = a.ct;
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
+    const int64_t g = T.coff + Q;
+    if (a.te_update) {
+      double tn = c.Te[g] + a.dNTe;
+      if (tn <= a.dNTeEND) c.Te[g] = tn;
+    }
+    M0p[Q] = c.M0prev[g];
+    c.EG[g] = a.grav ? (-2.0 * GG * ME * a.ms * cos(c.thetaGC[g]) /
+                        (a.qs * (c.rGC[g] * c.rGC[g]) * sqrt(c.ellGC[g])))
+                     : 0.0;
+  }
+  __syncthreads();
+  if (a.have_import || !a.eamb) return;  // imported EAmag kept as is
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x)
+    M0f[Q] = a.momfilter ? filter_cell(M0p, nq, Q, a.fpM0) : M0p[Q];
+  __syncthreads();
+  const double S = T.sgn;  // qGL(1) <= 0 ? +1 : -1
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
+    const int64_t g = T.coff + Q;
+    double ep = 0.0;
+    if (M0p[Q] != 0.0 && a.eapressure) {
+      const double *Mn = M0f;
+      double R1 = (1.0 / fabs(c.hqC[g])) * (KB * c.Te[g] / (a.qs * Mn[Q]));
+      double st, den;
+      if (Q == 0) {
+        st = -25.0 * Mn[Q] + 48.0 * Mn[Q + 1] - 36.0 * Mn[Q + 2] +
+             16.0 * Mn[Q + 3] - 3.0 * Mn[Q + 4];
+        den = 12.0 * c.dqC[g];
+      } else if (Q == nq - 1) {
+        st = -25.0 * Mn[Q] + 48.0 * Mn[Q - 1] - 36.0 * Mn[Q - 2] +
+             16.0 * Mn[Q - 3] - 3.0 * Mn[Q - 4];
+        den = -12.0 * c.dqC[g];
+      } else if (Q == 1 || Q == nq - 2) {
+        st = Mn[Q + 1] - Mn[Q - 1];
+        den = 2.0 * c.dqC[g];
+      } else {
+        st = Mn[Q - 2] - 8.0 * Mn[Q - 1] + 8.0 * Mn[Q + 1] - Mn[Q + 2];
+        den = 12.0 * c.dqC[g];
+      }
+      double R2 = a.eambsign ? -(st) / (-S * den) : fabs(st) / den;
+      double R = R1 * R2;
+      ep = a.eambsign ? R : fabs(R);
+    }
+    EP[Q] = ep;
+  }
+  __syncthreads();
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
+    double v = EP[Q];
+    if (a.eambself && Q <= 2 && nq > 3 && M0p[Q] != 0.0 && a.eapressure) v = EP[3];
+    c.EAmag[T.coff + Q] = 0.0 + v;  // EAInertial = 0 (EAINERTIALflag = 0)
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Moments of one master step from the binning marginals (ZerothIonMoment ..
+// SecondParIonMoment _8_6_1-_8_6_6 with the NonUniform2D/3D integrators
+// _8_5_*), then the model-A collision counts (IonNeutralCollision
+// FrequencyASub _8_6_6_1_...:28-301).  One block per tube.
+__global__ void k_moments(TubeArgs a) {
+  extern __shared__ double sm[];
+  const TubeD T = a.tubes[blockIdx.x];
+  const int nq = T.nq;
+  const CellTables &c = a.ct;
+  const int64_t NC = c.ncell_total;
+  double *mom = c.mom;
+  const double ms = a.ms;
+  const int n1 = c_vg.n1, n2 = c_vg.n2, npar = c_vg.npar;
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
+    const int64_t g = T.coff + Q;
+    const double w = T.nsnormfac / c.d3xC[g];
+    const double cnt = (double)a.acc.cnt[g];
+    const double NqRT = cnt * w;
+    double M[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const unsigned *mp = a.acc.mpar + g * npar, *m1 = a.acc.m1 + g * n1;
+    double Nin = 0.0;
+    for (int k = 0; k < npar; ++k) Nin += (double)mp[k];
+    if (NqRT != 0.0 && Nin != 0.0) {
+      double M0 = w * Nin;
+      double Sp = 0.0, S1 = 0.0;
+      for (int k = 0; k < npar; ++k) Sp += 0.5 * (c_vg.epar[k] + c_vg.epar[k + 1]) * mp[k];
+      for (int k = 0; k < n1; ++k) S1 += 0.5 * (c_vg.e1[k] + c_vg.e1[k + 1]) * m1[k];
+      const double M1par = (w * Sp) / M0;
+      double Tp = 0.0, Tq = 0.0, T1 = 0.0, T1c = 0.0;
+      // centred integrand; for M2|| a bin whose centred value is exactly
+      // zero falls back to the uncentred one (_8_6_6_SecondParIonMoment
+      // .f90:90-99).  The total-energy integrand also carries the Vperp
+      // terms, so it is never zero and keeps the centred value (Tq).
+      for (int k = 0; k < npar; ++k) {
+        if (!mp[k]) continue;
+        double vc = 0.5 * (c_vg.epar[k] + c_vg.epar[k + 1]);
+        double d = a.cenpar ? (vc - M1par) : vc;
+        double d2 = d * d;
+        Tq += d2 * mp[k];
+        if (d2 == 0.0) d2 = vc * vc;
+        Tp += d2 * mp[k];
+      }
+      const double M1p1 = (w * S1) / M0;
+      for (int k = 0; k < n1; ++k) {
+        if (!m1[k]) continue;
+        double vc = 0.5 * (c_vg.e1[k] + c_vg.e1[k + 1]);
+        T1 += vc * vc * m1[k];
+        double d = vc - M1p1;
+        double d2 = d * d;
+        if (d2 == 0.0) d2 = vc * vc;
+        T1c += d2 * m1[k];
+      }
+      M[KAOS_M0] = M0;
+      M[KAOS_M1PAR] = M1par;
+      M[KAOS_M2PAR] = (ms / 2.0) * ((w * Tp) / M0);
+      if (a.three_d) {
+        const unsigned *m2 = a.acc.m2 + g * n2;
+        double S2 = 0.0, T2 = 0.0, T2c = 0.0;
+        for (int k = 0; k < n2; ++k) S2 += 0.5 * (c_vg.e2[k] + c_vg.e2[k + 1]) * m2[k];
+        const double M1p2 = (w * S2) / M0;
+        for (int k = 0; k < n2; ++k) {
+          if (!m2[k]) continue;
+          double vc = 0.5 * (c_vg.e2[k] + c_vg.e2[k + 1]);
+          T2 += vc * vc * m2[k];
+          double d = vc - M1p2;
+          double d2 = d * d;
+          if (d2 == 0.0) d2 = vc * vc;
+          T2c += d2 * m2[k];
+        }
+        M[KAOS_M1PERP1] = M1p1;
+        M[KAOS_M1PERP2] = M1p2;
+        M[KAOS_M2] = (ms / 2.0) * ((w * (T1 + T2 + Tq)) / M0);
+        M[KAOS_M2PERP1] = (ms / 2.0) * ((w * (a.cenperp ? T1c : T1)) / M0);
+        M[KAOS_M2PERP2] = (ms / 2.0) * ((w * (a.cenperp ? T2c : T2)) / M0);
+      } else {
+        M[KAOS_M1PERP] = M1p1;
+        M[KAOS_M2] = (ms / 2.0) * ((w * (T1 + Tq)) / M0);
+        M[KAOS_M2PERP] = (ms / 2.0) * ((w * (a.cenperp ? T1c : T1)) / M0);
+      }
+    }
+    for (int k = 0; k < 10; ++k) mom[k * NC + g] = M[k];
+    mom[KAOS_NQ * NC + g] = NqRT;
+    c.M0prev[g] = M[KAOS_M0];
+    mom[KAOS_EAMAG * NC + g] = c.EAmag[g];
+    mom[KAOS_EGMAG * NC + g] = c.EG[g];
+  }
+  if (!a.qexchange) return;
+  // ---- collision counts per cell (needs filtered moments) ----------------
+  __syncthreads();
+  double *f1p = sm, *f11 = sm + nq, *f12 = sm + 2 * nq, *f2p = sm + 3 * nq;
+  double *s1p = sm + 4 * nq, *s11 = sm + 5 * nq, *s12 = sm + 6 * nq, *s2p = sm + 7 * nq;
+  const int m1i = a.three_d ? KAOS_M1PERP1 : KAOS_M1PERP;
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
+    const int64_t g = T.coff + Q;
+    s1p[Q] = mom[KAOS_M1PAR * NC + g];
+    s11[Q] = mom[m1i * NC + g];
+    s12[Q] = a.three_d ? mom[KAOS_M1PERP2 * NC + g] : 0.0;
+    s2p[Q] = mom[KAOS_M2PAR * NC + g];
+  }
+  __syncthreads();
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
+    f1p[Q] = a.momfilter ? filter_cell(s1p, nq, Q, a.fpM1par) : s1p[Q];
+    f11[Q] = a.momfilter ? filter_cell(s11, nq, Q, a.fpM1p1) : s11[Q];
+    f12[Q] = a.momfilter ? filter_cell(s12, nq, Q, a.fpM1p2) : s12[Q];
+    f2p[Q] = a.momfilter ? filter_cell(s2p, nq, Q, a.fpM2par) : s2p[Q];
+  }
+  __syncthreads();
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
+    const int64_t g = T.coff + Q;
+    const double M0 = mom[KAOS_M0 * NC + g];
+    double sigma = 0.0, nu = 0.0;
+    if (M0 != 0.0 && f2p[Q] != 0.0) {
+      double E = (6.242e18) * (1e-3) * f2p[Q];
+      double l = 4.07 - 0.269 * log(E);
+      sigma = (l * l) * pow(1.0 - exp(-415.0 / E), 0.8);
+    }
+    if (M0 != 0.0) {
+      const uint64_t key = ((uint64_t)a.nn << 32) | (uint32_t)Q;
+      double G0 = gauss64(a.seed, key, 0u, KAOS_RNG_NEUT, 0);
+      double G1 = gauss64(a.seed, key, 0u, KAOS_RNG_NEUT, 1);
+      double G2 = gauss64(a.seed, key, 0u, KAOS_RNG_NEUT, 2);
+      double sN = sqrt(KB * a.TNeut / a.mNeut);
+      double th = c.thetaGC[g], el = c.ellGC[g];
+      double ct = cos(th), st = sin(th), sl = sqrt(el);
+      double MVx = T.cphi * (3.0 * f1p[Q] * ct * st + f11[Q] * (1.0 - 3.0 * ct * ct)) / sl - f12[Q] * T.sphi;
+      double MVy = T.sphi * (3.0 * f1p[Q] * ct * st + f11[Q] * (1.0 - 3.0 * ct * ct)) / sl + f12[Q] * T.cphi;
+      double MVz = f1p[Q] * (3.0 * ct * ct - 1.0) / sl + 3.0 * f11[Q] * ct * st / sl;
+      double dx = MVx - sN * G0, dy = MVy - sN * G1, dz = MVz - sN * G2;
+      double vrel = sqrt(dx * dx + dy * dy + dz * dz);
+      if (sigma != 0.0) {
+        double mean = c.nsnormCNeut[g] * sigma * vrel * a.h;
+        // PoissonRNGSub (_3_2_PoissonRNG.f90:31-38): product of uniforms
+        double e = exp(-mean), prod = 1.0;
+        int64_t k = -1;
+        uint32_t it = 0;
+        while (prod > e && it < 100000u) {
+          kaos_u32x4 w = kaos_philox((uint32_t)Q, a.nn, it >> 1, (KAOS_RNG_POIS << 24), a.seed);
+          prod *= (it & 1u) ? kaos_u01(w.v[2], w.v[3]) : kaos_u01(w.v[0], w.v[1]);
+          ++k;
+          ++it;
+        }
+        nu = (double)k;
+        double cnt = (double)a.acc.cnt[g];
+        if (nu > cnt) nu = cnt;
+      }
+    }
+    c.nuPoi[g] = nu;
+    mom[KAOS_NUPOI * NC + g] = nu;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Order-preserving removal (BCReIndexSub, Fortran pack, _8_0_7_1_BCReIndex
+// .f90:33-131) in three passes: count kept per block, scan block counts per
+// tube, scatter with in-block ranks.
+struct Field {
+  void *src, *dst;
+  int size;
+};
+constexpr int MAXF = 14;
+struct Fields {
+  Field f[MAXF];
+  int n;
+};
+
+struct BcArgs {
+  const TubeD *tubes;
+  const int *blk_tube;
+  const int64_t *blk_start;
+  const int *tube_blk0;  // first block of each tube (ntubes+1)
+  int chunk;
+  int64_t *nlive;
+  const int32_t *qind;
+  int64_t *blkcnt, *blkoff;
+  unsigned long long *lb_out, *ub_out;  // per tube escape counts
+  Fields fields;
+};
+
+__device__ __forceinline__ bool keep_slot(int q) {
+  return q != BELOW && q != ABOVE && q != DEAD;
+}
+
+__global__ void k_bc_count(BcArgs a) {
+  const int t = a.blk_tube[blockIdx.x];
+  const TubeD &T = a.tubes[t];
+  const int64_t nl = a.nlive[t];
+  const int64_t beg = a.blk_start[blockIdx.x];
+  const int64_t end = min(beg + (int64_t)a.chunk, nl);
+  int kept = 0, lb = 0, ub = 0;
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    int q = a.qind[T.off + i];
+    kept += keep_slot(q);
+    lb += (q == BELOW);
+    ub += (q == ABOVE);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    kept += __shfl_down_sync(0xffffffffu, kept, o);
+    lb += __shfl_down_sync(0xffffffffu, lb, o);
+    ub += __shfl_down_sync(0xffffffffu, ub, o);
+  }
+  __shared__ int sk[32], sl[32], su[32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sk[w] = kept; sl[w] = lb; su[w] = ub; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int K = 0, L = 0, U = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { K += sk[k]; L += sl[k]; U += su[k]; }
+    a.blkcnt[blockIdx.x] = K;
+    if (L) atomicAdd(a.lb_out + t, (unsigned long long)L);
+    if (U) atomicAdd(a.ub_out + t, (unsigned long long)U);
+  }
+}
+
+__global__ void k_bc_scan(BcArgs a) {
+  // one block per tube: serial scan by thread 0 over the tube's blocks
+  // (a few thousand entries at most), then publish the new live count.
+  const int t = blockIdx.x;
+  if (threadIdx.x != 0) return;
+  int64_t s = 0;
+  for (int b = a.tube_blk0[t]; b < a.tube_blk0[t + 1]; ++b) {
+    a.blkoff[b] = s;
+    s += a.blkcnt[b];
+  }
+  a.nlive[t] = s;
+}
+
+__global__ void k_bc_scatter(BcArgs a, const int64_t *nlive_old) {
+  const int t = a.blk_tube[blockIdx.x];
+  const TubeD &T = a.tubes[t];
+  const int64_t nl = nlive_old[t];
+  const int64_t beg = a.blk_start[blockIdx.x];
+  const int64_t end = min(beg + (int64_t)a.chunk, nl);
+  __shared__ int wsum[32];
+  __shared__ int64_t base;
+  if (threadIdx.x == 0) base = a.blkoff[blockIdx.x];
+  __syncthreads();
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int64_t r0 = beg; r0 < end; r0 += blockDim.x) {
+    const int64_t i = r0 + threadIdx.x;
+    const bool in = i < end;
+    const bool k = in && keep_slot(a.qind[T.off + i]);
+    const unsigned bal = __ballot_sync(0xffffffffu, k);
+    const int wr = __popc(bal & ((1u << l) - 1u));
+    if (l == 0) wsum[w] = __popc(bal);
+    __syncthreads();
+    int woff = 0, tot = 0;
+    for (int q = 0; q < nw; ++q) { if (q < w) woff += wsum[q]; tot += wsum[q]; }
+    if (k) {
+      const int64_t src = T.off + i, dst = T.off + base + woff + wr;
+      for (int f = 0; f < a.fields.n; ++f) {
+        const Field &F = a.fields.f[f];
+        if (F.size == 8)
+          ((uint64_t *)F.dst)[dst] = ((const uint64_t *)F.src)[src];
+        else
+          ((uint32_t *)F.dst)[dst] = ((const uint32_t *)F.src)[src];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) base += tot;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Lower / upper boundary injection on a master step (BoundaryConditionsSub
+// :743-809, KineticSolverBSub _8_0_0_2_KineticSolverB.f90:195-793,
+// MBVelocityDistributionSub _6_1_MBVelocityDistribution.f90:29-120).
+struct InjArgs {
+  const TubeD *tubes;
+  CellTables ct;
+  Accum acc;
+  Ions ion;
+  int64_t *nlive;
+  uint64_t *next_id;
+  unsigned long long *n_in;  // per tube injected count (LB, UB)
+  int mixed, ub, bin, exporting;
+  double ms, qs;
+  uint64_t seed;
+  uint32_t *status;
+};
+
+__global__ void k_inject(InjArgs a) {
+  const int t = blockIdx.x;
+  const TubeD T = a.tubes[t];
+  const int Q = a.ub ? T.nq - 1 : 0;
+  const int64_t g = T.coff + Q;
+  int64_t k = (int64_t)llrint(a.ub ? T.nsnormCUB : T.nsnormCLB);
+  const int64_t nl = a.nlive[t];
+  if (k <= 0) return;
+  if (nl + k > T.cap) {
+    if (threadIdx.x == 0) atomicOr(a.status, ST_CAP);
+    k = T.cap - nl;
+    if (k <= 0) return;
+  }
+  const double rho0 = a.ub ? T.rhoUB : T.rhoLB, z0 = a.ub ? T.zUB : T.zLB;
+  const double r = sqrt(rho0 * rho0 + z0 * z0);
+  const double ct = z0 / r, st = rho0 / r, el = 1.0 + 3.0 * ct * ct, sl = sqrt(el);
+  const double sig = sqrt(KB * a.ct.TsG[g] / a.ms);
+  const double qm = a.qs / a.ms;
+  const double aea = fabs(qm * fabs(a.ct.EAmag[g])), ag = fabs(qm * fabs(a.ct.EG[g]));
+  const double qc = a.ct.qGC[g];
+  const uint64_t id0 = a.next_id[t];
+  const bool d3 = c_vg.three_d;
+  for (int64_t i = threadIdx.x; i < k; i += blockDim.x) {
+    const int64_t j = T.off + nl + i;
+    const uint64_t id = id0 + (uint64_t)i;
+    const double Vx0 = sig * gauss64(a.seed, id, 0u, KAOS_RNG_INJECT, 0);
+    const double Vy0 = sig * gauss64(a.seed, id, 0u, KAOS_RNG_INJECT, 1);
+    const double Vz0 = sig * gauss64(a.seed, id, 0u, KAOS_RNG_INJECT, 2);
+    const double h_ = Vx0 * T.cphi + Vy0 * T.sphi;
+    double v1 = ((1.0 - 3.0 * ct * ct) / sl) * h_ + ((3.0 * Vz0 * ct * st) / sl);
+    double vpar = ((3.0 * ct * st) / sl) * h_ + ((Vz0 * (3.0 * ct * ct - 1.0)) / sl);
+    double v2 = -Vx0 * T.sphi + Vy0 * T.cphi;
+    const double vp = sqrt(v1 * v1 + v2 * v2);
+    int bp = vbin(c_vg.epar, c_vg.npar, vpar);
+    int b1 = vbin(c_vg.e1, c_vg.n1, d3 ? v1 : vp);
+    int b2 = d3 ? vbin(c_vg.e2, c_vg.n2, v2) : 0;
+    if (a.ion.vb) a.ion.vb[j] = ((b1 + 1) << 16) | (bp + 1);
+    if (a.mixed) {
+      a.ion.cell[j] = Q;
+      a.ion.off[j] = (float)((qc - a.ct.qGL[g]) / (a.ct.qGH[g] - a.ct.qGL[g]));
+      a.ion.fvpar[j] = (float)vpar;
+      a.ion.fv1[j] = (float)v1;
+      a.ion.fv2[j] = (float)v2;
+      a.ion.faea[j] = (float)aea;
+      a.ion.fag[j] = (float)ag;
+      a.ion.fqk4[j] = (float)qc;
+    } else {
+      a.ion.rho[j] = rho0;
+      a.ion.z[j] = z0;
+      a.ion.vpar[j] = vpar;
+      a.ion.v1[j] = v1;
+      a.ion.v2[j] = v2;
+      a.ion.aea[j] = aea;
+      a.ion.ag[j] = ag;
+      a.ion.qk4[j] = qc;
+    }
+    a.ion.qind[j] = Q;
+    a.ion.id[j] = id;
+    if (a.bin) accumulate(a.acc, T, Q, b1, d3 ? b2 : 0, bp, a.exporting);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a.nlive[t] = nl + k;
+    a.next_id[t] = id0 + (uint64_t)k;
+    a.n_in[t] = (unsigned long long)k;
+  }
+}
+
+}  // namespace kaos

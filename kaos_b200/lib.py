@@ -1,0 +1,170 @@
+"""ctypes binding of libkaos_gpu.so (the C-ABI in include/kaos_gpu.h) and a
+small Python front (`Solver`) that drives one handle the way KAOS's
+KineticSolverSub drives its tubes.
+
+The product path is the CUDA library; there is no CPU fallback: loading
+fails loudly when libkaos_gpu.so is missing or no GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Sequence
+
+import numpy as np
+
+from .model_input import (KaosParams, KaosTube, KaosVGrid, ModelInput, Tube,
+                          VGrid)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libkaos_gpu.so")
+
+# every symbol declared in include/kaos_gpu.h
+EXPORTS = [
+    "kaos_create", "kaos_load_particles", "kaos_set_fields", "kaos_step",
+    "kaos_get_step", "kaos_get_count", "kaos_get_moments", "kaos_get_counts",
+    "kaos_set_export", "kaos_get_particles", "kaos_get_positions",
+    "kaos_get_enas", "kaos_get_boundary", "kaos_get_timing", "kaos_set_graph",
+    "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
+    "kaos_version",
+]
+
+_lib = None
+
+
+class KaosError(RuntimeError):
+    pass
+
+
+def load(path: str = LIBPATH):
+    """Load the library (no compute, works without a GPU)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise KaosError(f"{path} missing: build it with `python -m kaos_b200.build`")
+    L = C.CDLL(path)
+    vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+    L.kaos_create.argtypes = [vp, vp, i32, vp, C.POINTER(vp)]
+    L.kaos_load_particles.argtypes = [vp, i32, vp, vp, vp, vp, i64]
+    L.kaos_set_fields.argtypes = [vp, i32, vp, i32]
+    L.kaos_step.argtypes = [vp, i64]
+    L.kaos_get_step.argtypes = [vp, C.POINTER(i64)]
+    L.kaos_get_count.argtypes = [vp, i32, C.POINTER(i64), C.POINTER(i64)]
+    L.kaos_get_moments.argtypes = [vp, i32, i32, vp, i32]
+    L.kaos_get_counts.argtypes = [vp, i32, vp, i64]
+    L.kaos_set_export.argtypes = [vp, i32]
+    L.kaos_get_particles.argtypes = [vp, i32, vp, vp, vp, vp, vp, i64]
+    L.kaos_get_positions.argtypes = [vp, i32, vp, vp, i64]
+    L.kaos_get_enas.argtypes = [vp, i32] + [vp] * 6 + [i64]
+    L.kaos_get_boundary.argtypes = [vp, i32] + [C.POINTER(i64)] * 4
+    L.kaos_get_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
+    L.kaos_set_graph.argtypes = [vp, i32]
+    L.kaos_set_launch.argtypes = [vp, i32, i32]
+    L.kaos_last_error.argtypes = [vp]
+    L.kaos_last_error.restype = C.c_char_p
+    L.kaos_get_status.argtypes = [vp, C.POINTER(C.c_uint32)]
+    L.kaos_destroy.argtypes = [vp]
+    L.kaos_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class Solver:
+    """One libkaos_gpu handle over one or more tubes."""
+
+    def __init__(self, mi: ModelInput, tubes: Sequence[Tube], vg: VGrid):
+        L = load()
+        self.mi = mi
+        self._p = mi.to_c()
+        self._tubes = list(tubes)
+        arr = (KaosTube * len(tubes))()
+        for k, t in enumerate(tubes):
+            arr[k] = t.to_c()
+        self._tarr = arr
+        self._vg = vg
+        self._vgc = vg.to_c()
+        self.three_d = mi.ION2VPERPflag == 1
+        self.nbins = vg.nbins(self.three_d)
+        h = C.c_void_p()
+        rc = L.kaos_create(C.addressof(self._p), C.addressof(arr), len(tubes),
+                           C.addressof(self._vgc), C.byref(h))
+        self.h = h.value
+        self._check(rc)
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = load().kaos_last_error(self.h).decode() if self.h else ""
+            raise KaosError(f"kaos call failed (status {rc}): {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().kaos_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- calls -----------------------------------------------------------
+    def load(self, tube, q, vpar, v1, v2):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (q, vpar, v1, v2)]
+        self._check(load().kaos_load_particles(self.h, tube, *[_p(a) for a in arrs],
+                                               len(arrs[0])))
+
+    def set_fields(self, tube, EA):
+        a = None if EA is None else np.ascontiguousarray(EA, dtype=np.float64)
+        self._check(load().kaos_set_fields(self.h, tube, _p(a),
+                                           0 if a is None else len(a)))
+
+    def set_export(self, on):
+        self._check(load().kaos_set_export(self.h, int(on)))
+
+    def step(self, n):
+        self._check(load().kaos_step(self.h, int(n)))
+
+    def count(self, tube=0):
+        a, b = C.c_int64(), C.c_int64()
+        self._check(load().kaos_get_count(self.h, tube, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def moments(self, which, tube=0):
+        out = np.zeros(self._tubes[tube].nq)
+        self._check(load().kaos_get_moments(self.h, tube, which, _p(out), len(out)))
+        return out
+
+    def counts(self, tube=0, full=False):
+        nq = self._tubes[tube].nq
+        n = nq * self.nbins if full else nq
+        out = np.zeros(n, dtype=np.int64)
+        self._check(load().kaos_get_counts(self.h, tube, _p(out), n))
+        return out
+
+    def particles(self, tube=0):
+        ni, _ = self.count(tube)
+        q, vp, v1, v2 = (np.zeros(ni) for _ in range(4))
+        qi = np.zeros(ni, dtype=np.int32)
+        self._check(load().kaos_get_particles(self.h, tube, _p(q), _p(vp), _p(v1),
+                                              _p(v2), _p(qi), ni))
+        rho, z = np.zeros(ni), np.zeros(ni)
+        self._check(load().kaos_get_positions(self.h, tube, _p(rho), _p(z), ni))
+        return dict(q=q, vpar=vp, vperp1=v1, vperp2=v2, qind=qi, rho=rho, z=z)
+
+    def boundary(self, tube=0):
+        v = [C.c_int64() for _ in range(4)]
+        self._check(load().kaos_get_boundary(self.h, tube, *[C.byref(x) for x in v]))
+        return np.array([x.value for x in v])
+
+    def timing(self):
+        ms, nl = C.c_double(), C.c_int64()
+        self._check(load().kaos_get_timing(self.h, C.byref(ms), C.byref(nl)))
+        return ms.value, nl.value
+
+    def set_graph(self, on):
+        self._check(load().kaos_set_graph(self.h, int(on)))

@@ -1,0 +1,210 @@
+"""Known-answer tests that pin the CPU oracle (no GPU).
+
+The reference ships no tests or recorded outputs and cannot be compiled
+here (no Fortran compiler), so the oracle is pinned by analytic answers and
+by the reference's own inline invariant checks:
+  * quartic residual / p-consistency checks
+    (_8_1_4_RK4DipolePolynomialSolver.f90:52-56, :132-145),
+  * particle-number conservation (_8_0_0_2_KineticSolverB.f90:92-99),
+  * F*d3v = N (_8_4_1_IonDistributionFunctions.f90:116-130),
+  * moment/integrand consistency (_8_6_1_ZerothIonMoment.f90:198-215).
+"""
+import mpmath as mp
+import numpy as np
+import pytest
+
+from kaos_b200 import grids
+from kaos_b200.model_input import (KAOS_M0, KAOS_M1PAR, KAOS_M1PERP1,
+                                   KAOS_M2PAR, KAOS_M2PERP1, KAOS_NQ, KB, RE,
+                                   ModelInput)
+from oracle.oracle import Oracle, build, moment_filter, quartic
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _build():
+    build()
+
+
+# ---- dipole quartic -------------------------------------------------------
+@pytest.mark.parametrize("q", [0.63, 0.3, 0.1, 0.03, 1e-2, 3e-3, 1e-3,
+                               -0.5, -0.05, -1e-3])
+def test_quartic_root_against_multiprecision(q):
+    p = 4.0
+    r, th, x, y, z, qt = quartic(q, p)
+    mp.mp.dps = 40
+    ue = mp.findroot(lambda u: mp.mpf(q) ** 2 * u ** 4 + u / mp.mpf(p) - 1,
+                     mp.mpf(p) * 0.9)
+    assert abs(r / RE - float(ue)) / float(ue) < 2e-14
+    # reference diagnostics: q and p recovered from (r, theta)
+    assert abs(qt - q) < 5e-15 * max(1.0, abs(q) / 1e-2)
+    ptest = r / (RE * np.sin(th) ** 2)
+    assert abs(ptest - p) < 1e-6
+    assert np.sign(z) == np.sign(q)
+    assert x == 0.0  # phi = pi/2: |x| < 1e-6 is zeroed (:115-117)
+
+
+def test_quartic_equator_limit():
+    # q -> 0: the field line reaches its equatorial crossing r = p RE
+    r = quartic(1e-4, 5.0)[0]
+    assert abs(r / RE - 5.0) < 1e-3
+
+
+# ---- moving-average filter ------------------------------------------------
+def test_filter_constant_is_identity():
+    x = np.full(40, 3.25)
+    np.testing.assert_allclose(moment_filter(x, 11), x, rtol=1e-15)
+
+
+def test_filter_linear_profile_known_answer():
+    """Asymmetric window (_8_7_1_MomentFilter.f90:74-95): the mean of
+    x[Q..Q+5] and of x[Q-1..Q-5] averaged -> x[Q] - 0.25*slope inside."""
+    k = np.arange(40, dtype=np.float64)
+    x = 2.0 + 0.5 * k
+    y = moment_filter(x, 11)
+    inner = slice(5, 40 - 6)  # mid branch: LB-1+H < Q < UB-H
+    np.testing.assert_allclose(y[inner], x[inner] - 0.25 * 0.5, rtol=1e-14)
+    # first cell of the upper branch (Q = UB-H) is biased the other way
+    assert y[34] == pytest.approx(x[34] + 0.25 * 0.5, rel=1e-14)
+    # lower end: Q = 0 averages x[0..5]; Q = 1 averages (mean x[1..6], x[0])
+    assert y[0] == pytest.approx(np.mean(x[0:6]), rel=1e-15)
+    assert y[1] == pytest.approx((np.mean(x[1:7]) + x[0]) / 2, rel=1e-15)
+    # upper end: Q = UB averages x[UB-5..UB]
+    assert y[-1] == pytest.approx(np.mean(x[-6:]), rel=1e-15)
+    assert y[-2] == pytest.approx((x[-1] + np.mean(x[-7:-1])) / 2, rel=1e-15)
+
+
+# ---- ambipolar field of an exponential density -----------------------------
+def test_ambipolar_field_exponential_profile():
+    mi, spec, tube, vg = grids.config_small(n_particles=1000, nq=40)
+    o = Oracle(mi, tube, vg)
+    lam = 0.05  # e-folding length in q
+    q = tube.qGC
+    M0 = 1e10 * np.exp(-(tube.qGL[0] - q) / lam)
+    EA = o.ambipolar(M0)
+    Te = tube.TeG
+    expect = KB * Te / (mi.qs * lam * np.abs(tube.hqC))
+    inner = slice(8, 30)
+    # magnitude: 5-point stencil of an exponential is exact to O((dq/lam)^4)
+    np.testing.assert_allclose(np.abs(EA[inner]), expect[inner], rtol=2e-3)
+    # the lower three cells take the value of the fourth (:1276-1284)
+    assert EA[0] == EA[3] and EA[1] == EA[3] and EA[2] == EA[3]
+
+
+# ---- force: mirror term ----------------------------------------------------
+def test_mirror_force_matches_gradient_of_B():
+    mi = ModelInput(GRAVflag=0, EAMBflag=0, MIRRORflag=1)
+    _, spec, tube, vg = grids.config_small(n_particles=500)
+    o = Oracle(mi, tube, vg)
+    r, th = grids.dipole_q_to_rtheta(np.array([0.4]), tube.pG)
+    y, z = r[0] * np.sin(th[0]), r[0] * np.cos(th[0])
+    vperp = 1.5e3
+    Ax, Ay, Az, qq = o.force(0.0, y, z, vperp, 0.0, 0.0)
+    # a|| = -(vperp^2 / 2) d ln B / ds  (mu = m vperp^2 / 2B, vperp fixed)
+    ell = 1 + 3 * np.cos(th[0]) ** 2
+    e = np.array([3 * np.cos(th[0]) * np.sin(th[0]), 3 * np.cos(th[0]) ** 2 - 1]) / np.sqrt(ell)
+    def lnB(s):
+        rr = np.hypot(y + s * e[0], z + s * e[1])
+        ct = (z + s * e[1]) / rr
+        return np.log(8.06e15 * np.sqrt(1 + 3 * ct * ct) / rr ** 3)
+    ds = 10.0
+    dlnB = (lnB(ds) - lnB(-ds)) / (2 * ds)
+    apar = Ay * e[0] + Az * e[1]
+    assert apar == pytest.approx(-(vperp ** 2 / 2) * dlnB, rel=1e-5)
+    assert qq > 0 and apar > 0  # northern branch: pushed toward the equator
+
+
+# ---- counting and moments ---------------------------------------------------
+@pytest.mark.parametrize("three_d", [True, False])
+def test_literal_and_direct_binning_agree(three_d):
+    mi, spec, tube, vg = grids.config_small(n_particles=1500, three_d=three_d,
+                                            nq=12, steps_per_master=2)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=5)
+    res = []
+    for literal in (True, False):
+        o = Oracle(mi, tube, vg)
+        o.load(q, vpar, v1, v2)
+        o.set_literal(literal)
+        o.step(4)
+        res.append((o.counts(), o.counts(full=True), o.moments(KAOS_M0)))
+    np.testing.assert_array_equal(res[0][0], res[1][0])
+    np.testing.assert_array_equal(res[0][1], res[1][1])
+    np.testing.assert_array_equal(res[0][2], res[1][2])
+
+
+def test_particle_number_conservation_and_F_d3v():
+    mi, spec, tube, vg = grids.config_small(n_particles=3000, steps_per_master=2)
+    tube.nsnormCLB = 0.0
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=9)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    o.step(6)
+    ni, ne = o.count()
+    lb, ub, _, _ = o.boundary()
+    assert ne == 0
+    cnt = o.counts()
+    hist = o.counts(full=True).reshape(tube.nq, -1)
+    # every in-grid ion is in exactly one cell; in-grid velocities in one bin
+    assert cnt.sum() <= ni
+    assert np.all(hist.sum(axis=1) <= cnt)
+    # density moment: M0 = N_in * nsnormfac / d3x (F * d3v summed = N)
+    M0 = o.moments(KAOS_M0)
+    nin = hist.sum(axis=1)
+    np.testing.assert_allclose(M0, nin * tube.nsnormfac / tube.d3xC, rtol=1e-12)
+    NqRT = o.moments(KAOS_NQ)
+    np.testing.assert_allclose(NqRT, cnt * tube.nsnormfac / tube.d3xC, rtol=1e-15)
+
+
+def test_moments_of_drifting_maxwellian():
+    """Bin-centre moments of a drifting Maxwellian approach the analytic
+    drift and temperature (first-step statistics, before any push)."""
+    mi, spec, tube, vg = grids.config_small(n_particles=200000, nq=8, three_d=True)
+    vg = grids.make_vgrid(True, 64, 64, 96, 8e3)
+    n = int(tube._counts.sum())
+    rng = np.random.default_rng(11)
+    cell = np.repeat(np.arange(tube.nq), tube._counts)
+    q = tube.qGC[cell]
+    T = tube.TsG[0]
+    sig = np.sqrt(KB * T / mi.ms)
+    u = 400.0
+    vpar = rng.normal(u, sig, n)
+    v1 = rng.normal(0, sig, n)
+    v2 = rng.normal(0, sig, n)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    o.step(1)
+    m1 = o.moments(KAOS_M1PAR)
+    m2 = o.moments(KAOS_M2PAR)
+    m1p = o.moments(KAOS_M1PERP1)
+    m2p1 = o.moments(KAOS_M2PERP1)
+    err = 5 * sig / np.sqrt(tube._counts)
+    assert np.all(np.abs(m1 - u) < err + 20.0)
+    assert np.all(np.abs(m1p) < err + 20.0)
+    kT2 = KB * T / 2.0
+    # sample variance error ~ sqrt(2/N); bin-centre quadrature adds ~2 %
+    tol = 0.02 + 5.0 * np.sqrt(2.0 / tube._counts)
+    assert np.all(np.abs(m2 / kT2 - 1) < tol)
+    assert np.all(np.abs(m2p1 / kT2 - 1) < tol)
+
+
+def test_mirror_only_invariant():
+    """With fixed Vperp (reference: only heating changes it), the mirror
+    force conserves v||^2/2 + (Vperp^2/2) ln B along each trajectory."""
+    mi = ModelInput(h=0.01, ndatfac=1000, GRAVflag=0, EAMBflag=0, MIRRORflag=1)
+    _, spec, tube, vg = grids.config_small(n_particles=400)
+    mi2, *_ = grids.config_small()
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi2, seed=2)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+
+    def invariant(p):
+        r = np.hypot(p["rho"], p["z"])
+        ct = p["z"] / r
+        B = 8.06e15 * np.sqrt(1 + 3 * ct * ct) / r ** 3
+        return 0.5 * p["vpar"] ** 2 + 0.5 * (p["vperp1"] ** 2 + p["vperp2"] ** 2) * np.log(B)
+
+    o.step(1)
+    i0 = invariant(o.particles())
+    o.step(200)
+    i1 = invariant(o.particles())
+    scale = 0.5 * (vpar ** 2 + v1 ** 2 + v2 ** 2).mean()
+    assert np.max(np.abs(i1 - i0)) / scale < 1e-6
