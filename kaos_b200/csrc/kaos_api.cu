@@ -211,7 +211,7 @@ int max_nq(const kaos_handle *h) {
 int launch_push(kaos_handle *h, const PushArgs &a) {
   const int nq = max_nq(h);
   size_t smem = (size_t)(2 * nq + 1) * sizeof(double);
-  if (h->mixed) smem += (size_t)4 * nq * sizeof(double);
+  if (h->mixed) smem += (size_t)5 * nq * sizeof(double) + (size_t)6 * nq * sizeof(float);
   if (h->mixed) {
     if (h->three_d) k_push32<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
     else k_push32<false><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
@@ -431,7 +431,8 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
 
   // ---- tubes: descriptors, concatenated per-cell tables -----------------
   std::vector<double> qGL, qGH, qGC, hqC, dqC, d3xC, rGC, thC, elC, TeG, TsG,
-      neut, lam, eta, xi1, xi2, S0, Om0, chi1, chi2, uL, uH;
+      neut, lam, eta, xi1, xi2, S0, Om0, chi1, chi2, uL, uH, hK1, hK2, hc1,
+      hc2, hiom0;
   int64_t poff = 0, coff = 0, moff = 0, hoff = 0;
   for (int t = 0; t < ntubes; ++t) {
     const kaos_tube_c &T = tubes[t];
@@ -475,6 +476,16 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     app(lam, T.lambdaPerp, 0); app(eta, T.EtaLH, 0); app(xi1, T.XiPerp1, 0);
     app(xi2, T.XiPerp2, 0); app(S0, T.S0, 0); app(Om0, T.OmegaG0, 1);
     app(chi1, T.ChiPerp1, 0); app(chi2, T.ChiPerp2, 0);
+    // wave-heating constants: K_i = h sqrt(q^2 xi_i eta S0 / (2 m^2 pi))
+    for (int k = 0; k < T.nq; ++k) {
+      const double pre = (p->qs * p->qs / (2.0 * p->ms * p->ms)) *
+                         (T.S0 ? T.S0[k] : 0.0) * (T.EtaLH ? T.EtaLH[k] : 0.0);
+      hK1.push_back(p->h * std::sqrt(pre * (T.XiPerp1 ? T.XiPerp1[k] : 0.0) / PI));
+      hK2.push_back(p->h * std::sqrt(pre * (T.XiPerp2 ? T.XiPerp2[k] : 0.0) / PI));
+      hc1.push_back(0.5 * (T.ChiPerp1 ? T.ChiPerp1[k] : 0.0));
+      hc2.push_back(0.5 * (T.ChiPerp2 ? T.ChiPerp2[k] : 0.0));
+      hiom0.push_back(T.OmegaG0 && T.OmegaG0[k] != 0.0 ? 1.0 / T.OmegaG0[k] : 0.0);
+    }
     for (int k = 0; k < T.nq; ++k) {
       uL.push_back(host_quartic_u(T.qGL[k], T.pG));
       uH.push_back(host_quartic_u(T.qGH[k], T.pG));
@@ -501,6 +512,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   UP(TsG, TsG) UP(nsnormCNeut, neut) UP(lambdaPerp, lam) UP(EtaLH, eta)
   UP(XiPerp1, xi1) UP(XiPerp2, xi2) UP(S0, S0) UP(OmegaG0, Om0)
   UP(ChiPerp1, chi1) UP(ChiPerp2, chi2) UP(uL, uL) UP(uH, uH)
+  UP(hK1, hK1) UP(hK2, hK2) UP(hc1, hc1) UP(hc2, hc2) UP(hiom0, hiom0)
   UP(Te, TeG)
 #undef UP
   if ((rc = dalloc(h, &c.EAmag, coff))) return rc;

@@ -57,6 +57,7 @@ struct CellTables {
   const double *lambdaPerp, *EtaLH, *XiPerp1, *XiPerp2, *S0, *OmegaG0,
       *ChiPerp1, *ChiPerp2;
   const double *uL, *uH;  // quartic root u = r/RE at the cell edges
+  const double *hK1, *hK2, *hc1, *hc2, *hiom0;  // wave-heating constants
   double *Te, *EAmag, *EG, *M0prev, *nuPoi;
   double *mom;            // [KAOS_NMOMENTS][ncell_total]
   int64_t ncell_total;

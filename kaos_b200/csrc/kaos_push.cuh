@@ -112,8 +112,33 @@ __device__ __forceinline__ void field_prologue(const PushArgs &a,
   }
 }
 
-// Box-Muller Gaussian from one Philox draw (GaussianRNGSub
-// _3_1_GaussianRNG.f90:33); the FP32 variant transforms the same uniforms.
+// Two Box-Muller Gaussians (cos and sin branches) from one Philox draw
+// keyed by (seed, particle id, step): GaussianRNGSub's transform
+// (_3_1_GaussianRNG.f90:33) with both outputs used.
+__device__ __forceinline__ void gauss2_64(uint64_t seed, uint64_t id,
+                                          uint32_t step, uint32_t stream,
+                                          double &g1, double &g2) {
+  kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), step,
+                             stream << 24, seed);
+  double u1 = kaos_u01(w.v[0], w.v[1]);
+  double u2 = kaos_u01(w.v[2], w.v[3]);
+  double R = sqrt(-2.0 * log(u1)), sn, cs;
+  sincospi(2.0 * u2, &sn, &cs);
+  g1 = R * cs;
+  g2 = R * sn;
+}
+__device__ __forceinline__ void gauss2_32(uint64_t seed, uint64_t id,
+                                          uint32_t step, uint32_t stream,
+                                          float &g1, float &g2) {
+  kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), step,
+                             stream << 24, seed);
+  float u1 = kaos_u01f(w.v[0]), u2 = kaos_u01f(w.v[2]);
+  float R = sqrtf(-2.0f * __logf(u1)), sn, cs;
+  __sincosf(6.2831853071795865f * u2, &sn, &cs);
+  g1 = R * cs;
+  g2 = R * sn;
+}
+// Single Gaussian (injection): cos branch of one draw.
 __device__ __forceinline__ double gauss64(uint64_t seed, uint64_t id,
                                           uint32_t step, uint32_t stream,
                                           uint32_t sub) {
@@ -123,80 +148,104 @@ __device__ __forceinline__ double gauss64(uint64_t seed, uint64_t id,
   double u2 = kaos_u01(w.v[2], w.v[3]);
   return sqrt(-2.0 * log(u1)) * cos(2.0 * PI * u2);
 }
-__device__ __forceinline__ float gauss32(uint64_t seed, uint64_t id,
-                                         uint32_t step, uint32_t stream,
-                                         uint32_t sub) {
-  kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), step,
-                             (stream << 24) | sub, seed);
-  float u1 = (float)kaos_u01(w.v[0], w.v[1]);
-  float u2 = (float)kaos_u01(w.v[2], w.v[3]);
-  return sqrtf(-2.0f * __logf(u1)) * __cosf(6.2831853071795865f * u2);
-}
 
-// WaveHeatingSub stochastic / coherent kicks (_8_1_1_0_WaveHeating.f90:
-// 39-312) for an ion in valid cell gc with gyrofrequency Om at k1.
+// Per-cell wave-heating constants, precomputed on the host from the ICR
+// tables (_1_SimParameterization.f90:1408-1444):
+//   K_i = h sqrt(q^2 xi_i eta S0 / (2 m^2 pi)),  c_i = chi_i / 2,
+//   w0 = 1/OmegaG0, lam = lambdaPerp.
+template <typename T> struct HeatC {
+  T K1, K2, c1, c2, iom0, lam;
+};
+
+// WaveHeatingSub kicks (_8_1_1_0_WaveHeating.f90:72-312).  With
+// D_i = q^2/(2m^2) xi_i eta S0 (Omega/Omega0)^-chi_i Sigma^-3,
+// eps = |V|/(Omega sum ds), tau = 1/((Omega/2pi) sqrt eps) and the kick
+// (h/tau) sqrt(2 D_i tau) G_i, the algebra reduces to
+//   kick_i = K_i x^(-chi_i/2) Sigma^(-3/2) sqrt(Omega s) G_i,  s = sqrt(eps),
+// applied while h <= tau, i.e. h Omega s <= 2 pi (stochastic branch);
+// the coherent branch kicks |Vperp| by sqrt(k1^2+k2^2) G1 with a uniform
+// gyro-angle.  invOm = 1/Omega is passed in (no division needed).
 template <typename T>
-__device__ __forceinline__ void heat(const PushArgs &a, int64_t gc, uint64_t id,
-                                     double sumds, T Om, T vparabs, T &v1,
-                                     T &v2) {
-  const CellTables &c = a.ct;
+__device__ __forceinline__ void heat(const PushArgs &a, const HeatC<T> &c,
+                                     uint64_t id, T invsumds, T Om, T invOm,
+                                     T vparabs, T &v1, T &v2) {
   const bool f64 = sizeof(T) == 8;
-  T lam = (T)c.lambdaPerp[gc], eta = (T)c.EtaLH[gc], xi1 = (T)c.XiPerp1[gc],
-    xi2 = (T)c.XiPerp2[gc], Om0 = (T)c.OmegaG0[gc],
-    chi1 = (T)c.ChiPerp1[gc], chi2 = (T)c.ChiPerp2[gc];
-  const T h = (T)a.h, twopi = (T)(2.0 * PI);
-  T vpm = sqrt(v1 * v1 + v2 * v2);
-  T Sig = T(1);
-  if (lam != T(0) && ((twopi * vpm) / Om) >= lam) Sig = (twopi * vpm) / (lam * Om);
-  // q^2/(2 m^2) S0 in FP64: m^2 (~1e-51 kg^2) is below the FP32 range
-  T pre = (T)((a.qs * a.qs / (2.0 * a.ms * a.ms)) * c.S0[gc]);
-  T sig3 = (Sig == T(1)) ? T(1) : T(1) / (Sig * Sig * Sig);
-  T p1, p2;
+  const T x = Om * c.iom0;
+  T e1, e2;
   if (f64) {
-    p1 = (T)pow((double)(Om / Om0), -(double)chi1);
-    p2 = (T)pow((double)(Om / Om0), -(double)chi2);
+    double lx = log((double)x);
+    e1 = (T)exp(-(double)c.c1 * lx);
+    e2 = (c.c2 == c.c1) ? e1 : (T)exp(-(double)c.c2 * lx);
   } else {
-    float lr = __log2f((float)(Om / Om0));
-    p1 = (T)exp2f(-(float)chi1 * lr);
-    p2 = (T)exp2f(-(float)chi2 * lr);
+    float lx = __logf((float)x);
+    e1 = (T)__expf(-(float)c.c1 * lx);
+    e2 = (c.c2 == c.c1) ? e1 : (T)__expf(-(float)c.c2 * lx);
   }
-  T D1 = (pre * (xi1 * eta) * p1) * sig3;
-  T D2 = (pre * (xi2 * eta) * p2) * sig3;
-  // epsilon = |V_R| / (Omega * sum ds_ICR); tau = 1/((Omega/2pi) sqrt(eps))
-  T eps = vparabs / (Om * (T)sumds);
-  T tau = T(1) / ((Om / twopi) * sqrt(eps));
-  T G1 = f64 ? (T)gauss64(a.seed, id, a.step, KAOS_RNG_HEAT, 0)
-             : (T)gauss32(a.seed, id, a.step, KAOS_RNG_HEAT, 0);
+  const T s = sqrt(vparabs * invsumds * invOm);
+  const T w = sqrt(Om * s);
+  T k1 = c.K1 * e1 * w, k2 = c.K2 * e2 * w;
+  if (c.lam != T(0)) {
+    const T vpm = sqrt(v1 * v1 + v2 * v2);
+    const T Sig = T(2.0 * PI) * vpm * invOm / c.lam;
+    if (Sig >= T(1)) {
+      const T f = T(1) / (Sig * sqrt(Sig));
+      k1 *= f;
+      k2 *= f;
+    }
+  }
+  T G1, G2;
+  if (f64) {
+    double g1, g2;
+    gauss2_64(a.seed, id, a.step, KAOS_RNG_HEAT, g1, g2);
+    G1 = (T)g1;
+    G2 = (T)g2;
+  } else {
+    float g1, g2;
+    gauss2_32(a.seed, id, a.step, KAOS_RNG_HEAT, g1, g2);
+    G1 = (T)g1;
+    G2 = (T)g2;
+  }
   if (a.icrcoh) {
-    T dV = h * sqrt(T(2) * (D1 + D2) / tau) * G1;
-    T vpn = fabs(vpm + dV);
-    kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), a.step,
+    const T vpn = fabs(sqrt(v1 * v1 + v2 * v2) + sqrt(k1 * k1 + k2 * k2) * G1);
+    kaos_u32x4 r = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), a.step,
                                (KAOS_RNG_HEAT << 24) | 2u, a.seed);
-    T ga = (T)kaos_u01(w.v[0], w.v[1]) * twopi;
+    const T ga = (T)kaos_u01(r.v[0], r.v[1]) * T(2.0 * PI);
     v1 = vpn * cos(ga);
     v2 = vpn * sin(ga);
     return;
   }
-  T G2 = f64 ? (T)gauss64(a.seed, id, a.step, KAOS_RNG_HEAT, 1)
-             : (T)gauss32(a.seed, id, a.step, KAOS_RNG_HEAT, 1);
-  if (h <= tau) {  // (h/tau) sqrt(2 D tau) written as h sqrt(2 D / tau)
-    v1 = v1 + h * sqrt(T(2) * D1 / tau) * G1;
-    v2 = v2 + h * sqrt(T(2) * D2 / tau) * G2;
+  if (a.h * (double)(Om * s) <= 2.0 * PI) {
+    v1 = v1 + k1 * G1;
+    v2 = v2 + k2 * G2;
   }
 }
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0 by Newton from u0 (the
-// function is increasing and convex for u > 0, so the root is unique).
-__device__ __forceinline__ double quartic_newton(double q, double p, double u,
+// function is increasing and convex for u > 0: the root is unique).  The
+// derivative is inverted in FP32; each step still contracts the error by
+// ~1e-7 on top of the quadratic term.
+__device__ __forceinline__ double quartic_newton(double q, double ip, double u,
                                                  int iters) {
-  double q2 = q * q, ip = 1.0 / p;
+  const double q2 = q * q;
   for (int k = 0; k < iters; ++k) {
-    double u2 = u * u;
-    double f = fma(q2 * u2, u2, fma(u, ip, -1.0));
-    double fp = fma(4.0 * q2 * u2, u, ip);
-    u = u - f / fp;
+    const double u2 = u * u;
+    const double f = fma(q2 * u2, u2, fma(u, ip, -1.0));
+    const double fp = fma(4.0 * q2 * u2, u, ip);
+    u = fma(-f, (double)__frcp_rn((float)fp), u);
   }
   return u;
+}
+
+// Cell search starting from the cell of the previous step (particles move a
+// small fraction of a cell per step); falls back to the bisection.
+__device__ __forceinline__ int cell_search_from(const double *E, int nq,
+                                                double s, int g) {
+  if (g >= 0 && g < nq) {
+    if (s <= E[g + 1] && (g == 0 ? s >= E[0] : s > E[g])) return g;
+    if (g + 1 < nq && s > E[g + 1] && s <= E[g + 2]) return g + 1;
+    if (g > 0 && s <= E[g] && (g == 1 ? s >= E[0] : s > E[g - 1])) return g - 1;
+  }
+  return cell_search(E, nq, s);
 }
 
 // Load this block's tube and its oriented cell edges / centres into smem.
@@ -210,38 +259,51 @@ __device__ __forceinline__ void load_tube_smem(const PushArgs &a, int t,
     E[k] = (k < T.nq) ? T.sgn * qGL[k] : T.sgn * qGH[T.nq - 1];
     if (k < T.nq) Cc[k] = T.sgn * qGC[k];
   }
-  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ HeatC<T> heat_consts(const CellTables &c, int64_t g) {
+  HeatC<T> h;
+  h.K1 = (T)c.hK1[g];
+  h.K2 = (T)c.hK2[g];
+  h.c1 = (T)c.hc1[g];
+  h.c2 = (T)c.hc2[g];
+  h.iom0 = (T)c.hiom0[g];
+  h.lam = (T)c.lambdaPerp[g];
+  return h;
 }
 
 // ---------------------------------------------------------------------------
 // FP64 kernel: ions stored as meridian-plane (rho, z) in FP64.
 template <bool THREE_D>
-__global__ void __launch_bounds__(256) k_push64(PushArgs a) {
+__global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   extern __shared__ double sm[];
   const int t = a.blk_tube[blockIdx.x];
   TubeD T;
   const int nqmax = a.tubes[t].nq;
   double *E = sm, *Cc = sm + nqmax + 1;
   load_tube_smem(a, t, T, E, Cc);
+  __syncthreads();
   const int64_t nl = a.nlive[t];
   const int64_t beg = a.blk_start[blockIdx.x];
   const int64_t end = min(beg + (int64_t)a.chunk, nl);
-  const double h = a.h, hh = 0.5 * a.h, h6 = a.h / 6.0;
+  const double h = a.h, hh = 0.5 * a.h, h6 = a.h / 6.0, hsq2 = 0.5 * a.h * a.h;
   const double qs_ms = a.qs / a.ms;
+  const double c_invOm = a.ms / (a.qs * MDIP);
+  const double ipG = 1.0 / T.pG, invsumds = 1.0 / T.sumdsICR;
   Ions I = a.ion;
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t j = T.off + i;
     const int qprev = I.qind[j];
     if (qprev == DEAD) continue;
-    double rho = I.rho[j], z = I.z[j], vpar = I.vpar[j];
+    const double rho = I.rho[j], z = I.z[j], vpar = I.vpar[j];
     double v1 = I.v1[j], v2 = I.v2[j];
     double aea = I.aea[j], ag = I.ag[j];
     if (a.prologue) field_prologue(a, T, E, Cc, I.qk4[j], aea, ag);
     const double vp2 = v1 * v1 + v2 * v2;
     // ---- k1: KineticUpdateA -------------------------------------------
-    Geo<double> g1 = geo(rho, z);
-    const int qi = cell_search(E, T.nq, T.sgn * g1.q);
-    // velocity bins at k1 (stale-index rule of the 2D grid kept in vb)
+    const Geo<double> g1 = geo(rho, z);
+    const int qi = cell_search_from(E, T.nq, T.sgn * g1.q, qprev);
     int b1 = -1, b2 = -1, bp = -1;
     if (THREE_D) {
       if (a.bin) {
@@ -249,10 +311,10 @@ __global__ void __launch_bounds__(256) k_push64(PushArgs a) {
         b1 = vbin(c_vg.e1, c_vg.n1, v1);
         b2 = vbin(c_vg.e2, c_vg.n2, v2);
       }
-    } else {
+    } else {  // 2D grid: an out-of-grid speed keeps its previous bin
       const int old = I.vb[j];
-      int np_ = vbin(c_vg.epar, c_vg.npar, vpar);
-      int n1_ = vbin(c_vg.e1, c_vg.n1, sqrt(vp2));
+      const int np_ = vbin(c_vg.epar, c_vg.npar, vpar);
+      const int n1_ = vbin(c_vg.e1, c_vg.n1, sqrt(vp2));
       bp = np_ >= 0 ? np_ : (old & 0xffff) - 1;
       b1 = n1_ >= 0 ? n1_ : (old >> 16) - 1;
       const int nw = ((b1 + 1) << 16) | (bp + 1);
@@ -264,21 +326,23 @@ __global__ void __launch_bounds__(256) k_push64(PushArgs a) {
       continue;
     }
     const double a1 = apar(g1, vp2, aea, ag, a.ff);
-    // wave heating (uses Vperp before the kick for the mirror force)
+    // wave heating (the mirror force keeps the pre-kick Vperp)
     double v1n = v1, v2n = v2;
     if (a.icr && qi >= 0) {
-      const double B = MDIP * (g1.ell * g1.isl) * (g1.ir * g1.ir * g1.ir);
-      heat<double>(a, (int64_t)T.coff + qi, I.id[j], T.sumdsICR, qs_ms * B,
-                   fabs(vpar), v1n, v2n);
+      const double sl = g1.ell * g1.isl;
+      const double Om = qs_ms * MDIP * sl * (g1.ir * g1.ir * g1.ir);
+      const double r = 1.0 / g1.ir;
+      const double invOm = c_invOm * (r * r * r) * g1.isl;
+      const HeatC<double> hc = heat_consts<double>(a.ct, (int64_t)T.coff + qi);
+      heat<double>(a, hc, I.id[j], invsumds, Om, invOm, fabs(vpar), v1n, v2n);
     }
     // ---- k2: half step along V_R (KineticUpdateB) -----------------------
     const double VRr = vpar * g1.er, VRz = vpar * g1.ez;
-    Geo<double> g2 = geo(rho + hh * VRr, z + hh * VRz);
+    const Geo<double> g2 = geo(fma(hh, VRr, rho), fma(hh, VRz, z));
     const double a2 = apar(g2, vp2, aea, ag, a.ff);
     // ---- k4: x + h V_R + h^2/2 A1 (KineticUpdateC) ----------------------
     const double A1r = a1 * g1.er, A1z = a1 * g1.ez;
-    Geo<double> g4 = geo(rho + h * VRr + (0.5 * h * h) * A1r,
-                         z + h * VRz + (0.5 * h * h) * A1z);
+    const Geo<double> g4 = geo(rho + h * VRr + hsq2 * A1r, z + h * VRz + hsq2 * A1z);
     const double a4 = apar(g4, vp2, aea, ag, a.ff);
     if (a.write_qk4) I.qk4[j] = g4.q;
     const double A2r = a2 * g2.er, A2z = a2 * g2.ez;
@@ -294,11 +358,12 @@ __global__ void __launch_bounds__(256) k_push64(PushArgs a) {
     const double r2 = xr * xr + xz * xz;
     const double ir = rsqrt(r2);
     const double qN = (RE * RE) * (xz * ir) * (ir * ir);
-    const double u = quartic_newton(qN, T.pG, r2 * ir * (1.0 / RE), 3);
-    const double st = sqrt(u / T.pG);
+    const double u = quartic_newton(qN, ipG, r2 * ir * (1.0 / RE), 2);
+    const double s2 = u * ipG;                 // sin^2(theta)
+    const double st = s2 * rsqrt(s2);
     const double ctn = qN * u * u;
-    const double r = u * RE;
-    double rhoN = r * st, zN = r * ctn;
+    const double rr = u * RE;
+    double rhoN = rr * st, zN = rr * ctn;
     if (fabs(rhoN) < 1e-6) rhoN = 0.0;
     if (fabs(zN) < 1e-6) zN = 0.0;
     // ---- V|| along the new field direction ------------------------------
@@ -322,40 +387,54 @@ __global__ void __launch_bounds__(256) k_push64(PushArgs a) {
 
 // ---------------------------------------------------------------------------
 // Mixed kernel: position = (cell, FP32 offset in q); FP32 velocities and RK
-// stages; FP64 for the q reconstruction, the quartic root (Newton, table
-// guess) and the renormalised q of the new position.
+// stages; FP64 for the q reconstruction, the quartic root (Newton from a
+// per-cell linear guess) and the renormalised q of the new position.
 template <bool THREE_D>
-__global__ void __launch_bounds__(256) k_push32(PushArgs a) {
+__global__ void __launch_bounds__(256, 3) k_push32(PushArgs a) {
   extern __shared__ double sm[];
   const int t = a.blk_tube[blockIdx.x];
   TubeD T;
   const int nqmax = a.tubes[t].nq;
   double *E = sm, *Cc = sm + nqmax + 1;
-  double *UL = Cc + nqmax, *UD = UL + nqmax, *QL = UD + nqmax, *DQ = QL + nqmax;
+  double *UL = Cc + nqmax, *UD = UL + nqmax, *QL = UD + nqmax, *IDQ = QL + nqmax,
+         *DQ = IDQ + nqmax;
+  float *HK = (float *)(DQ + nqmax);  // 6 floats per cell: K1 K2 c1 c2 iom0 lam
   load_tube_smem(a, t, T, E, Cc);
   for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
-    const double ql = a.ct.qGL[T.coff + k], qh = a.ct.qGH[T.coff + k];
+    const int64_t g = T.coff + k;
+    const double ql = a.ct.qGL[g], qh = a.ct.qGH[g];
     QL[k] = ql;
     DQ[k] = qh - ql;
-    UL[k] = a.ct.uL[T.coff + k];
-    UD[k] = a.ct.uH[T.coff + k] - a.ct.uL[T.coff + k];
+    IDQ[k] = 1.0 / (qh - ql);
+    UL[k] = a.ct.uL[g];
+    UD[k] = a.ct.uH[g] - a.ct.uL[g];
+    if (a.icr) {
+      HK[6 * k + 0] = (float)a.ct.hK1[g];
+      HK[6 * k + 1] = (float)a.ct.hK2[g];
+      HK[6 * k + 2] = (float)a.ct.hc1[g];
+      HK[6 * k + 3] = (float)a.ct.hc2[g];
+      HK[6 * k + 4] = (float)a.ct.hiom0[g];
+      HK[6 * k + 5] = (float)a.ct.lambdaPerp[g];
+    }
   }
   __syncthreads();
   const int64_t nl = a.nlive[t];
   const int64_t beg = a.blk_start[blockIdx.x];
   const int64_t end = min(beg + (int64_t)a.chunk, nl);
-  const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f;
-  const float hsq2 = 0.5f * h * h;
-  const double qs_ms = a.qs / a.ms;
-  const double pG = T.pG, ipG = 1.0 / T.pG;
+  const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
+  const float qs_ms = (float)(a.qs / a.ms);
+  const float c_invOm = (float)(a.ms / (a.qs * MDIP));
+  const float invsumds = (float)(1.0 / T.sumdsICR);
+  const double ipG = 1.0 / T.pG;
+  const float fRE = (float)RE;
   Ions I = a.ion;
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t j = T.off + i;
-    const int qprev = I.qind[j];
-    if (qprev == DEAD) continue;
     const int c0 = I.cell[j];
+    if (c0 == DEAD) continue;
     const float o0 = I.off[j];
-    float vpar = I.fvpar[j], v1 = I.fv1[j], v2 = I.fv2[j];
+    const float vpar = I.fvpar[j];
+    float v1 = I.fv1[j], v2 = I.fv2[j];
     float aea = I.faea[j], ag = I.fag[j];
     if (a.prologue) {
       double da = aea, dg = ag;
@@ -364,21 +443,19 @@ __global__ void __launch_bounds__(256) k_push32(PushArgs a) {
       ag = (float)dg;
     }
     // ---- start-of-step position: q, then (r, theta) by FP64 Newton -------
-    const double q0 = QL[c0] + (double)o0 * DQ[c0];
-    const double ug = UL[c0] + (double)o0 * UD[c0];
-    const double u = quartic_newton(q0, pG, ug, 2);
-    const double s2 = u * ipG;                       // sin^2(theta)
-    float sf = sqrtf((float)s2);
-    const double st = (double)sf + (s2 - (double)sf * sf) * (0.5 / (double)sf);
+    const double q0 = fma((double)o0, DQ[c0], QL[c0]);
+    const double u = quartic_newton(q0, ipG, fma((double)o0, UD[c0], UL[c0]), 2);
+    const double s2 = u * ipG;  // sin^2(theta)
+    const double st = s2 * rsqrt(s2);
     const double ct = q0 * u * u;
     const double r = u * RE;
     const double rho0 = r * st, z0 = r * ct;
-    const int qi = cell_search(E, T.nq, T.sgn * q0);
+    const int qi = cell_search_from(E, T.nq, T.sgn * q0, c0);
     // ---- k1 geometry in FP32 ---------------------------------------------
     Geo<float> g1;
     g1.ct = (float)ct;
     g1.st = (float)st;
-    g1.ir = (float)(1.0 / r);
+    g1.ir = __frcp_rn((float)u * fRE);
     g1.q = (float)q0;
     g1.ell = 1.0f + 3.0f * g1.ct * g1.ct;
     g1.isl = rsqrtf(g1.ell);
@@ -394,8 +471,8 @@ __global__ void __launch_bounds__(256) k_push32(PushArgs a) {
       }
     } else {
       const int old = I.vb[j];
-      int np_ = vbin(c_vg.fpar, c_vg.npar, vpar);
-      int n1_ = vbin(c_vg.f1, c_vg.n1, sqrtf(vp2));
+      const int np_ = vbin(c_vg.fpar, c_vg.npar, vpar);
+      const int n1_ = vbin(c_vg.f1, c_vg.n1, sqrtf(vp2));
       bp = np_ >= 0 ? np_ : (old & 0xffff) - 1;
       b1 = n1_ >= 0 ? n1_ : (old >> 16) - 1;
       const int nw = ((b1 + 1) << 16) | (bp + 1);
@@ -409,16 +486,21 @@ __global__ void __launch_bounds__(256) k_push32(PushArgs a) {
     const float a1 = apar(g1, vp2, aea, ag, a.ff);
     float v1n = v1, v2n = v2;
     if (a.icr && qi >= 0) {
-      const float B = (float)MDIP * (g1.ell * g1.isl) * (g1.ir * g1.ir * g1.ir);
-      heat<float>(a, (int64_t)T.coff + qi, I.id[j], T.sumdsICR,
-                  (float)qs_ms * B, fabsf(vpar), v1n, v2n);
+      const float rf = (float)r;
+      const float sl = g1.ell * g1.isl;
+      const float ir3 = g1.ir * g1.ir * g1.ir;
+      const float Om = qs_ms * (float)MDIP * sl * ir3;
+      const float invOm = c_invOm * (rf * rf * rf) * g1.isl;
+      const float *hk = HK + 6 * qi;
+      const HeatC<float> hc{hk[0], hk[1], hk[2], hk[3], hk[4], hk[5]};
+      heat<float>(a, hc, I.id[j], invsumds, Om, invOm, fabsf(vpar), v1n, v2n);
     }
     const float rf = (float)rho0, zf = (float)z0;
     const float VRr = vpar * g1.er, VRz = vpar * g1.ez;
-    Geo<float> g2 = geo(rf + hh * VRr, zf + hh * VRz);
+    const Geo<float> g2 = geo(fmaf(hh, VRr, rf), fmaf(hh, VRz, zf));
     const float a2 = apar(g2, vp2, aea, ag, a.ff);
     const float A1r = a1 * g1.er, A1z = a1 * g1.ez;
-    Geo<float> g4 = geo(rf + h * VRr + hsq2 * A1r, zf + h * VRz + hsq2 * A1z);
+    const Geo<float> g4 = geo(rf + h * VRr + hsq2 * A1r, zf + h * VRz + hsq2 * A1z);
     const float a4 = apar(g4, vp2, aea, ag, a.ff);
     if (a.write_qk4) I.fqk4[j] = g4.q;
     const float A2r = a2 * g2.er, A2z = a2 * g2.ez;
@@ -432,13 +514,13 @@ __global__ void __launch_bounds__(256) k_push32(PushArgs a) {
     const double xr = rho0 + (double)dr, xz = z0 + (double)dz;
     const double r2 = xr * xr + xz * xz;
     double y = (double)rsqrtf((float)r2);
-    y = y * (1.5 - 0.5 * r2 * y * y);
+    y = y * fma(-0.5 * r2 * y, y, 1.5);
     const double qN = (RE * RE) * xz * (y * y * y);
-    int cN = cell_search(E, T.nq, T.sgn * qN);
+    const int cN = cell_search_from(E, T.nq, T.sgn * qN, qi >= 0 ? qi : c0);
     const int cpos = cN >= 0 ? cN : (cN == BELOW ? 0 : T.nq - 1);
-    const float oN = (float)((qN - QL[cpos]) / DQ[cpos]);
+    const float oN = (float)((qN - QL[cpos]) * IDQ[cpos]);
     // ---- V|| along the new field direction (FP32) -----------------------
-    Geo<float> gN = geo((float)xr, (float)xz);
+    const Geo<float> gN = geo((float)xr, (float)xz);
     const float vparN = gN.er * VNr + gN.ez * VNz;
     if (!isfinite(vparN) || !isfinite(oN)) atomicOr(a.status, ST_NAN);
     I.cell[j] = cpos;

@@ -312,8 +312,13 @@ static void wave_heating(orc *o, int64_t j, int64_t Qk1, double OmegaGk1,
          xi2 = o->XiPerp2[c], S0 = o->S0[c], Om0 = o->OmegaG0[c],
          chi1 = o->ChiPerp1[c], chi2 = o->ChiPerp2[c];
   uint32_t step = (uint32_t)o->n;
-  double G1 = gauss(P->seed, o->id[j], step, KAOS_RNG_HEAT, 0);
-  double G2 = gauss(P->seed, o->id[j], step, KAOS_RNG_HEAT, 1);
+  /* two Gaussians from one draw: both Box-Muller branches */
+  kaos_u32x4 wr = kaos_philox((uint32_t)o->id[j], (uint32_t)(o->id[j] >> 32),
+                              step, KAOS_RNG_HEAT << 24, P->seed);
+  double R = sqrt(-2.0 * log(kaos_u01(wr.v[0], wr.v[1])));
+  double u2 = kaos_u01(wr.v[2], wr.v[3]);
+  double G1 = R * cos(2.0 * PI * u2);
+  double G2 = R * sin(2.0 * PI * u2);
   double vpm = sqrt(sq(o->V1[j]) + sq(o->V2[j]));
   double Sig = 1.0;
   if ((lam != 0.0) && (((2.0 * PI * vpm) / OmegaGk1) >= lam))
