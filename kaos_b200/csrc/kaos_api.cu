@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "kaos_cx.cuh"
 #include "kaos_tube.cuh"
 
 using namespace kaos;
@@ -89,6 +90,18 @@ struct kaos_handle {
   Accum acc{};
   Ions ion[2]{};
   int cur = 0;
+  // ENA population (charge exchange)
+  Enas ena[2]{};
+  int ecur = 0;
+  int64_t *d_nena = nullptr, *d_nena_new = nullptr;
+  int *d_eblk_tube = nullptr, *d_tube_eblk0 = nullptr;
+  int64_t *d_eblk_start = nullptr, *d_eblkcnt = nullptr, *d_eblkoff = nullptr;
+  int neblk = 0;
+  unsigned long long *d_lbe_out = nullptr, *d_ube_out = nullptr;
+  int *d_cx_tube = nullptr, *d_tube_cx0 = nullptr, *d_cxneed = nullptr;
+  int64_t *d_cx_start = nullptr;
+  unsigned *d_cxc = nullptr, *d_cxo = nullptr;
+  int ncx = 0;
   int64_t n = 0;      // computational steps taken
   int export_on = 0;
   int have_import = 0;
@@ -270,6 +283,7 @@ Fields ion_fields(kaos_handle *h, int from, int to) {
     add(A.rho, B.rho, 8); add(A.z, B.z, 8); add(A.vpar, B.vpar, 8);
     add(A.v1, B.v1, 8); add(A.v2, B.v2, 8); add(A.aea, B.aea, 8);
     add(A.ag, B.ag, 8); add(A.qk4, B.qk4, 8);
+    add(A.rho4, B.rho4, 8); add(A.z4, B.z4, 8);
   }
   add(A.qind, B.qind, 4);
   add(A.vb, B.vb, 4);
@@ -331,6 +345,93 @@ int launch_inject(kaos_handle *h, int ub) {
   return KAOS_OK;
 }
 
+CxArgs cx_args(kaos_handle *h) {
+  CxArgs a{};
+  a.tubes = h->d_tubes;
+  a.cx_tube = h->d_cx_tube;
+  a.cx_start = h->d_cx_start;
+  a.tube_cx0 = h->d_tube_cx0;
+  a.nlive = h->d_nlive;
+  a.ct = h->ct;
+  a.ion = h->ion[h->cur];
+  a.ena = h->ena[h->ecur];
+  a.nena = h->d_nena;
+  a.cxc = h->d_cxc;
+  a.cxo = h->d_cxo;
+  a.cxneed = h->d_cxneed;
+  a.nqmax = max_nq(h);
+  a.mixed = h->mixed;
+  a.status = h->d_status;
+  return a;
+}
+
+// charge exchange at the start of a step (_8_KineticSolver.f90:95-166)
+int launch_cx(kaos_handle *h) {
+  CxArgs a = cx_args(h);
+  const int nq = max_nq(h);
+  k_cx_count<<<h->ncx, 256, (size_t)nq * sizeof(unsigned), h->s>>>(a);
+  k_cx_scan<<<h->ntubes, 256, 0, h->s>>>(a);
+  k_cx_convert<<<h->ncx, 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
+  h->launches += 3;
+  CK(cudaGetLastError());
+  return KAOS_OK;
+}
+
+int launch_push_ena(kaos_handle *h) {
+  EnaArgs a{};
+  a.tubes = h->d_tubes;
+  a.blk_tube = h->d_eblk_tube;
+  a.blk_start = h->d_eblk_start;
+  a.chunk = PUSH_THREADS * PUSH_ITEMS;
+  a.nena = h->d_nena;
+  a.ct = h->ct;
+  a.ena = h->ena[h->ecur];
+  a.h = h->P.h;
+  a.grav_GM = GG * ME;
+  a.grav = h->P.GRAVflag == 1;
+  k_push_ena<<<h->neblk, PUSH_THREADS, (size_t)(max_nq(h) + 1) * sizeof(double), h->s>>>(a);
+  h->launches++;
+  CK(cudaGetLastError());
+  return KAOS_OK;
+}
+
+int launch_boundary_ena(kaos_handle *h) {
+  BcArgs b{};
+  b.tubes = h->d_tubes;
+  b.blk_tube = h->d_eblk_tube;
+  b.blk_start = h->d_eblk_start;
+  b.tube_blk0 = h->d_tube_eblk0;
+  b.chunk = PUSH_THREADS * PUSH_ITEMS;
+  b.nlive = h->d_nena_new;
+  b.qind = h->ena[h->ecur].qind;
+  b.blkcnt = h->d_eblkcnt;
+  b.blkoff = h->d_eblkoff;
+  b.lb_out = h->d_lbe_out;
+  b.ub_out = h->d_ube_out;
+  b.ena = 1;
+  const Enas &A = h->ena[h->ecur], &B = h->ena[1 - h->ecur];
+  Fields F{};
+  F.f[F.n++] = Field{A.x, B.x, 8}; F.f[F.n++] = Field{A.y, B.y, 8};
+  F.f[F.n++] = Field{A.z, B.z, 8}; F.f[F.n++] = Field{A.vx, B.vx, 8};
+  F.f[F.n++] = Field{A.vy, B.vy, 8}; F.f[F.n++] = Field{A.vz, B.vz, 8};
+  F.f[F.n++] = Field{A.vps, B.vps, 8}; F.f[F.n++] = Field{A.vphs, B.vphs, 8};
+  F.f[F.n++] = Field{A.qind, B.qind, 4}; F.f[F.n++] = Field{A.id, B.id, 8};
+  b.fields = F;
+  CK(cudaMemsetAsync(h->d_lbe_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
+  CK(cudaMemsetAsync(h->d_ube_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
+  BcArgs bc = b;
+  bc.nlive = h->d_nena;
+  k_bc_count<<<h->neblk, BC_THREADS, 0, h->s>>>(bc);
+  k_bc_scan<<<h->ntubes, 32, 0, h->s>>>(b);
+  k_bc_scatter<<<h->neblk, BC_THREADS, 0, h->s>>>(b, h->d_nena);
+  h->launches += 3;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->d_nena, h->d_nena_new, h->ntubes * sizeof(int64_t),
+                     cudaMemcpyDeviceToDevice, h->s));
+  h->ecur = 1 - h->ecur;
+  return KAOS_OK;
+}
+
 // One computational step n = h->n + 1.
 int step_once(kaos_handle *h) {
   const int64_t n = h->n + 1;
@@ -359,15 +460,17 @@ int step_once(kaos_handle *h) {
     p.step = (uint32_t)n;
     p.prologue = 1;  // interpolate at q0 (qk4 holds q0 after loading)
     p.write_qind = 1;
-    p.write_qk4 = next_master;
+    p.write_qk4 = next_master || qx;
     if ((rc = launch_push(h, p))) return rc;
     h->n = n;
     return KAOS_OK;
   }
   const bool master = is_master(h, n);
   const uint32_t nn = (uint32_t)(n / h->P.ndatfac + 1);
+  if (qx && (rc = launch_cx(h))) return rc;
   if (master) {
     if ((rc = launch_boundary(h))) return rc;
+    if (qx && (rc = launch_boundary_ena(h))) return rc;
     if ((rc = launch_fields(h, 1))) return rc;
     if ((rc = zero_accum(h))) return rc;
   }
@@ -376,8 +479,9 @@ int step_once(kaos_handle *h) {
   p.bin = master;
   p.prologue = master;
   p.write_qind = (!h->mixed) || next_master || qx || h->export_on;
-  p.write_qk4 = next_master;
+  p.write_qk4 = next_master || qx;
   if ((rc = launch_push(h, p))) return rc;
+  if (qx && (rc = launch_push_ena(h))) return rc;
   if (master) {
     if (h->P.LBCONDITIONflag == 1 && (rc = launch_inject(h, 0))) return rc;
     if (h->P.UBCONDITIONflag == 1 && (rc = launch_inject(h, 1))) return rc;
@@ -433,7 +537,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   std::vector<double> qGL, qGH, qGC, hqC, dqC, d3xC, rGC, thC, elC, TeG, TsG,
       neut, lam, eta, xi1, xi2, S0, Om0, chi1, chi2, uL, uH, hK1, hK2, hc1,
       hc2, hiom0;
-  int64_t poff = 0, coff = 0, moff = 0, hoff = 0;
+  int64_t poff = 0, coff = 0, moff = 0, hoff = 0, eoff = 0;
   for (int t = 0; t < ntubes; ++t) {
     const kaos_tube_c &T = tubes[t];
     if (T.nq < 6 || T.nq > 4096 || T.capacity < 1 || !T.qGL || !T.qGH ||
@@ -463,6 +567,9 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     d.sumdsICR = T.sumdsICR;
     d.moff = moff;
     d.hoff = hoff;
+    d.ecap = (p->QEXCHANGEflag == 1) ? (int64_t)T.capacity / 4 + 4096 : 0;
+    d.eoff = eoff;
+    eoff += d.ecap;
     host_rho_z(T.qGC[0], T.pG, &d.rhoLB, &d.zLB);
     host_rho_z(T.qGC[T.nq - 1], T.pG, &d.rhoUB, &d.zUB);
     h->th.push_back(d);
@@ -579,10 +686,68 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
       if ((rc = dalloc(h, &I.aea, cap))) return rc;
       if ((rc = dalloc(h, &I.ag, cap))) return rc;
       if ((rc = dalloc(h, &I.qk4, cap))) return rc;
+      if (p->QEXCHANGEflag == 1) {
+        if ((rc = dalloc(h, &I.rho4, cap))) return rc;
+        if ((rc = dalloc(h, &I.z4, cap))) return rc;
+      }
     }
     if ((rc = dalloc(h, &I.qind, cap))) return rc;
     if (!h->three_d && (rc = dalloc(h, &I.vb, cap))) return rc;
     if ((rc = dalloc(h, &I.id, cap))) return rc;
+  }
+  // ENA arrays, block map and charge-exchange chunk map
+  if (p->QEXCHANGEflag == 1) {
+    const int64_t ecap_all = eoff;
+    for (int b = 0; b < 2; ++b) {
+      Enas &E = h->ena[b];
+      if ((rc = dalloc(h, &E.x, ecap_all)) || (rc = dalloc(h, &E.y, ecap_all)) ||
+          (rc = dalloc(h, &E.z, ecap_all)) || (rc = dalloc(h, &E.vx, ecap_all)) ||
+          (rc = dalloc(h, &E.vy, ecap_all)) || (rc = dalloc(h, &E.vz, ecap_all)) ||
+          (rc = dalloc(h, &E.vps, ecap_all)) || (rc = dalloc(h, &E.vphs, ecap_all)) ||
+          (rc = dalloc(h, &E.qind, ecap_all)) || (rc = dalloc(h, &E.id, ecap_all)))
+        return rc;
+    }
+    std::vector<int> ebt, te0, cxt, tc0;
+    std::vector<int64_t> ebs, cxs;
+    for (int t = 0; t < ntubes; ++t) {
+      te0.push_back((int)ebt.size());
+      for (int64_t s0 = 0; s0 < h->th[t].ecap; s0 += chunk) {
+        ebt.push_back(t);
+        ebs.push_back(s0);
+      }
+      tc0.push_back((int)cxt.size());
+      for (int64_t s0 = 0; s0 < h->th[t].cap; s0 += CX_CHUNK) {
+        cxt.push_back(t);
+        cxs.push_back(s0);
+      }
+    }
+    te0.push_back((int)ebt.size());
+    tc0.push_back((int)cxt.size());
+    h->neblk = (int)ebt.size();
+    h->ncx = (int)cxt.size();
+    auto up_i = [&](int **d, const std::vector<int> &v) {
+      int r = dalloc(h, d, v.size());
+      if (!r && cudaMemcpy(*d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        r = fail(h, KAOS_ERR_CUDA, "upload failed");
+      return r;
+    };
+    auto up_l = [&](int64_t **d, const std::vector<int64_t> &v) {
+      int r = dalloc(h, d, v.size());
+      if (!r && cudaMemcpy(*d, v.data(), v.size() * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess)
+        r = fail(h, KAOS_ERR_CUDA, "upload failed");
+      return r;
+    };
+    if ((rc = up_i(&h->d_eblk_tube, ebt)) || (rc = up_l(&h->d_eblk_start, ebs)) ||
+        (rc = up_i(&h->d_tube_eblk0, te0)) || (rc = up_i(&h->d_cx_tube, cxt)) ||
+        (rc = up_l(&h->d_cx_start, cxs)) || (rc = up_i(&h->d_tube_cx0, tc0)))
+      return rc;
+    if ((rc = dalloc(h, &h->d_nena, ntubes)) || (rc = dalloc(h, &h->d_nena_new, ntubes)) ||
+        (rc = dalloc(h, &h->d_eblkcnt, ebt.size())) || (rc = dalloc(h, &h->d_eblkoff, ebt.size())) ||
+        (rc = dalloc(h, &h->d_lbe_out, ntubes)) || (rc = dalloc(h, &h->d_ube_out, ntubes)) ||
+        (rc = dalloc(h, &h->d_cxneed, cxt.size())) ||
+        (rc = dalloc(h, &h->d_cxc, cxt.size() * (size_t)max_nq(h))) ||
+        (rc = dalloc(h, &h->d_cxo, cxt.size() * (size_t)max_nq(h))))
+      return rc;
   }
   CK(cudaDeviceSynchronize());
   return KAOS_OK;
@@ -754,7 +919,12 @@ int kaos_get_count(kaos_handle *h, int32_t tube, int64_t *nion, int64_t *nena) {
   int64_t dead = 0;
   for (auto v : q) dead += (v == DEAD);
   if (nion) *nion = nl - dead;
-  if (nena) *nena = 0;
+  int64_t ne = 0;
+  if (h->d_nena) {
+    CK(cudaMemcpy(&ne, h->d_nena + tube, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    ne = std::min(ne, h->th[tube].ecap);
+  }
+  if (nena) *nena = ne;
   return KAOS_OK;
 }
 
@@ -887,9 +1057,18 @@ int kaos_get_positions(kaos_handle *h, int32_t tube, double *rho, double *z,
 
 int kaos_get_enas(kaos_handle *h, int32_t tube, double *x, double *y, double *z,
                   double *vx, double *vy, double *vz, int64_t n) {
-  (void)x; (void)y; (void)z; (void)vx; (void)vy; (void)vz;
   if (!h || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
-  if (n != 0) return fail(h, KAOS_ERR_PARAM, "no ENA population");
+  int64_t ni = 0, ne = 0;
+  int rc = kaos_get_count(h, tube, &ni, &ne);
+  if (rc) return rc;
+  if (n != ne) return fail(h, KAOS_ERR_PARAM, "n (%lld) must equal the ENA count (%lld)", (long long)n, (long long)ne);
+  if (ne == 0) return KAOS_OK;
+  const Enas &E = h->ena[h->ecur];
+  const int64_t o = h->th[tube].eoff;
+  double *dst[6] = {x, y, z, vx, vy, vz};
+  double *src[6] = {E.x, E.y, E.z, E.vx, E.vy, E.vz};
+  for (int k = 0; k < 6; ++k)
+    if (dst[k]) CK(cudaMemcpy(dst[k], src[k] + o, ne * sizeof(double), cudaMemcpyDeviceToHost));
   return KAOS_OK;
 }
 

@@ -66,6 +66,7 @@ struct CellTables {
 // Ion particle arrays.  FP64 mode uses the d* arrays, mixed the f* ones.
 struct Ions {
   double *rho, *z, *vpar, *v1, *v2, *aea, *ag, *qk4;  // FP64 mode
+  double *rho4, *z4;   // FP64 + charge exchange: the k4 point of the step
   int32_t *cell;                                      // mixed: position cell
   float *off, *fvpar, *fv1, *fv2, *faea, *fag, *fqk4;  // mixed mode
   int32_t *qind;       // start-of-step cell Qindk1 (0-based, sentinels)

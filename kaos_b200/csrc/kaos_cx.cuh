@@ -1,0 +1,300 @@
+// kaos_cx.cuh -- ion -> ENA charge exchange and the ballistic ENA push.
+//
+// Reference: the production loop of KineticSolverSub
+// (_8_KineticSolver.f90:95-166) converts, on every computational step, the
+// first nint(nuIonNeutPoiT(nn-1,Q)) ions (in particle-index order) whose
+// Qindk1 is Q into ENAs (IonNeutralCollisionsSub
+// _8_1_1_1_IonNeutralCollisions.f90:25-58); ENAs then move under gravity
+// only (AGENA*sub _KineticMainParams.f90:695-714, KineticRK4UpdateSub
+// :186-193, :292-314).
+//
+// Selection on the GPU keeps the index order exactly: per-chunk counts of
+// eligible ions per cell, an exclusive scan over chunks per cell, then an
+// in-order walk of only those chunks that hold converted ions.
+#pragma once
+#include "kaos_push.cuh"
+
+namespace kaos {
+
+constexpr int CX_CHUNK = 16384;  // particles per selection chunk
+
+struct CxArgs {
+  const TubeD *tubes;
+  const int *cx_tube;        // chunk -> tube
+  const int64_t *cx_start;   // chunk -> first particle (tube-relative)
+  const int *tube_cx0;       // first chunk of each tube (ntubes+1)
+  const int64_t *nlive;
+  CellTables ct;
+  Ions ion;
+  Enas ena;
+  int64_t *nena;
+  unsigned *cxc;             // [chunk][nq_max] eligible counts
+  unsigned *cxo;             // [chunk][nq_max] exclusive prefix
+  int *cxneed;               // chunk has conversions
+  int nqmax, mixed;
+  uint32_t *status;
+};
+
+// per-chunk counts of ions per start-of-step cell
+__global__ void k_cx_count(CxArgs a) {
+  extern __shared__ unsigned hs[];
+  const int c = blockIdx.x;
+  const int t = a.cx_tube[c];
+  const TubeD &T = a.tubes[t];
+  for (int k = threadIdx.x; k < T.nq; k += blockDim.x) hs[k] = 0;
+  __syncthreads();
+  const int64_t nl = a.nlive[t];
+  const int64_t beg = a.cx_start[c], end = min(beg + (int64_t)CX_CHUNK, nl);
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const int q = a.ion.qind[T.off + i];
+    if (q >= 0 && a.ct.nuPoi[T.coff + q] > 0.0) atomicAdd(&hs[q], 1u);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < T.nq; k += blockDim.x)
+    a.cxc[(int64_t)c * a.nqmax + k] = hs[k];
+}
+
+// exclusive scan over the chunks of each tube, per cell; flags chunks that
+// contain ions to convert.  One block per tube, one thread per cell.
+__global__ void k_cx_scan(CxArgs a) {
+  const int t = blockIdx.x;
+  const TubeD &T = a.tubes[t];
+  const int c0 = a.tube_cx0[t], c1 = a.tube_cx0[t + 1];
+  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) a.cxneed[c] = 0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
+    const double nu = a.ct.nuPoi[T.coff + k];
+    const unsigned need = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
+    unsigned s = 0;
+    for (int c = c0; c < c1; ++c) {
+      const unsigned n = a.cxc[(int64_t)c * a.nqmax + k];
+      a.cxo[(int64_t)c * a.nqmax + k] = s;
+      if (n && s < need) a.cxneed[c] = 1;
+      s += n;
+    }
+  }
+}
+
+// Cartesian unit vectors along B (par), across the shell (p) and in
+// longitude (phi) at polar cos/sin (ct, st) and longitude (cp, sp).
+__device__ __forceinline__ void dipole_frame(double ct, double st, double cp,
+                                             double sp, double e_par[3],
+                                             double e_p[3], double e_phi[3]) {
+  const double isl = rsqrt(1.0 + 3.0 * ct * ct);
+  const double a = 3.0 * ct * st * isl, b = (3.0 * ct * ct - 1.0) * isl;
+  const double c = (1.0 - 3.0 * ct * ct) * isl;
+  e_par[0] = cp * a; e_par[1] = sp * a; e_par[2] = b;
+  e_p[0] = cp * c;   e_p[1] = sp * c;   e_p[2] = a;
+  e_phi[0] = -sp;    e_phi[1] = cp;     e_phi[2] = 0.0;
+}
+
+// in-order conversion of the first need[Q] eligible ions per cell
+__global__ void k_cx_convert(CxArgs a) {
+  const int c = blockIdx.x;
+  if (!a.cxneed[c]) return;
+  extern __shared__ unsigned sm_[];
+  const int t = a.cx_tube[c];
+  const TubeD &T = a.tubes[t];
+  unsigned *need = sm_;                 // remaining conversions per cell
+  unsigned *wcnt = sm_ + a.nqmax;       // [8 warps][nq] per-tile counts
+  for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
+    const double nu = a.ct.nuPoi[T.coff + k];
+    const unsigned nd = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
+    const unsigned o = a.cxo[(int64_t)c * a.nqmax + k];
+    need[k] = nd > o ? nd - o : 0u;
+  }
+  __syncthreads();
+  const int64_t nl = a.nlive[t];
+  const int64_t beg = a.cx_start[c], end = min(beg + (int64_t)CX_CHUNK, nl);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int64_t r0 = beg; r0 < end; r0 += blockDim.x) {
+    const int64_t i = r0 + threadIdx.x;
+    int q = -1;
+    if (i < end) {
+      q = a.ion.qind[T.off + i];
+      if (q < 0 || need[q] == 0) q = -1;
+    }
+    // rank among same-cell candidates of this tile, in index order
+    const unsigned peers = __match_any_sync(0xffffffffu, q);
+    const int wr = __popc(peers & ((1u << l) - 1u));
+    for (int k = threadIdx.x; k < nw * T.nq; k += blockDim.x) wcnt[k] = 0;
+    __syncthreads();
+    if (q >= 0 && wr == 0) wcnt[w * T.nq + q] = __popc(peers);
+    __syncthreads();
+    bool conv = false;
+    if (q >= 0) {
+      unsigned before = 0;
+      for (int v = 0; v < w; ++v) before += wcnt[v * T.nq + q];
+      conv = (before + (unsigned)wr) < need[q];
+    }
+    __syncthreads();
+    // consume: need[q] -= min(need, tile count) (one thread per cell)
+    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
+      unsigned tot = 0;
+      for (int v = 0; v < nw; ++v) tot += wcnt[v * T.nq + k];
+      need[k] = need[k] > tot ? need[k] - tot : 0u;
+    }
+    if (conv) {
+      const int64_t j = T.off + i;
+      // ion position and velocity at the end of the previous step
+      double rho, z, vpar, v1, v2, qk4;
+      if (a.mixed) {
+        const int cc = a.ion.cell[j];
+        const double qq = a.ct.qGL[T.coff + cc] +
+                          (double)a.ion.off[j] * (a.ct.qGH[T.coff + cc] - a.ct.qGL[T.coff + cc]);
+        const double ug = a.ct.uL[T.coff + cc] +
+                          (double)a.ion.off[j] * (a.ct.uH[T.coff + cc] - a.ct.uL[T.coff + cc]);
+        const double u = quartic_newton(qq, 1.0 / T.pG, ug, 3);
+        const double s2 = u / T.pG;
+        rho = u * RE * sqrt(s2);
+        z = u * RE * qq * u * u;
+        vpar = a.ion.fvpar[j];
+        v1 = a.ion.fv1[j];
+        v2 = a.ion.fv2[j];
+        qk4 = a.ion.fqk4[j];
+      } else {
+        rho = a.ion.rho[j];
+        z = a.ion.z[j];
+        vpar = a.ion.vpar[j];
+        v1 = a.ion.v1[j];
+        v2 = a.ion.v2[j];
+        qk4 = a.ion.qk4[j];
+      }
+      // geometry of the k4 point of the previous step: stored exactly in
+      // FP64 mode, rebuilt from its q (p = pG) in mixed mode
+      double ctk, stk;
+      if (a.ion.rho4) {
+        const Geo<double> g4 = geo(a.ion.rho4[j], a.ion.z4[j]);
+        ctk = g4.ct;
+        stk = g4.st;
+      } else {
+        const double uk = quartic_newton(qk4, 1.0 / T.pG, sqrt(rho * rho + z * z) / RE, 4);
+        ctk = qk4 * uk * uk;
+        stk = sqrt(uk / T.pG);
+      }
+      const Geo<double> gN = geo(rho, z);
+      double ep[3], epp[3], eph[3], e4[3], e4p[3], e4h[3];
+      dipole_frame(gN.ct, gN.st, T.cphi, T.sphi, ep, epp, eph);
+      dipole_frame(ctk, stk, T.cphi, T.sphi, e4, e4p, e4h);
+      const double VN[3] = {vpar * ep[0], vpar * ep[1], vpar * ep[2]};
+      const double vp4 = e4[0] * VN[0] + e4[1] * VN[1] + e4[2] * VN[2];
+      const int64_t slot = atomicAdd((unsigned long long *)&a.nena[t], 1ull);
+      if (slot < T.ecap) {
+        const int64_t e = T.eoff + slot;
+        a.ena.x[e] = rho * T.cphi;
+        a.ena.y[e] = rho * T.sphi;
+        a.ena.z[e] = z;
+        a.ena.vx[e] = vp4 * e4[0] + v1 * e4p[0] + v2 * e4h[0];
+        a.ena.vy[e] = vp4 * e4[1] + v1 * e4p[1] + v2 * e4h[1];
+        a.ena.vz[e] = vp4 * e4[2] + v1 * e4p[2] + v2 * e4h[2];
+        a.ena.vps[e] = 0.0;  // Vp(j), Vphi(j) still hold the ion zeros
+        a.ena.vphs[e] = 0.0;
+        a.ena.qind[e] = q;
+        a.ena.id[e] = a.ion.id[j];
+      } else {
+        atomicOr(a.status, ST_CAP);
+      }
+      a.ion.qind[j] = DEAD;
+      if (a.mixed) a.ion.cell[j] = DEAD;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ballistic ENA step under gravity (FP64): the ENA branch of
+// KineticUpdateA/B/C and KineticRK4UpdateSub, including the reference's
+// |Vp| in the rebuilt velocity (_8_1_1_KineticUpdateA.f90:1155-1160,
+// _8_1_KineticRK4Update.f90:292-314) and the cell index for removal.
+struct EnaArgs {
+  const TubeD *tubes;
+  const int *blk_tube;
+  const int64_t *blk_start;
+  int chunk;
+  const int64_t *nena;
+  CellTables ct;
+  Enas ena;
+  double h, grav_GM;
+  int grav;
+};
+
+__device__ __forceinline__ void ena_geo(const double x[3], double &ct,
+                                        double &st, double &cp, double &sp,
+                                        double &q, double &ir) {
+  const double rho2 = x[0] * x[0] + x[1] * x[1];
+  const double r2 = rho2 + x[2] * x[2];
+  ir = rsqrt(r2);
+  ct = x[2] * ir;
+  const double rho = sqrt(rho2);
+  st = rho * ir;
+  if (rho > 0.0) { cp = x[0] / rho; sp = x[1] / rho; } else { cp = 1.0; sp = 0.0; }
+  q = (RE * RE) * ct * ir * ir;
+}
+
+__device__ __forceinline__ void ena_acc(const EnaArgs &a, const double x[3],
+                                        double A[3]) {
+  if (!a.grav) { A[0] = A[1] = A[2] = 0.0; return; }
+  const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+  const double ir = rsqrt(r2);
+  const double g = -a.grav_GM * ir * ir * ir;
+  A[0] = g * x[0]; A[1] = g * x[1]; A[2] = g * x[2];
+}
+
+__global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
+  extern __shared__ double sm[];
+  const int t = a.blk_tube[blockIdx.x];
+  const TubeD &T = a.tubes[t];
+  double *E = sm;
+  for (int k = threadIdx.x; k <= T.nq; k += blockDim.x)
+    E[k] = (k < T.nq) ? T.sgn * a.ct.qGL[T.coff + k] : T.sgn * a.ct.qGH[T.coff + T.nq - 1];
+  __syncthreads();
+  const int64_t nl = min(a.nena[t], T.ecap);
+  const int64_t beg = a.blk_start[blockIdx.x];
+  const int64_t end = min(beg + (int64_t)a.chunk, nl);
+  const double h = a.h, hh = 0.5 * h, h6 = h / 6.0, hsq2 = 0.5 * h * h;
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const int64_t e = T.eoff + i;
+    double x[3] = {a.ena.x[e], a.ena.y[e], a.ena.z[e]};
+    const double V[3] = {a.ena.vx[e], a.ena.vy[e], a.ena.vz[e]};
+    double ct, st, cp, sp, q, ir;
+    ena_geo(x, ct, st, cp, sp, q, ir);
+    int qi = cell_search(E, T.nq, T.sgn * q);
+    double ep[3], epp[3], eph[3];
+    dipole_frame(ct, st, cp, sp, ep, epp, eph);
+    const double vpar = ep[0] * V[0] + ep[1] * V[1] + ep[2] * V[2];
+    double vps = a.ena.vps[e], vphs = a.ena.vphs[e];
+    if (qi >= 0) {
+      vps = fabs(epp[0] * V[0] + epp[1] * V[1] + epp[2] * V[2]);
+      vphs = eph[0] * V[0] + eph[1] * V[1];
+    }
+    double VR[3], A1[3], A2[3], A4[3], x2[3], x4[3];
+    for (int k = 0; k < 3; ++k) VR[k] = vpar * ep[k] + vps * epp[k] + vphs * eph[k];
+    ena_acc(a, x, A1);
+    for (int k = 0; k < 3; ++k) x2[k] = x[k] + hh * VR[k];
+    ena_acc(a, x2, A2);
+    for (int k = 0; k < 3; ++k) x4[k] = x[k] + h * VR[k] + hsq2 * A1[k];
+    ena_acc(a, x4, A4);
+    double VN[3], xN[3];
+    for (int k = 0; k < 3; ++k) {
+      VN[k] = VR[k] + h6 * (A1[k] + 2.0 * A2[k] + 2.0 * A2[k] + A4[k]);
+      const double vk2 = VR[k] + hh * A1[k], vk4 = VR[k] + h * A2[k];
+      xN[k] = x[k] + h6 * (VR[k] + 2.0 * vk2 + 2.0 * vk2 + vk4);
+    }
+    ena_geo(xN, ct, st, cp, sp, q, ir);
+    dipole_frame(ct, st, cp, sp, ep, epp, eph);
+    const double vparN = ep[0] * VN[0] + ep[1] * VN[1] + ep[2] * VN[2];
+    const double vpN = fabs(epp[0] * VN[0] + epp[1] * VN[1] + epp[2] * VN[2]);
+    const double vphN = eph[0] * VN[0] + eph[1] * VN[1];
+    a.ena.x[e] = xN[0];
+    a.ena.y[e] = xN[1];
+    a.ena.z[e] = xN[2];
+    a.ena.vx[e] = vparN * ep[0] + vpN * epp[0] + vphN * eph[0];
+    a.ena.vy[e] = vparN * ep[1] + vpN * epp[1] + vphN * eph[1];
+    a.ena.vz[e] = vparN * ep[2] + vpN * epp[2] + vphN * eph[2];
+    a.ena.vps[e] = vps;
+    a.ena.vphs[e] = vphs;
+    a.ena.qind[e] = qi;
+  }
+}
+
+}  // namespace kaos

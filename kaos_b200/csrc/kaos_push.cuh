@@ -344,7 +344,13 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
     const double A1r = a1 * g1.er, A1z = a1 * g1.ez;
     const Geo<double> g4 = geo(rho + h * VRr + hsq2 * A1r, z + h * VRz + hsq2 * A1z);
     const double a4 = apar(g4, vp2, aea, ag, a.ff);
-    if (a.write_qk4) I.qk4[j] = g4.q;
+    if (a.write_qk4) {
+      I.qk4[j] = g4.q;
+      if (I.rho4) {  // KineticUpdateC stores the k4 geometry for collisions
+        I.rho4[j] = rho + h * VRr + hsq2 * A1r;
+        I.z4[j] = z + h * VRz + hsq2 * A1z;
+      }
+    }
     const double A2r = a2 * g2.er, A2z = a2 * g2.ez;
     const double A4r = a4 * g4.er, A4z = a4 * g4.ez;
     // ---- RK combination (k3 = k2) ---------------------------------------

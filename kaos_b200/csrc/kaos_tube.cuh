@@ -302,6 +302,7 @@ struct BcArgs {
   int64_t *blkcnt, *blkoff;
   unsigned long long *lb_out, *ub_out;  // per tube escape counts
   Fields fields;
+  int ena;  // 1: operate on the ENA segments (tube.eoff) instead of ions
 };
 
 __device__ __forceinline__ bool keep_slot(int q) {
@@ -311,12 +312,13 @@ __device__ __forceinline__ bool keep_slot(int q) {
 __global__ void k_bc_count(BcArgs a) {
   const int t = a.blk_tube[blockIdx.x];
   const TubeD &T = a.tubes[t];
-  const int64_t nl = a.nlive[t];
+  const int64_t toff = a.ena ? T.eoff : T.off;
+  const int64_t nl = a.ena ? min(a.nlive[t], T.ecap) : a.nlive[t];
   const int64_t beg = a.blk_start[blockIdx.x];
   const int64_t end = min(beg + (int64_t)a.chunk, nl);
   int kept = 0, lb = 0, ub = 0;
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
-    int q = a.qind[T.off + i];
+    int q = a.qind[toff + i];
     kept += keep_slot(q);
     lb += (q == BELOW);
     ub += (q == ABOVE);
@@ -355,7 +357,8 @@ __global__ void k_bc_scan(BcArgs a) {
 __global__ void k_bc_scatter(BcArgs a, const int64_t *nlive_old) {
   const int t = a.blk_tube[blockIdx.x];
   const TubeD &T = a.tubes[t];
-  const int64_t nl = nlive_old[t];
+  const int64_t toff = a.ena ? T.eoff : T.off;
+  const int64_t nl = a.ena ? min(nlive_old[t], T.ecap) : nlive_old[t];
   const int64_t beg = a.blk_start[blockIdx.x];
   const int64_t end = min(beg + (int64_t)a.chunk, nl);
   __shared__ int wsum[32];
@@ -366,7 +369,7 @@ __global__ void k_bc_scatter(BcArgs a, const int64_t *nlive_old) {
   for (int64_t r0 = beg; r0 < end; r0 += blockDim.x) {
     const int64_t i = r0 + threadIdx.x;
     const bool in = i < end;
-    const bool k = in && keep_slot(a.qind[T.off + i]);
+    const bool k = in && keep_slot(a.qind[toff + i]);
     const unsigned bal = __ballot_sync(0xffffffffu, k);
     const int wr = __popc(bal & ((1u << l) - 1u));
     if (l == 0) wsum[w] = __popc(bal);
@@ -374,7 +377,7 @@ __global__ void k_bc_scatter(BcArgs a, const int64_t *nlive_old) {
     int woff = 0, tot = 0;
     for (int q = 0; q < nw; ++q) { if (q < w) woff += wsum[q]; tot += wsum[q]; }
     if (k) {
-      const int64_t src = T.off + i, dst = T.off + base + woff + wr;
+      const int64_t src = toff + i, dst = toff + base + woff + wr;
       for (int f = 0; f < a.fields.n; ++f) {
         const Field &F = a.fields.f[f];
         if (F.size == 8)

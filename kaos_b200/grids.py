@@ -187,7 +187,7 @@ def config_small(n_particles=4000, three_d=True, nq=32, steps_per_master=5,
     spec = TubeSpec(L=4.0, nq=nq, n_particles=n_particles,
                     q_ub=0.15, H=600e3,
                     heat_rate_eV_s=5.0 if heating else 0.0,
-                    neut_n0=1e16 if collisions else 0.0, neut_H=300e3)
+                    neut_n0=3e18 if collisions else 0.0, neut_H=300e3)
     tube = make_tube(spec, mi)
     vg = (make_vgrid(True, 16, 16, 24, 8e3) if three_d
           else make_vgrid(False, 16, 0, 24, 8e3))

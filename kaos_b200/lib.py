@@ -156,6 +156,12 @@ class Solver:
         self._check(load().kaos_get_positions(self.h, tube, _p(rho), _p(z), ni))
         return dict(q=q, vpar=vp, vperp1=v1, vperp2=v2, qind=qi, rho=rho, z=z)
 
+    def enas(self, tube=0):
+        _, ne = self.count(tube)
+        a = [np.zeros(ne) for _ in range(6)]
+        self._check(load().kaos_get_enas(self.h, tube, *[_p(x) for x in a], ne))
+        return dict(zip(("x", "y", "z", "vx", "vy", "vz"), a))
+
     def boundary(self, tube=0):
         v = [C.c_int64() for _ in range(4)]
         self._check(load().kaos_get_boundary(self.h, tube, *[C.byref(x) for x in v]))
