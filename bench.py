@@ -89,12 +89,16 @@ def build_workload(precision, n_part=N_PART, heating=True, collisions=False):
     return mi, spec, tube, vg, (q, vpar, v1, v2)
 
 
-def bytes_per_particle_step(mixed, heating):
+def bytes_per_particle_step(mixed, heating, collisions):
     """Algorithmic HBM bytes per ion per ordinary step (reads + writes)."""
     if mixed:  # cell, offset, V||, Vperp1, Vperp2, AEA, AG (4 B each)
         rd, wr = 7 * 4, (5 if heating else 3) * 4
+        if collisions:  # Qindk1 + q at k4 written for the charge exchange
+            wr += 8
     else:      # rho, z, V||, Vperp1, Vperp2, AEA, AG (8 B) + Qindk1 (4 B)
         rd, wr = 7 * 8, (5 if heating else 3) * 8 + 4
+        if collisions:  # q, rho, z at k4
+            wr += 24
     return rd + wr
 
 
@@ -115,16 +119,11 @@ def run_ours(args, precision, mi_tag):
     # library's stream; inputs 0.5-1 GB > L2, so no explicit flush) --------
     s.step(args.steps)
     ms, launches = s.timing()
+    pms, pl = s.push_timing()  # events around each push launch
     n1, _ = s.count()
     nmean = 0.5 * (n0 + n1)
     value = nmean * args.steps / (ms * 1e-3)
-    # --- per-step breakdown: ordinary steps are one push launch ------------
-    per = []
-    for _ in range(min(args.steps, 20)):
-        s.step(1)
-        per.append(s.timing())
-    ordinary = [m for (m, l) in per if l == 1]
-    push_ms = statistics.median(ordinary) if ordinary else ms / args.steps
+    push_ms = pms / max(pl, 1)
     return dict(value=value, ms=ms, launches=launches, n=nmean, push_ms=push_ms,
                 t_load=t_load, solver=s, init=init, tube=tube, mi=mi)
 
@@ -231,7 +230,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--no-heating", action="store_true")
-    ap.add_argument("--collisions", action="store_true")
+    ap.add_argument("--no-collisions", dest="collisions", action="store_false")
     ap.add_argument("--skip-e2e", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -269,7 +268,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * r32["n"] * args.steps / (ms * 1e-3)
-    mixed_bytes = bytes_per_particle_step(True, not args.no_heating)
+    mixed_bytes = bytes_per_particle_step(True, not args.no_heating, args.collisions)
     achieved = mixed_bytes * r32["n"] / (r32["push_ms"] * 1e-3) / 1e9
     peak, peak_kind = peaks()
     e2e = None

@@ -225,6 +225,10 @@ int kaos_get_boundary(kaos_handle *h, int32_t tube, int64_t *lb_out,
  * the handle's stream, and the number of kernels it launched. */
 int kaos_get_timing(kaos_handle *h, double *ms, int64_t *launches);
 
+/* Device time (ms) spent in the particle push kernels alone during the last
+ * kaos_step call (CUDA events around each push launch) and their count. */
+int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches);
+
 /* Record the whole computational step in CUDA graphs (1) or launch the
  * kernels directly (0, default). */
 int kaos_set_graph(kaos_handle *h, int32_t on);

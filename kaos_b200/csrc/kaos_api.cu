@@ -101,6 +101,7 @@ struct kaos_handle {
   int *d_cx_tube = nullptr, *d_tube_cx0 = nullptr, *d_cxneed = nullptr;
   int64_t *d_cx_start = nullptr;
   unsigned *d_cxc = nullptr, *d_cxo = nullptr;
+  int *d_cell_tube = nullptr, *d_cell_q = nullptr;  // global cell -> (tube, cell)
   int ncx = 0;
   int64_t n = 0;      // computational steps taken
   int export_on = 0;
@@ -109,6 +110,9 @@ struct kaos_handle {
   int graph = 0;
   double last_ms = 0.0;
   int64_t launches = 0;
+  std::vector<cudaEvent_t> pev;  // event pairs around push launches
+  int npev = 0;
+  double push_ms = 0.0;
   char err[512] = {0};
 };
 
@@ -223,6 +227,14 @@ int max_nq(const kaos_handle *h) {
 
 int launch_push(kaos_handle *h, const PushArgs &a) {
   const int nq = max_nq(h);
+  if ((int)h->pev.size() < 2 * (h->npev + 1)) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    h->pev.push_back(e0);
+    h->pev.push_back(e1);
+  }
+  CK(cudaEventRecord(h->pev[2 * h->npev], h->s));
   size_t smem = (size_t)(2 * nq + 1) * sizeof(double);
   if (h->mixed) smem += (size_t)5 * nq * sizeof(double) + (size_t)6 * nq * sizeof(float);
   if (h->mixed) {
@@ -232,6 +244,8 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
     if (h->three_d) k_push64<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
     else k_push64<false><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
   }
+  CK(cudaEventRecord(h->pev[2 * h->npev + 1], h->s));
+  h->npev++;
   h->launches++;
   CK(cudaGetLastError());
   return KAOS_OK;
@@ -370,7 +384,8 @@ int launch_cx(kaos_handle *h) {
   CxArgs a = cx_args(h);
   const int nq = max_nq(h);
   k_cx_count<<<h->ncx, 256, (size_t)nq * sizeof(unsigned), h->s>>>(a);
-  k_cx_scan<<<h->ntubes, 256, 0, h->s>>>(a);
+  CK(cudaMemsetAsync(h->d_cxneed, 0, h->ncx * sizeof(int), h->s));
+  k_cx_scan<<<(int)h->ncell, 256, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
   k_cx_convert<<<h->ncx, 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
   h->launches += 3;
   CK(cudaGetLastError());
@@ -737,6 +752,10 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
         r = fail(h, KAOS_ERR_CUDA, "upload failed");
       return r;
     };
+    std::vector<int> ctb, cq;
+    for (int t = 0; t < ntubes; ++t)
+      for (int k = 0; k < h->th[t].nq; ++k) { ctb.push_back(t); cq.push_back(k); }
+    if ((rc = up_i(&h->d_cell_tube, ctb)) || (rc = up_i(&h->d_cell_q, cq))) return rc;
     if ((rc = up_i(&h->d_eblk_tube, ebt)) || (rc = up_l(&h->d_eblk_start, ebs)) ||
         (rc = up_i(&h->d_tube_eblk0, te0)) || (rc = up_i(&h->d_cx_tube, cxt)) ||
         (rc = up_l(&h->d_cx_start, cxs)) || (rc = up_i(&h->d_tube_cx0, tc0)))
@@ -879,6 +898,7 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
   if (nsteps < 0) return fail(h, KAOS_ERR_PARAM, "nsteps < 0");
   CK(cudaMemcpyToSymbolAsync(c_vg, &h->vg, sizeof(VGridC), 0, cudaMemcpyHostToDevice, h->s));
   h->launches = 0;
+  h->npev = 0;
   CK(cudaEventRecord(h->e0, h->s));
   for (int64_t k = 0; k < nsteps; ++k) {
     int rc = step_once(h);
@@ -889,6 +909,12 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, h->e0, h->e1));
   h->last_ms = ms;
+  h->push_ms = 0.0;
+  for (int k = 0; k < h->npev; ++k) {
+    float m = 0.f;
+    CK(cudaEventElapsedTime(&m, h->pev[2 * k], h->pev[2 * k + 1]));
+    h->push_ms += m;
+  }
   uint32_t st = 0;
   CK(cudaMemcpy(&st, h->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
   if (st & ST_NAN) return fail(h, KAOS_ERR_NAN, "non-finite particle state on the device");
@@ -1095,9 +1121,17 @@ int kaos_get_timing(kaos_handle *h, double *ms, int64_t *launches) {
   return KAOS_OK;
 }
 
+int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches) {
+  if (!h) return KAOS_ERR_PARAM;
+  if (ms) *ms = h->push_ms;
+  if (launches) *launches = h->npev;
+  return KAOS_OK;
+}
+
 void kaos_destroy(kaos_handle *h) {
   if (!h) return;
   if (h->s) cudaStreamSynchronize(h->s);
+  for (auto e : h->pev) cudaEventDestroy(e);
   for (void *p : h->allocs) cudaFree(p);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);

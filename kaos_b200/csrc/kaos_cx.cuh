@@ -54,24 +54,39 @@ __global__ void k_cx_count(CxArgs a) {
     a.cxc[(int64_t)c * a.nqmax + k] = hs[k];
 }
 
-// exclusive scan over the chunks of each tube, per cell; flags chunks that
-// contain ions to convert.  One block per tube, one thread per cell.
-__global__ void k_cx_scan(CxArgs a) {
-  const int t = blockIdx.x;
+// exclusive scan over the chunks of a tube for one cell (one block per
+// (tube, cell) pair, block-wide scan); flags chunks holding ions to convert.
+__global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
+  const int t = cell_tube[blockIdx.x], k = cell_q[blockIdx.x];
   const TubeD &T = a.tubes[t];
+  const double nu = a.ct.nuPoi[T.coff + k];
+  const unsigned need = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
   const int c0 = a.tube_cx0[t], c1 = a.tube_cx0[t + 1];
-  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) a.cxneed[c] = 0;
+  __shared__ unsigned wsum[32];
+  __shared__ unsigned base;
+  if (threadIdx.x == 0) base = 0;
   __syncthreads();
-  for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
-    const double nu = a.ct.nuPoi[T.coff + k];
-    const unsigned need = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
-    unsigned s = 0;
-    for (int c = c0; c < c1; ++c) {
-      const unsigned n = a.cxc[(int64_t)c * a.nqmax + k];
+  const int l = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r0 = c0; r0 < c1; r0 += blockDim.x) {
+    const int c = r0 + threadIdx.x;
+    const unsigned n = (c < c1) ? a.cxc[(int64_t)c * a.nqmax + k] : 0u;
+    unsigned x = n;  // inclusive warp scan
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+      if (l >= o) x += y;
+    }
+    if (l == 31) wsum[w] = x;
+    __syncthreads();
+    unsigned woff = 0, tot = 0;
+    for (int v = 0; v < nw; ++v) { if (v < w) woff += wsum[v]; tot += wsum[v]; }
+    const unsigned s = base + woff + x - n;  // exclusive prefix
+    if (c < c1) {
       a.cxo[(int64_t)c * a.nqmax + k] = s;
       if (n && s < need) a.cxneed[c] = 1;
-      s += n;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) base += tot;
+    __syncthreads();
   }
 }
 
@@ -97,17 +112,25 @@ __global__ void k_cx_convert(CxArgs a) {
   const TubeD &T = a.tubes[t];
   unsigned *need = sm_;                 // remaining conversions per cell
   unsigned *wcnt = sm_ + a.nqmax;       // [8 warps][nq] per-tile counts
+  __shared__ unsigned remaining;
+  if (threadIdx.x == 0) remaining = 0;
+  __syncthreads();
   for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
     const double nu = a.ct.nuPoi[T.coff + k];
     const unsigned nd = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
     const unsigned o = a.cxo[(int64_t)c * a.nqmax + k];
+    const unsigned cnt = a.cxc[(int64_t)c * a.nqmax + k];
     need[k] = nd > o ? nd - o : 0u;
+    // conversions that can happen in this chunk
+    const unsigned here = need[k] < cnt ? need[k] : cnt;
+    if (here) atomicAdd(&remaining, here);
   }
   __syncthreads();
   const int64_t nl = a.nlive[t];
   const int64_t beg = a.cx_start[c], end = min(beg + (int64_t)CX_CHUNK, nl);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int64_t r0 = beg; r0 < end; r0 += blockDim.x) {
+    if (remaining == 0) break;  // uniform: read after the tile's last sync
     const int64_t i = r0 + threadIdx.x;
     int q = -1;
     if (i < end) {
@@ -135,6 +158,7 @@ __global__ void k_cx_convert(CxArgs a) {
       need[k] = need[k] > tot ? need[k] - tot : 0u;
     }
     if (conv) {
+      atomicSub(&remaining, 1u);
       const int64_t j = T.off + i;
       // ion position and velocity at the end of the previous step
       double rho, z, vpar, v1, v2, qk4;

@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
 // stages; FP64 for the q reconstruction, the quartic root (Newton from a
 // per-cell linear guess) and the renormalised q of the new position.
 template <bool THREE_D>
-__global__ void __launch_bounds__(256, 3) k_push32(PushArgs a) {
+__global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
   extern __shared__ double sm[];
   const int t = a.blk_tube[blockIdx.x];
   TubeD T;

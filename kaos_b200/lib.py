@@ -26,7 +26,7 @@ EXPORTS = [
     "kaos_set_export", "kaos_get_particles", "kaos_get_positions",
     "kaos_get_enas", "kaos_get_boundary", "kaos_get_timing", "kaos_set_graph",
     "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
-    "kaos_version",
+    "kaos_version", "kaos_get_push_timing",
 ]
 
 _lib = None
@@ -59,6 +59,7 @@ def load(path: str = LIBPATH):
     L.kaos_get_enas.argtypes = [vp, i32] + [vp] * 6 + [i64]
     L.kaos_get_boundary.argtypes = [vp, i32] + [C.POINTER(i64)] * 4
     L.kaos_get_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
+    L.kaos_get_push_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
     L.kaos_set_graph.argtypes = [vp, i32]
     L.kaos_set_launch.argtypes = [vp, i32, i32]
     L.kaos_last_error.argtypes = [vp]
@@ -170,6 +171,11 @@ class Solver:
     def timing(self):
         ms, nl = C.c_double(), C.c_int64()
         self._check(load().kaos_get_timing(self.h, C.byref(ms), C.byref(nl)))
+        return ms.value, nl.value
+
+    def push_timing(self):
+        ms, nl = C.c_double(), C.c_int64()
+        self._check(load().kaos_get_push_timing(self.h, C.byref(ms), C.byref(nl)))
         return ms.value, nl.value
 
     def set_graph(self, on):
