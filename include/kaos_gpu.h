@@ -245,6 +245,37 @@ int kaos_get_status(kaos_handle *h, uint32_t *status);
 
 void kaos_destroy(kaos_handle *h);
 
+/*
+ * Start-of-step statistics without any device allocation.  This entry point
+ * has no counterpart in the reference; it serves callers that cannot call
+ * cudaMalloc -- a host running under a fixed device-memory pool of its own,
+ * code issuing work while a stream is being captured into a CUDA graph, or
+ * a process sharing a GPU under an external memory cap.  It bins n ions
+ * (field-line q, V||, Vperp1, Vperp2: device arrays) into the nq cells
+ * bounded by the nq+1 device edges d_qedges (lower boundary first) and the
+ * velocity grid vg (host arrays), and writes the per-cell moments exactly as
+ * kaos_get_moments reports them after a first step: d_moments is a device
+ * array [11][nq] holding the selectors KAOS_M0 .. KAOS_NQ, d_counts (device,
+ * may be NULL) the nq per-cell ion counts.  `stream` is a cudaStream_t
+ * (NULL: the default stream).
+ *
+ * Scratch histograms live in one file-scope device array of at most 512
+ * cells x (1 + 3 x 128) counters (about 0.79 MB), held by every GPU that
+ * loads the library until the process exits.  nq > 512 or more than 128
+ * velocity cells per axis return KAOS_ERR_CAPACITY.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress) with
+ * the device current; make that first call before any stream capture.  All
+ * calls share the array and each clears it first, so calls that overlap on
+ * the GPU race: serialise them.
+ */
+int kaos_moments_noalloc(const kaos_params_c *p, const kaos_vgrid_c *vg,
+                         int32_t nq, const double *d_qedges,
+                         const double *d_d3x, double nsnormfac,
+                         const double *d_q, const double *d_vpar,
+                         const double *d_vperp1, const double *d_vperp2,
+                         int64_t n, double *d_moments, int64_t *d_counts,
+                         void *stream);
+
 /* Library version string. */
 const char *kaos_version(void);
 

@@ -126,6 +126,81 @@ __global__ void k_fields(TubeArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Moments of one cell from its count and binning marginals, for the
+// allocation-free statistics entry point (ZerothIonMoment
+// .. SecondParIonMoment _8_6_1-_8_6_6 with the NonUniform2D/3D integrators
+// _8_5_*): every integrand there is a sum of single-axis terms at the bin
+// centres, so the per-axis marginal counts carry all the information.
+// M[] is indexed by the KAOS_M* selectors 0..9.
+__device__ void cell_moments(double w, double cnt, const unsigned *mp,
+                             const unsigned *m1, const unsigned *m2,
+                             const double *epar, const double *e1,
+                             const double *e2, int npar, int n1, int n2,
+                             int three_d, int cenpar, int cenperp, double ms,
+                             double M[10]) {
+  for (int k = 0; k < 10; ++k) M[k] = 0.0;
+  const double NqRT = cnt * w;
+  double Nin = 0.0;
+  for (int k = 0; k < npar; ++k) Nin += (double)mp[k];
+  if (NqRT == 0.0 || Nin == 0.0) return;
+  const double M0 = w * Nin;
+  double Sp = 0.0, S1 = 0.0;
+  for (int k = 0; k < npar; ++k) Sp += 0.5 * (epar[k] + epar[k + 1]) * mp[k];
+  for (int k = 0; k < n1; ++k) S1 += 0.5 * (e1[k] + e1[k + 1]) * m1[k];
+  const double M1par = (w * Sp) / M0;
+  double Tp = 0.0, Tq = 0.0, T1 = 0.0, T1c = 0.0;
+  // centred integrand; for M2|| a bin whose centred value is exactly zero
+  // falls back to the uncentred one (_8_6_6_SecondParIonMoment.f90:90-99).
+  // The total-energy integrand also carries the Vperp terms, so it is never
+  // zero and keeps the centred value (Tq).
+  for (int k = 0; k < npar; ++k) {
+    if (!mp[k]) continue;
+    const double vc = 0.5 * (epar[k] + epar[k + 1]);
+    const double d = cenpar ? (vc - M1par) : vc;
+    double d2 = d * d;
+    Tq += d2 * mp[k];
+    if (d2 == 0.0) d2 = vc * vc;
+    Tp += d2 * mp[k];
+  }
+  const double M1p1 = (w * S1) / M0;
+  for (int k = 0; k < n1; ++k) {
+    if (!m1[k]) continue;
+    const double vc = 0.5 * (e1[k] + e1[k + 1]);
+    T1 += vc * vc * m1[k];
+    const double d = vc - M1p1;
+    double d2 = d * d;
+    if (d2 == 0.0) d2 = vc * vc;
+    T1c += d2 * m1[k];
+  }
+  M[KAOS_M0] = M0;
+  M[KAOS_M1PAR] = M1par;
+  M[KAOS_M2PAR] = (ms / 2.0) * ((w * Tp) / M0);
+  if (three_d) {
+    double S2 = 0.0, T2 = 0.0, T2c = 0.0;
+    for (int k = 0; k < n2; ++k) S2 += 0.5 * (e2[k] + e2[k + 1]) * m2[k];
+    const double M1p2 = (w * S2) / M0;
+    for (int k = 0; k < n2; ++k) {
+      if (!m2[k]) continue;
+      const double vc = 0.5 * (e2[k] + e2[k + 1]);
+      T2 += vc * vc * m2[k];
+      const double d = vc - M1p2;
+      double d2 = d * d;
+      if (d2 == 0.0) d2 = vc * vc;
+      T2c += d2 * m2[k];
+    }
+    M[KAOS_M1PERP1] = M1p1;
+    M[KAOS_M1PERP2] = M1p2;
+    M[KAOS_M2] = (ms / 2.0) * ((w * (T1 + T2 + Tq)) / M0);
+    M[KAOS_M2PERP1] = (ms / 2.0) * ((w * (cenperp ? T1c : T1)) / M0);
+    M[KAOS_M2PERP2] = (ms / 2.0) * ((w * (cenperp ? T2c : T2)) / M0);
+  } else {
+    M[KAOS_M1PERP] = M1p1;
+    M[KAOS_M2] = (ms / 2.0) * ((w * (T1 + Tq)) / M0);
+    M[KAOS_M2PERP] = (ms / 2.0) * ((w * (cenperp ? T1c : T1)) / M0);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Moments of one master step from the binning marginals (ZerothIonMoment ..
 // SecondParIonMoment _8_6_1-_8_6_6 with the NonUniform2D/3D integrators
 // _8_5_*), then the model-A collision counts (IonNeutralCollision

@@ -26,7 +26,7 @@ EXPORTS = [
     "kaos_set_export", "kaos_get_particles", "kaos_get_positions",
     "kaos_get_enas", "kaos_get_boundary", "kaos_get_timing", "kaos_set_graph",
     "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
-    "kaos_version", "kaos_get_push_timing",
+    "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
 ]
 
 _lib = None
@@ -60,6 +60,8 @@ def load(path: str = LIBPATH):
     L.kaos_get_boundary.argtypes = [vp, i32] + [C.POINTER(i64)] * 4
     L.kaos_get_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
     L.kaos_get_push_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
+    L.kaos_moments_noalloc.argtypes = [vp, vp, i32, vp, vp, C.c_double, vp, vp,
+                                        vp, vp, i64, vp, vp, vp]
     L.kaos_set_graph.argtypes = [vp, i32]
     L.kaos_set_launch.argtypes = [vp, i32, i32]
     L.kaos_last_error.argtypes = [vp]
