@@ -1,0 +1,40 @@
+"""DataExport2 layout: file names, raw stream contents, Fortran order of the
+phase-space arrays (_8_0_2_DataExport2.f90:29-800).  The CPU oracle stands in
+for the solver (same .moments / .counts surface)."""
+import os
+
+import numpy as np
+
+from kaos_b200 import export, grids
+from kaos_b200.model_input import KAOS_M0, KAOS_M1PAR
+from oracle.oracle import Oracle
+
+
+class _OracleAsSolver:
+    def __init__(self, o):
+        self.o = o
+
+    def moments(self, k, tube=0):
+        return self.o.moments(k)
+
+
+def test_export_layout_roundtrip(tmp_path):
+    mi, spec, tube, vg = grids.config_small(n_particles=1500, three_d=True, nq=10)
+    o = Oracle(mi, tube, vg)
+    o.load(*grids.initial_particles(tube, spec, mi, seed=4))
+    o.step(1)
+    hist = o.counts(full=True)
+    files = export.write_master_step(str(tmp_path), 1, _OracleAsSolver(o), 0, tube, vg,
+                                     True, 0.0, mi.ndatfac, hist=hist)
+    assert os.path.basename(files["M0phRT"]) == "1_1_1_M0phRTfort.bin"
+    assert os.path.basename(files["3_TeNT"]) == "1_1_1_3_TeNTfort.bin"
+    np.testing.assert_array_equal(export.read(files["M0phRT"]), o.moments(KAOS_M0))
+    np.testing.assert_array_equal(export.read(files["M1ParphRT"]), o.moments(KAOS_M1PAR))
+    assert export.read(files["ndatfacGT"], np.int64)[0] == mi.ndatfac
+    # N2PerpphRT(Vperp1, Vperp2, Vpar) in column-major order, density units
+    n1, n2, npar = vg.n1, vg.n2, vg.npar
+    k = 2
+    N = export.read(files[f"{k + 1}_N2PerpphRT"], shape=(n1, n2, npar))
+    ref = hist.reshape(tube.nq, n1, n2, npar)[k] * tube.nsnormfac / tube.d3xC[k]
+    np.testing.assert_allclose(N, ref, rtol=1e-15)
+    assert os.path.getsize(files[f"{k + 1}_d3vCTp"]) == 8 * n1 * n2 * npar

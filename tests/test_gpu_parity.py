@@ -146,3 +146,37 @@ def test_charge_exchange_and_ena_push(mixed):
         a, b = es[k][is_], eo[k][io]
         scale = max(np.max(np.abs(eo["z"])) if k in "xyz" else np.max(np.abs(eo["vz"])), 1.0)
         assert np.max(np.abs(a - b)) / scale < tol, k
+
+
+def test_batched_uneven_tubes_one_launch():
+    """Several tubes of different L-shell, cell count and particle count
+    advance together (one launch per kernel over a (tube, chunk) map); each
+    tube matches its own oracle run."""
+    from kaos_b200.grids import TubeSpec, make_tube, make_vgrid
+    from kaos_b200.model_input import ModelInput
+    mi = ModelInput(h=0.01, ndatfac=4, ION2VPERPflag=1, ICRflag=1)
+    vg = make_vgrid(True, 16, 16, 24, 8e3)
+    specs = [TubeSpec(L=3.0, nq=24, n_particles=1500, q_ub=0.2, H=500e3, heat_rate_eV_s=5.0),
+             TubeSpec(L=5.0, nq=40, n_particles=2500, q_ub=0.1, H=700e3, heat_rate_eV_s=1.0),
+             TubeSpec(L=7.0, nq=12, n_particles=700, q_ub=0.05, H=900e3, heat_rate_eV_s=0.0)]
+    tubes = [make_tube(sp, mi) for sp in specs]
+    for t in tubes:
+        t.nsnormCLB = 15.0
+    s = Solver(mi, tubes, vg)
+    inits = []
+    for k, (sp, t) in enumerate(zip(specs, tubes)):
+        init = grids.initial_particles(t, sp, mi, seed=100 + k)
+        inits.append(init)
+        s.load(k, *init)
+    s.step(10)
+    for k, (sp, t) in enumerate(zip(specs, tubes)):
+        o = Oracle(mi, t, vg)
+        o.load(*inits[k])
+        o.step(10)
+        po, ps = o.particles(), s.particles(k)
+        assert len(po["q"]) == len(ps["q"]), k
+        for key in ("z", "vpar", "vperp1"):
+            assert rel_norm(ps[key], po[key]) < TRAJ_TOL, (k, key)
+        np.testing.assert_array_equal(s.counts(k), o.counts())
+        a, b = s.moments(KAOS_M0, k), o.moments(KAOS_M0)
+        assert rel_norm(a, b) < MOM_TOL, k
