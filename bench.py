@@ -96,10 +96,25 @@ def bytes_per_particle_step(mixed, heating, collisions):
         if collisions:  # Qindk1 + q at k4 written for the charge exchange
             wr += 8
     else:      # rho, z, V||, Vperp1, Vperp2, AEA, AG (8 B) + Qindk1 (4 B)
-        rd, wr = 7 * 8, (5 if heating else 3) * 8 + 4
+        rd, wr = 7 * 8 + 4, (5 if heating else 3) * 8 + 4
         if collisions:  # q, rho, z at k4
             wr += 24
+    if heating:  # the 64-bit ion id keys the Philox stream of the kicks
+        rd += 8
     return rd + wr
+
+
+def profiled_traffic(name):
+    """DRAM bytes per ion-step of a push kernel from its committed ncu
+    summary (the `traffic_bytes_per_ion:` line), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_ion:"):
+                    return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
 
 
 def run_ours(args, precision, mi_tag):
@@ -276,13 +291,8 @@ def main():
         r32["solver"].close()
         e2e = run_e2e(args, KAOS_PREC_MIXED)
     cpu = cpu_baseline(args) if (rank == 0 and world == 1) else None
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "push_traffic.json")) as f:
-            tr = json.load(f)
-        traffic = tr.get("mixed_bytes_per_particle") * r32["n"]
-    except Exception:
-        pass
+    tpi = profiled_traffic("k_push32_mixed_c2.md")
+    traffic = None if tpi is None else tpi * r32["n"]
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s",
@@ -305,7 +315,9 @@ def main():
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "k_push32 (mixed push)",
-                         "bytes_per_particle": mixed_bytes},
+                         "bytes_per_particle": mixed_bytes,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           "per ion on a 6e6-ion launch, scaled to this launch"},
             "cpu_baseline": cpu,
             "e2e": None if e2e is None else {
                 "value": e2e["value"] * world, "unit": "particle-steps/s",

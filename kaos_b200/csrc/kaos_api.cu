@@ -23,7 +23,7 @@ using namespace kaos;
 namespace {
 
 constexpr int PUSH_THREADS = 256;
-constexpr int PUSH_ITEMS = 4;
+constexpr int PUSH_ITEMS = 8;
 constexpr int BC_THREADS = 256;
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0: closed form of the
