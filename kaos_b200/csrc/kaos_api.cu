@@ -25,6 +25,8 @@ namespace {
 constexpr int PUSH_THREADS = 256;
 constexpr int PUSH_ITEMS = 8;
 constexpr int BC_THREADS = 256;
+// a push block's ions lie in one charge-exchange selection chunk
+static_assert(CX_CHUNK % (PUSH_THREADS * PUSH_ITEMS) == 0, "chunk sizes");
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0: closed form of the
 // depressed resolvent cubic in hyperbolic form, then Newton polish.
@@ -102,6 +104,7 @@ struct kaos_handle {
   int *d_cx_tube = nullptr, *d_tube_cx0 = nullptr, *d_cxneed = nullptr;
   int64_t *d_cx_start = nullptr;
   unsigned *d_cxc = nullptr, *d_cxo = nullptr;
+  int *d_cxend = nullptr;
   int *d_cell_tube = nullptr, *d_cell_q = nullptr;  // global cell -> (tube, cell)
   int ncx = 0;
   int64_t n = 0;      // computational steps taken
@@ -161,6 +164,12 @@ bool is_master(const kaos_handle *h, int64_t n) {
   return n >= 2 && (n % h->P.ndatfac) == 0;
 }
 
+int max_nq(const kaos_handle *h) {
+  int m = 0;
+  for (auto &t : h->th) m = std::max(m, t.nq);
+  return m;
+}
+
 PushArgs push_args(kaos_handle *h) {
   PushArgs a{};
   a.tubes = h->d_tubes;
@@ -183,6 +192,10 @@ PushArgs push_args(kaos_handle *h) {
   a.icrcoh = h->P.ICRCOHERENCEflag == 1;
   a.status = h->d_status;
   a.exporting = h->export_on;
+  a.cxc = nullptr;  // set by the pushes whose Qindk1 feeds a selection
+  a.tube_cx0 = h->d_tube_cx0;
+  a.cx_stride = max_nq(h);
+  a.cx_chunk = CX_CHUNK;
   return a;
 }
 
@@ -220,12 +233,6 @@ TubeArgs tube_args(kaos_handle *h, uint32_t nn) {
   return a;
 }
 
-int max_nq(const kaos_handle *h) {
-  int m = 0;
-  for (auto &t : h->th) m = std::max(m, t.nq);
-  return m;
-}
-
 int launch_push(kaos_handle *h, const PushArgs &a) {
   const int nq = max_nq(h);
   if ((int)h->pev.size() < 2 * (h->npev + 1)) {
@@ -236,7 +243,7 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
     h->pev.push_back(e1);
   }
   CK(cudaEventRecord(h->pev[2 * h->npev], h->s));
-  size_t smem = (size_t)(2 * nq + 1) * sizeof(double);
+  size_t smem = (size_t)(2 * nq + 1) * sizeof(double) + (size_t)nq * sizeof(unsigned);
   if (h->mixed) smem += (size_t)5 * nq * sizeof(double) + (size_t)6 * nq * sizeof(float);
   if (h->mixed) {
     if (h->three_d) k_push32<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
@@ -354,6 +361,12 @@ int launch_inject(kaos_handle *h, int ub) {
   a.qs = h->P.qs;
   a.seed = h->P.seed;
   a.status = h->d_status;
+  if (h->P.QEXCHANGEflag == 1) {  // injected ions join the next selection
+    a.cxc = h->d_cxc;
+    a.tube_cx0 = h->d_tube_cx0;
+    a.cx_stride = max_nq(h);
+    a.cx_chunk = CX_CHUNK;
+  }
   k_inject<<<h->ntubes, 256, 0, h->s>>>(a);
   h->launches++;
   CK(cudaGetLastError());
@@ -374,6 +387,7 @@ CxArgs cx_args(kaos_handle *h) {
   a.cxc = h->d_cxc;
   a.cxo = h->d_cxo;
   a.cxneed = h->d_cxneed;
+  a.cxend = h->d_cxend;
   a.nqmax = max_nq(h);
   a.mixed = h->mixed;
   a.status = h->d_status;
@@ -384,11 +398,11 @@ CxArgs cx_args(kaos_handle *h) {
 int launch_cx(kaos_handle *h) {
   CxArgs a = cx_args(h);
   const int nq = max_nq(h);
-  k_cx_count<<<h->ncx, 256, (size_t)nq * sizeof(unsigned), h->s>>>(a);
+  // the per-chunk Qindk1 counts were accumulated by the previous push
   CK(cudaMemsetAsync(h->d_cxneed, 0, h->ncx * sizeof(int), h->s));
   k_cx_scan<<<(int)h->ncell, 256, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
   k_cx_convert<<<h->ncx, 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
-  h->launches += 3;
+  h->launches += 2;
   CK(cudaGetLastError());
   return KAOS_OK;
 }
@@ -477,6 +491,7 @@ int step_once(kaos_handle *h) {
     p.prologue = 1;  // interpolate at q0 (qk4 holds q0 after loading)
     p.write_qind = 1;
     p.write_qk4 = next_master || qx;
+    if (qx) p.cxc = h->d_cxc;
     if ((rc = launch_push(h, p))) return rc;
     h->n = n;
     return KAOS_OK;
@@ -496,6 +511,7 @@ int step_once(kaos_handle *h) {
   p.prologue = master;
   p.write_qind = (!h->mixed) || next_master || qx || h->export_on;
   p.write_qk4 = next_master || qx;
+  if (qx) p.cxc = h->d_cxc;
   if ((rc = launch_push(h, p))) return rc;
   if (qx && (rc = launch_push_ena(h))) return rc;
   if (master) {
@@ -765,6 +781,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
         (rc = dalloc(h, &h->d_eblkcnt, ebt.size())) || (rc = dalloc(h, &h->d_eblkoff, ebt.size())) ||
         (rc = dalloc(h, &h->d_lbe_out, ntubes)) || (rc = dalloc(h, &h->d_ube_out, ntubes)) ||
         (rc = dalloc(h, &h->d_cxneed, cxt.size())) ||
+        (rc = dalloc(h, &h->d_cxend, (size_t)h->ncell)) ||
         (rc = dalloc(h, &h->d_cxc, cxt.size() * (size_t)max_nq(h))) ||
         (rc = dalloc(h, &h->d_cxo, cxt.size() * (size_t)max_nq(h))))
       return rc;
@@ -852,6 +869,8 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
   uint64_t nid = (uint64_t)n;
   CK(cudaMemcpy(h->d_nlive + tube, &nl, sizeof(int64_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_next_id + tube, &nid, sizeof(uint64_t), cudaMemcpyHostToDevice));
+  if (h->d_cxc)  // the first push starts the selection counts from zero
+    CK(cudaMemset(h->d_cxc, 0, (size_t)h->ncx * max_nq(h) * sizeof(unsigned)));
   h->loaded = 1;
   return KAOS_OK;
 }

@@ -8,9 +8,10 @@
 // only (AGENA*sub _KineticMainParams.f90:695-714, KineticRK4UpdateSub
 // :186-193, :292-314).
 //
-// Selection on the GPU keeps the index order exactly: per-chunk counts of
-// eligible ions per cell, an exclusive scan over chunks per cell, then an
-// in-order walk of only those chunks that hold converted ions.
+// Selection on the GPU keeps the index order exactly: the push that writes
+// Qindk1 also counts, per selection chunk of CX_CHUNK ions, the ions of each
+// cell (flush_cx_counts); an exclusive scan over chunks per cell follows,
+// then an in-order walk of only those chunks that hold converted ions.
 #pragma once
 #include "kaos_push.cuh"
 
@@ -28,39 +29,25 @@ struct CxArgs {
   Ions ion;
   Enas ena;
   int64_t *nena;
-  unsigned *cxc;             // [chunk][nq_max] eligible counts
+  unsigned *cxc;             // [chunk][nq_max] Qindk1 counts (from the push)
   unsigned *cxo;             // [chunk][nq_max] exclusive prefix
   int *cxneed;               // chunk has conversions
+  int *cxend;                // per cell (all tubes): chunks >= cxend convert none
   int nqmax, mixed;
   uint32_t *status;
 };
 
-// per-chunk counts of ions per start-of-step cell
-__global__ void k_cx_count(CxArgs a) {
-  extern __shared__ unsigned hs[];
-  const int c = blockIdx.x;
-  const int t = a.cx_tube[c];
-  const TubeD &T = a.tubes[t];
-  for (int k = threadIdx.x; k < T.nq; k += blockDim.x) hs[k] = 0;
-  __syncthreads();
-  const int64_t nl = a.nlive[t];
-  const int64_t beg = a.cx_start[c], end = min(beg + (int64_t)CX_CHUNK, nl);
-  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
-    const int q = a.ion.qind[T.off + i];
-    if (q >= 0 && a.ct.nuPoi[T.coff + q] > 0.0) atomicAdd(&hs[q], 1u);
-  }
-  __syncthreads();
-  for (int k = threadIdx.x; k < T.nq; k += blockDim.x)
-    a.cxc[(int64_t)c * a.nqmax + k] = hs[k];
-}
-
 // exclusive scan over the chunks of a tube for one cell (one block per
 // (tube, cell) pair, block-wide scan); flags chunks holding ions to convert.
+// A cell with no conversion does nothing; the scan of a cell stops after the
+// tile of chunks in which its prefix reaches the conversion count, and
+// cxend records the first chunk without a written prefix.
 __global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
   const int t = cell_tube[blockIdx.x], k = cell_q[blockIdx.x];
   const TubeD &T = a.tubes[t];
   const double nu = a.ct.nuPoi[T.coff + k];
   const unsigned need = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
+  if (need == 0u) return;
   const int c0 = a.tube_cx0[t], c1 = a.tube_cx0[t + 1];
   __shared__ unsigned wsum[32];
   __shared__ unsigned base;
@@ -87,7 +74,12 @@ __global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
     __syncthreads();
     if (threadIdx.x == 0) base += tot;
     __syncthreads();
+    if (base >= need) {
+      if (threadIdx.x == 0) a.cxend[blockIdx.x] = min(r0 + (int)blockDim.x, c1);
+      return;
+    }
   }
+  if (threadIdx.x == 0) a.cxend[blockIdx.x] = c1;
 }
 
 // Cartesian unit vectors along B (par), across the shell (p) and in
@@ -104,12 +96,17 @@ __device__ __forceinline__ void dipole_frame(double ct, double st, double cp,
 }
 
 // in-order conversion of the first need[Q] eligible ions per cell
+// (every block also clears its chunk's count row for the next push)
 __global__ void k_cx_convert(CxArgs a) {
   const int c = blockIdx.x;
-  if (!a.cxneed[c]) return;
-  extern __shared__ unsigned sm_[];
   const int t = a.cx_tube[c];
   const TubeD &T = a.tubes[t];
+  unsigned *crow = a.cxc + (int64_t)c * a.nqmax;
+  if (!a.cxneed[c]) {
+    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) crow[k] = 0u;
+    return;
+  }
+  extern __shared__ unsigned sm_[];
   unsigned *need = sm_;                 // remaining conversions per cell
   unsigned *wcnt = sm_ + a.nqmax;       // [8 warps][nq] per-tile counts
   __shared__ unsigned remaining;
@@ -117,9 +114,11 @@ __global__ void k_cx_convert(CxArgs a) {
   __syncthreads();
   for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
     const double nu = a.ct.nuPoi[T.coff + k];
-    const unsigned nd = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
-    const unsigned o = a.cxo[(int64_t)c * a.nqmax + k];
-    const unsigned cnt = a.cxc[(int64_t)c * a.nqmax + k];
+    unsigned nd = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
+    if (nd && c >= a.cxend[T.coff + k]) nd = 0u;  // prefix >= need
+    const unsigned o = nd ? a.cxo[(int64_t)c * a.nqmax + k] : 0u;
+    const unsigned cnt = crow[k];
+    crow[k] = 0u;
     need[k] = nd > o ? nd - o : 0u;
     // conversions that can happen in this chunk
     const unsigned here = need[k] < cnt ? need[k] : cnt;
@@ -268,13 +267,14 @@ __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
   extern __shared__ double sm[];
   const int t = a.blk_tube[blockIdx.x];
   const TubeD &T = a.tubes[t];
+  const int64_t nl = min(a.nena[t], T.ecap);
+  const int64_t beg = a.blk_start[blockIdx.x];
+  if (beg >= nl) return;  // whole block idle: before any barrier
+  const int64_t end = min(beg + (int64_t)a.chunk, nl);
   double *E = sm;
   for (int k = threadIdx.x; k <= T.nq; k += blockDim.x)
     E[k] = (k < T.nq) ? T.sgn * a.ct.qGL[T.coff + k] : T.sgn * a.ct.qGH[T.coff + T.nq - 1];
   __syncthreads();
-  const int64_t nl = min(a.nena[t], T.ecap);
-  const int64_t beg = a.blk_start[blockIdx.x];
-  const int64_t end = min(beg + (int64_t)a.chunk, nl);
   const double h = a.h, hh = 0.5 * h, h6 = h / 6.0, hsq2 = 0.5 * h * h;
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t e = T.eoff + i;

@@ -37,7 +37,22 @@ struct PushArgs {
   int exporting;  // also fill the full phase-space histogram
   int bin_only;   // count only, do not advance (first step statistics)
   uint32_t *status;
+  // charge exchange on: per (selection chunk, cell) counts of the Qindk1
+  // written by this push, for the next step's in-order selection
+  unsigned *cxc;
+  const int *tube_cx0;
+  int cx_stride, cx_chunk;
 };
+
+// Flush a block's per-cell Qindk1 counts into its selection-chunk row.
+__device__ __forceinline__ void flush_cx_counts(const PushArgs &a, int t,
+                                                int64_t beg, int nq,
+                                                const unsigned *HC) {
+  __syncthreads();
+  unsigned *row = a.cxc + (int64_t)(a.tube_cx0[t] + (int)(beg / a.cx_chunk)) * a.cx_stride;
+  for (int k = threadIdx.x; k < nq; k += blockDim.x)
+    if (HC[k]) atomicAdd(row + k, HC[k]);
+}
 
 // ---- warp-aggregated counter increment -----------------------------------
 __device__ __forceinline__ void agg_inc(unsigned int *base, int64_t idx) {
@@ -282,7 +297,10 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   TubeD T;
   const int nqmax = a.tubes[t].nq;
   double *E = sm, *Cc = sm + nqmax + 1;
+  unsigned *HC = (unsigned *)(Cc + nqmax);
   load_tube_smem(a, t, T, E, Cc);
+  if (a.cxc)
+    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
   __syncthreads();
   const int64_t nl = a.nlive[t];
   const int64_t beg = a.blk_start[blockIdx.x];
@@ -388,7 +406,9 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
       I.ag[j] = ag;
     }
     if (a.write_qind) I.qind[j] = qi;
+    if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);
   }
+  if (a.cxc) flush_cx_counts(a, t, beg, T.nq, HC);
 }
 
 // ---------------------------------------------------------------------------
@@ -405,7 +425,10 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
   double *UL = Cc + nqmax, *UD = UL + nqmax, *QL = UD + nqmax, *IDQ = QL + nqmax,
          *DQ = IDQ + nqmax;
   float *HK = (float *)(DQ + nqmax);  // 6 floats per cell: K1 K2 c1 c2 iom0 lam
+  unsigned *HC = (unsigned *)(HK + 6 * nqmax);
   load_tube_smem(a, t, T, E, Cc);
+  if (a.cxc)
+    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
   for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
     const int64_t g = T.coff + k;
     const double ql = a.ct.qGL[g], qh = a.ct.qGH[g];
@@ -434,14 +457,32 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
   const double ipG = 1.0 / T.pG;
   const float fRE = (float)RE;
   Ions I = a.ion;
+  // Software pipeline: the state of the next ion of this thread is loaded
+  // before the current one is pushed, so its HBM latency overlaps the work.
+  int n_c = DEAD;
+  float n_o = 0.f, n_vp = 0.f, n_v1 = 0.f, n_v2 = 0.f, n_ea = 0.f, n_ag = 0.f;
+  uint64_t n_id = 0;
+  if (beg + threadIdx.x < end) {
+    const int64_t j = T.off + beg + threadIdx.x;
+    n_c = I.cell[j]; n_o = I.off[j]; n_vp = I.fvpar[j]; n_v1 = I.fv1[j];
+    n_v2 = I.fv2[j]; n_ea = I.faea[j]; n_ag = I.fag[j];
+    if (a.icr) n_id = I.id[j];
+  }
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t j = T.off + i;
-    const int c0 = I.cell[j];
+    const int c0 = n_c;
+    const float o0 = n_o;
+    const float vpar = n_vp;
+    float v1 = n_v1, v2 = n_v2;
+    float aea = n_ea, ag = n_ag;
+    const uint64_t pid = n_id;
+    if (i + blockDim.x < end) {
+      const int64_t jn = j + blockDim.x;
+      n_c = I.cell[jn]; n_o = I.off[jn]; n_vp = I.fvpar[jn]; n_v1 = I.fv1[jn];
+      n_v2 = I.fv2[jn]; n_ea = I.faea[jn]; n_ag = I.fag[jn];
+      if (a.icr) n_id = I.id[jn];
+    }
     if (c0 == DEAD) continue;
-    const float o0 = I.off[j];
-    const float vpar = I.fvpar[j];
-    float v1 = I.fv1[j], v2 = I.fv2[j];
-    float aea = I.faea[j], ag = I.fag[j];
     if (a.prologue) {
       double da = aea, dg = ag;
       field_prologue(a, T, E, Cc, (double)I.fqk4[j], da, dg);
@@ -499,7 +540,7 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
       const float invOm = c_invOm * (rf * rf * rf) * g1.isl;
       const float *hk = HK + 6 * qi;
       const HeatC<float> hc{hk[0], hk[1], hk[2], hk[3], hk[4], hk[5]};
-      heat<float>(a, hc, I.id[j], invsumds, Om, invOm, fabsf(vpar), v1n, v2n);
+      heat<float>(a, hc, pid, invsumds, Om, invOm, fabsf(vpar), v1n, v2n);
     }
     const float rf = (float)rho0, zf = (float)z0;
     const float VRr = vpar * g1.er, VRz = vpar * g1.ez;
@@ -541,7 +582,9 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
       I.fag[j] = ag;
     }
     if (a.write_qind) I.qind[j] = qi;
+    if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);
   }
+  if (a.cxc) flush_cx_counts(a, t, beg, T.nq, HC);
 }
 
 }  // namespace kaos

@@ -483,6 +483,9 @@ struct InjArgs {
   double ms, qs;
   uint64_t seed;
   uint32_t *status;
+  unsigned *cxc;             // charge exchange on: selection-chunk counts
+  const int *tube_cx0;
+  int cx_stride, cx_chunk;
 };
 
 __global__ void k_inject(InjArgs a) {
@@ -543,6 +546,8 @@ __global__ void k_inject(InjArgs a) {
     }
     a.ion.qind[j] = Q;
     a.ion.id[j] = id;
+    if (a.cxc)
+      agg_inc(a.cxc, (int64_t)(a.tube_cx0[t] + (int)((nl + i) / a.cx_chunk)) * a.cx_stride + Q);
     if (a.bin) accumulate(a.acc, T, Q, b1, d3 ? b2 : 0, bp, a.exporting);
   }
   __syncthreads();
