@@ -80,11 +80,12 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def build_workload(precision, n_part=N_PART, heating=True, collisions=False):
+def build_workload(precision, n_part=N_PART, heating=True, collisions=False,
+                   ndatfac=50):
     from kaos_b200 import grids
     mi, spec, tube, vg = grids.config_c2(n_particles=n_part, heating=heating,
                                          collisions=collisions,
-                                         precision=precision)
+                                         precision=precision, ndatfac=ndatfac)
     q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=20261203)
     return mi, spec, tube, vg, (q, vpar, v1, v2)
 
@@ -117,30 +118,48 @@ def profiled_traffic(name):
     return None
 
 
-def run_ours(args, precision, mi_tag):
+def run_ours(args, precision, graph=False, ndatfac=50, steps=None):
     from kaos_b200 import build as kbuild
     from kaos_b200.lib import Solver
     kbuild.build()
+    steps = args.steps if steps is None else steps
     mi, spec, tube, vg, init = build_workload(precision, args.particles,
                                               heating=not args.no_heating,
-                                              collisions=args.collisions)
+                                              collisions=args.collisions,
+                                              ndatfac=ndatfac)
     s = Solver(mi, [tube], vg)
     t0 = time.perf_counter()
     s.load(0, *init)
     t_load = time.perf_counter() - t0
+    s.set_graph(graph)
     s.step(args.warmup)
     n0, _ = s.count()
     # --- device-timed region: K steps in one call (CUDA events on the
     # library's stream; inputs 0.5-1 GB > L2, so no explicit flush) --------
-    s.step(args.steps)
+    s.step(steps)
     ms, launches = s.timing()
     pms, pl = s.push_timing()  # events around each push launch
     n1, _ = s.count()
     nmean = 0.5 * (n0 + n1)
-    value = nmean * args.steps / (ms * 1e-3)
+    value = nmean * steps / (ms * 1e-3)
     push_ms = pms / max(pl, 1)
     return dict(value=value, ms=ms, launches=launches, n=nmean, push_ms=push_ms,
                 t_load=t_load, solver=s, init=init, tube=tube, mi=mi)
+
+
+def mixed_moment_error(s32, s64):
+    """Norm-wise relative difference max|m32 - m64| / max|m64| per moment."""
+    from kaos_b200 import model_input as M
+    names = {"M0": M.KAOS_M0, "M1par": M.KAOS_M1PAR, "M1perp1": M.KAOS_M1PERP1,
+             "M1perp2": M.KAOS_M1PERP2, "M2": M.KAOS_M2, "M2par": M.KAOS_M2PAR,
+             "M2perp1": M.KAOS_M2PERP1, "M2perp2": M.KAOS_M2PERP2, "Nq": M.KAOS_NQ,
+             "EAmag": M.KAOS_EAMAG, "nuPoi": M.KAOS_NUPOI}
+    out = {}
+    for k, m in names.items():
+        a, b = s32.moments(m), s64.moments(m)
+        scale = float(np.max(np.abs(b)))
+        out[k] = float(np.max(np.abs(a - b)) / scale) if scale > 0 else 0.0
+    return out
 
 
 def run_e2e(args, precision):
@@ -196,42 +215,68 @@ def cpu_baseline(args, sample_particles=20000, sample_steps=5):
                        "(oracle, direct binning, 1 thread)")
 
 
-def reference_arm(args):
-    """--impl reference: the CPU restatement of the reference loop (the
-    reference itself is Fortran+MPI and cannot be built in this image) on
-    the host cores, bounded sample per step."""
+def _reference_worker(job, barrier, out):
+    """One host core: the oracle on its own seeded sample of the workload;
+    all workers start their timed steps together."""
+    seed, npart, warmup, steps, heating, collisions = job
     from oracle.oracle import Oracle
     from kaos_b200 import grids
     from kaos_b200.model_input import KAOS_PREC_FP64
+    mi, spec, tube, vg = grids.config_c2(n_particles=npart, heating=heating,
+                                         collisions=collisions,
+                                         precision=KAOS_PREC_FP64)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=seed)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    o.step(warmup)
+    n0, _ = o.count()
+    barrier.wait()
+    t0 = time.time()
+    o.step(steps)
+    t1 = time.time()
+    n1, _ = o.count()
+    out.put((0.5 * (n0 + n1) * steps, t0, t1))
+
+
+def reference_arm(args):
+    """--impl reference: the CPU restatement of the reference loop (the
+    reference itself is Fortran+MPI and cannot be built in this image) on
+    every host core: one process per core, each advancing its own bounded
+    sample of the workload; throughput = all particle-steps / the span from
+    the first start to the last end."""
+    import multiprocessing as mp
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
     npart = 20000
-    mi, spec, tube, vg = grids.config_c2(n_particles=npart,
-                                         heating=not args.no_heating,
-                                         collisions=args.collisions,
-                                         precision=KAOS_PREC_FP64)
-    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=20261203)
-    o = Oracle(mi, tube, vg)
-    o.load(q, vpar, v1, v2)
-    o.step(args.warmup)
-    t0 = time.perf_counter()
-    o.step(args.steps)
-    dt = time.perf_counter() - t0
-    n, _ = o.count()
-    v = n * args.steps / dt
+    cores = len(os.sched_getaffinity(0))
+    jobs = [(20261203 + k, npart, args.warmup, args.steps, not args.no_heating,
+             args.collisions) for k in range(cores)]
+    ctx = mp.get_context("spawn")
+    barrier, out = ctx.Barrier(cores), ctx.Queue()
+    procs = [ctx.Process(target=_reference_worker, args=(j, barrier, out)) for j in jobs]
+    for p in procs:
+        p.start()
+    res = [out.get(timeout=900) for _ in procs]
+    for p in procs:
+        p.join()
+    work = sum(r[0] for r in res)
+    span = max(r[2] for r in res) - min(r[1] for r in res)
+    v = work / span
     return {
         "impl": "reference", "metric": METRIC, "value": v,
         "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * span / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"precision A/B tube, L=4, 256 cells, 48x48x64, "
-                               f"{npart} O+ sample (of 1e7), heating on, dt 5 ms"},
-        "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": 1,
+                               f"{cores} x {npart} O+ samples (of 1e7), heating "
+                               f"{'off' if args.no_heating else 'on'}, collisions "
+                               f"{'on' if args.collisions else 'off'}, dt 5 ms"},
+        "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores,
                          "kind": "port",
-                         "sample": f"{n} O+ x {args.steps} steps per run, oracle FP64, "
-                                   "direct binning, 1 thread"},
+                         "sample": f"{cores} processes x {npart} O+ x {args.steps} steps, "
+                                   "oracle FP64, direct binning"},
         "e2e": {"value": v, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -265,8 +310,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from kaos_b200.model_input import KAOS_PREC_FP64, KAOS_PREC_MIXED
     # FP64 path first (reported beside the headline)
-    r64 = run_ours(args, KAOS_PREC_FP64, "fp64")
-    r64["solver"].close()
+    r64 = run_ours(args, KAOS_PREC_FP64)
     stop = threading.Event()
     samples = []
     th = threading.Thread(target=clocks_sampler, args=(stop, samples), daemon=True)
@@ -274,9 +318,21 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     th.start()
-    r32 = run_ours(args, KAOS_PREC_MIXED, "mixed")
+    r32 = run_ours(args, KAOS_PREC_MIXED)
     torch.cuda.synchronize()
     stop.set()
+    # error of every moment of the mixed path against the FP64 path (same
+    # particles, same random streams, last master step)
+    moment_error = mixed_moment_error(r32["solver"], r64["solver"])
+    r64["solver"].close()
+    r32["solver"].close()
+    # the same steps replayed from CUDA graphs, and at cadence 1 (every step
+    # a master step: removal/injection, fields, counts and moments each step)
+    rg = run_ours(args, KAOS_PREC_MIXED, graph=True)
+    rg["solver"].close()
+    rc1 = run_ours(args, KAOS_PREC_MIXED, graph=True, ndatfac=1,
+                   steps=min(args.steps, 50))
+    rc1["solver"].close()
     ms = r32["ms"]
     if dist is not None:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -288,7 +344,6 @@ def main():
     peak, peak_kind = peaks()
     e2e = None
     if not args.skip_e2e:
-        r32["solver"].close()
         e2e = run_e2e(args, KAOS_PREC_MIXED)
     cpu = cpu_baseline(args) if (rank == 0 and world == 1) else None
     tpi = profiled_traffic("k_push32_mixed_c2.md")
@@ -311,6 +366,14 @@ def main():
             "fp64": {"value": r64["value"] * world, "ms_per_step": r64["ms"] / args.steps,
                      "push_ms": r64["push_ms"]},
             "mixed_over_fp64": value / (r64["value"] * world),
+            "mixed_push_ms": r32["push_ms"],
+            "moment_error_vs_fp64": moment_error,
+            "graph": {"value": rg["value"] * world, "ms_per_step": rg["ms"] / args.steps,
+                      "note": "mixed path, steps replayed from CUDA graphs"},
+            "cadence1": {"value": rc1["value"] * world,
+                         "ms_per_step": rc1["ms"] / min(args.steps, 50),
+                         "steps": min(args.steps, 50),
+                         "note": "mixed path, every step a master step, CUDA graphs"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,

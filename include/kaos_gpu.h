@@ -226,11 +226,19 @@ int kaos_get_boundary(kaos_handle *h, int32_t tube, int64_t *lb_out,
 int kaos_get_timing(kaos_handle *h, double *ms, int64_t *launches);
 
 /* Device time (ms) spent in the particle push kernels alone during the last
- * kaos_step call (CUDA events around each push launch) and their count. */
+ * kaos_step call (CUDA events around each push launch) and their count.
+ * Steps replayed from CUDA graphs carry no per-push events and are not
+ * included. */
 int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches);
 
-/* Record the whole computational step in CUDA graphs (1) or launch the
- * kernels directly (0, default). */
+/* Run the computational steps from CUDA graphs (1) or launch every kernel
+ * directly (0, default).  With graphs on, each kind of step (ordinary runs
+ * of up to 8 steps, the step before a master step, the master step) is
+ * captured once per ion/ENA buffer parity and replayed; the step number
+ * lives in device memory, so a replay needs no host update.  Results are
+ * identical to the direct launches.  Step 1 always runs directly.  No
+ * reference counterpart (the Fortran loop calls each routine per step,
+ * _8_KineticSolver.f90:54-239). */
 int kaos_set_graph(kaos_handle *h, int32_t on);
 
 /* Block shape for the push kernel (threads per block; 0 = autotuned). */

@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -101,7 +102,9 @@ struct kaos_handle {
   int64_t *d_eblk_start = nullptr, *d_eblkcnt = nullptr, *d_eblkoff = nullptr;
   int neblk = 0;
   unsigned long long *d_lbe_out = nullptr, *d_ube_out = nullptr;
-  int *d_cx_tube = nullptr, *d_tube_cx0 = nullptr, *d_cxneed = nullptr;
+  int *d_cx_tube = nullptr, *d_tube_cx0 = nullptr;
+  unsigned *d_cxconv = nullptr;
+  int64_t *d_cxbase = nullptr;
   int64_t *d_cx_start = nullptr;
   unsigned *d_cxc = nullptr, *d_cxo = nullptr;
   int *d_cxend = nullptr;
@@ -112,6 +115,16 @@ struct kaos_handle {
   int have_import = 0;
   int loaded = 0;
   int graph = 0;
+  // CUDA graphs of whole steps: kernels replayed from a graph read the step
+  // number from d_step (advanced by the first kernel of every step)
+  uint32_t *d_step = nullptr;
+  int capturing = 0;
+  int dstep_valid = 0;
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;
+  };
+  std::map<uint64_t, StepGraph> graphs;
   double last_ms = 0.0;
   int64_t launches = 0;
   std::vector<cudaEvent_t> pev;  // event pairs around push launches
@@ -196,6 +209,7 @@ PushArgs push_args(kaos_handle *h) {
   a.tube_cx0 = h->d_tube_cx0;
   a.cx_stride = max_nq(h);
   a.cx_chunk = CX_CHUNK;
+  a.dstep = h->capturing ? h->d_step : nullptr;
   return a;
 }
 
@@ -215,6 +229,8 @@ TubeArgs tube_args(kaos_handle *h, uint32_t nn) {
   a.dNTeEND = h->P.dNTeEND;
   a.seed = h->P.seed;
   a.nn = nn;
+  a.dstep = h->capturing ? h->d_step : nullptr;
+  a.ndatfac = h->P.ndatfac;
   a.three_d = h->three_d;
   a.eamb = h->P.EAMBflag == 1;
   a.grav = h->P.GRAVflag == 1;
@@ -235,14 +251,15 @@ TubeArgs tube_args(kaos_handle *h, uint32_t nn) {
 
 int launch_push(kaos_handle *h, const PushArgs &a) {
   const int nq = max_nq(h);
-  if ((int)h->pev.size() < 2 * (h->npev + 1)) {
+  const bool timed = !h->capturing;  // no per-push events inside a graph
+  if (timed && (int)h->pev.size() < 2 * (h->npev + 1)) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     h->pev.push_back(e0);
     h->pev.push_back(e1);
   }
-  CK(cudaEventRecord(h->pev[2 * h->npev], h->s));
+  if (timed) CK(cudaEventRecord(h->pev[2 * h->npev], h->s));
   size_t smem = (size_t)(2 * nq + 1) * sizeof(double) + (size_t)nq * sizeof(unsigned);
   if (h->mixed) smem += (size_t)5 * nq * sizeof(double) + (size_t)6 * nq * sizeof(float);
   if (h->mixed) {
@@ -252,8 +269,10 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
     if (h->three_d) k_push64<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
     else k_push64<false><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
   }
-  CK(cudaEventRecord(h->pev[2 * h->npev + 1], h->s));
-  h->npev++;
+  if (timed) {
+    CK(cudaEventRecord(h->pev[2 * h->npev + 1], h->s));
+    h->npev++;
+  }
   h->launches++;
   CK(cudaGetLastError());
   return KAOS_OK;
@@ -273,9 +292,15 @@ int zero_accum(kaos_handle *h) {
 
 int launch_moments(kaos_handle *h, uint32_t nn) {
   TubeArgs ta = tube_args(h, nn);
-  size_t smem = (size_t)8 * max_nq(h) * sizeof(double);
-  k_moments<<<h->ntubes, 256, smem, h->s>>>(ta);
+  const int cells_per_block = 256 / 32;
+  k_cell_moments<<<(int)((h->ncell + cells_per_block - 1) / cells_per_block), 256, 0, h->s>>>(
+      ta, h->d_cell_tube);
   h->launches++;
+  if (ta.qexchange) {
+    size_t smem = (size_t)8 * max_nq(h) * sizeof(double);
+    k_collision_counts<<<h->ntubes, 256, smem, h->s>>>(ta);
+    h->launches++;
+  }
   CK(cudaGetLastError());
   return KAOS_OK;
 }
@@ -386,7 +411,8 @@ CxArgs cx_args(kaos_handle *h) {
   a.nena = h->d_nena;
   a.cxc = h->d_cxc;
   a.cxo = h->d_cxo;
-  a.cxneed = h->d_cxneed;
+  a.cxconv = h->d_cxconv;
+  a.cxbase = h->d_cxbase;
   a.cxend = h->d_cxend;
   a.nqmax = max_nq(h);
   a.mixed = h->mixed;
@@ -399,10 +425,10 @@ int launch_cx(kaos_handle *h) {
   CxArgs a = cx_args(h);
   const int nq = max_nq(h);
   // the per-chunk Qindk1 counts were accumulated by the previous push
-  CK(cudaMemsetAsync(h->d_cxneed, 0, h->ncx * sizeof(int), h->s));
   k_cx_scan<<<(int)h->ncell, 256, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
+  k_cx_base<<<h->ntubes, 256, 0, h->s>>>(a);
   k_cx_convert<<<h->ncx, 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
-  h->launches += 2;
+  h->launches += 3;
   CK(cudaGetLastError());
   return KAOS_OK;
 }
@@ -462,12 +488,19 @@ int launch_boundary_ena(kaos_handle *h) {
   return KAOS_OK;
 }
 
+__global__ void k_set_step(uint32_t *d, uint32_t v) { *d = v; }
+__global__ void k_next_step(uint32_t *d) { *d += 1u; }
+
 // One computational step n = h->n + 1.
 int step_once(kaos_handle *h) {
   const int64_t n = h->n + 1;
   const bool next_master = is_master(h, n + 1);
   const bool qx = h->P.QEXCHANGEflag == 1;
   int rc;
+  if (h->capturing) {  // d_step: n - 1 -> n for the kernels of this step
+    k_next_step<<<1, 1, 0, h->s>>>(h->d_step);
+    h->launches++;
+  }
   if (n == 1) {
     // KineticSolverASub: statistics of the initial state, fields, push.
     if ((rc = zero_accum(h))) return rc;
@@ -522,6 +555,65 @@ int step_once(kaos_handle *h) {
   h->n = n;
   return KAOS_OK;
 }
+
+// Steps of one kind replayed from a cached CUDA graph.  A graph holds g
+// consecutive steps that share their launch sequence; its key is what the
+// sequence depends on: g, master / next-master step, the current ion and ENA
+// buffers (the compaction alternates them) and the export switch.  The first
+// use captures the steps (which advances the host state as an eager step
+// does); a replay applies the same host-side transitions.
+int graph_steps(kaos_handle *h, int g) {
+  const int64_t n = h->n + 1;
+  const uint64_t key = (uint64_t)g | ((uint64_t)is_master(h, n) << 16) |
+                       ((uint64_t)is_master(h, n + 1) << 17) |
+                       ((uint64_t)h->cur << 18) | ((uint64_t)h->ecur << 19) |
+                       ((uint64_t)(h->export_on != 0) << 20);
+  if (!h->dstep_valid) {
+    k_set_step<<<1, 1, 0, h->s>>>(h->d_step, (uint32_t)h->n);
+    h->launches++;
+    CK(cudaGetLastError());
+    h->dstep_valid = 1;
+  }
+  auto it = h->graphs.find(key);
+  if (it != h->graphs.end()) {
+    CK(cudaGraphLaunch(it->second.exec, h->s));
+    h->launches += it->second.launches;
+    for (int k = 0; k < g; ++k) {
+      const int64_t m = h->n + 1;
+      if (is_master(h, m)) {  // launch_boundary / launch_boundary_ena swaps
+        h->cur = 1 - h->cur;
+        if (h->P.QEXCHANGEflag == 1) h->ecur = 1 - h->ecur;
+      }
+      h->n = m;
+    }
+    return KAOS_OK;
+  }
+  kaos_handle::StepGraph sg;
+  const int64_t l0 = h->launches;
+  CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+  h->capturing = 1;
+  int rc = KAOS_OK;
+  for (int k = 0; k < g && rc == KAOS_OK; ++k) rc = step_once(h);
+  h->capturing = 0;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(h->s, &graph);
+  if (rc != KAOS_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ce != cudaSuccess)
+    return fail(h, KAOS_ERR_CUDA, "step capture: %s", cudaGetErrorString(ce));
+  const cudaError_t ie = cudaGraphInstantiate(&sg.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess)
+    return fail(h, KAOS_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+  sg.launches = h->launches - l0;
+  h->graphs[key] = sg;
+  CK(cudaGraphLaunch(sg.exec, h->s));
+  return KAOS_OK;
+}
+
+constexpr int GRAPH_RUN = 8;  // ordinary steps per replayed graph
 
 }  // namespace
 
@@ -696,6 +788,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   if ((rc = dalloc(h, &h->d_lb_in, ntubes))) return rc;
   if ((rc = dalloc(h, &h->d_ub_in, ntubes))) return rc;
   if ((rc = dalloc(h, &h->d_status, 1))) return rc;
+  if ((rc = dalloc(h, &h->d_step, 1))) return rc;
   // particle arrays (two buffer sets for the order-preserving compaction)
   const int64_t cap = poff;
   for (int b = 0; b < 2; ++b) {
@@ -726,6 +819,16 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     if ((rc = dalloc(h, &I.qind, cap))) return rc;
     if (!h->three_d && (rc = dalloc(h, &I.vb, cap))) return rc;
     if ((rc = dalloc(h, &I.id, cap))) return rc;
+  }
+  // global cell -> (tube, cell) map
+  {
+    std::vector<int> ctb, cq;
+    for (int t = 0; t < ntubes; ++t)
+      for (int k = 0; k < h->th[t].nq; ++k) { ctb.push_back(t); cq.push_back(k); }
+    if ((rc = dalloc(h, &h->d_cell_tube, ctb.size())) || (rc = dalloc(h, &h->d_cell_q, cq.size())))
+      return rc;
+    CK(cudaMemcpy(h->d_cell_tube, ctb.data(), ctb.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_cell_q, cq.data(), cq.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
   // ENA arrays, block map and charge-exchange chunk map
   if (p->QEXCHANGEflag == 1) {
@@ -769,10 +872,6 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
         r = fail(h, KAOS_ERR_CUDA, "upload failed");
       return r;
     };
-    std::vector<int> ctb, cq;
-    for (int t = 0; t < ntubes; ++t)
-      for (int k = 0; k < h->th[t].nq; ++k) { ctb.push_back(t); cq.push_back(k); }
-    if ((rc = up_i(&h->d_cell_tube, ctb)) || (rc = up_i(&h->d_cell_q, cq))) return rc;
     if ((rc = up_i(&h->d_eblk_tube, ebt)) || (rc = up_l(&h->d_eblk_start, ebs)) ||
         (rc = up_i(&h->d_tube_eblk0, te0)) || (rc = up_i(&h->d_cx_tube, cxt)) ||
         (rc = up_l(&h->d_cx_start, cxs)) || (rc = up_i(&h->d_tube_cx0, tc0)))
@@ -780,7 +879,8 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     if ((rc = dalloc(h, &h->d_nena, ntubes)) || (rc = dalloc(h, &h->d_nena_new, ntubes)) ||
         (rc = dalloc(h, &h->d_eblkcnt, ebt.size())) || (rc = dalloc(h, &h->d_eblkoff, ebt.size())) ||
         (rc = dalloc(h, &h->d_lbe_out, ntubes)) || (rc = dalloc(h, &h->d_ube_out, ntubes)) ||
-        (rc = dalloc(h, &h->d_cxneed, cxt.size())) ||
+        (rc = dalloc(h, &h->d_cxconv, cxt.size())) ||
+        (rc = dalloc(h, &h->d_cxbase, cxt.size())) ||
         (rc = dalloc(h, &h->d_cxend, (size_t)h->ncell)) ||
         (rc = dalloc(h, &h->d_cxc, cxt.size() * (size_t)max_nq(h))) ||
         (rc = dalloc(h, &h->d_cxo, cxt.size() * (size_t)max_nq(h))))
@@ -920,9 +1020,22 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
   h->launches = 0;
   h->npev = 0;
   CK(cudaEventRecord(h->e0, h->s));
-  for (int64_t k = 0; k < nsteps; ++k) {
-    int rc = step_once(h);
-    if (rc) return rc;
+  for (int64_t k = 0; k < nsteps;) {
+    const int64_t n = h->n + 1;
+    int rc;
+    if (!h->graph || n == 1) {
+      if ((rc = step_once(h))) return rc;
+      h->dstep_valid = 0;
+      ++k;
+      continue;
+    }
+    int g = 1;  // a run of ordinary steps (neither master nor next-master)
+    if (!is_master(h, n) && !is_master(h, n + 1))
+      while (g < GRAPH_RUN && k + g < nsteps && !is_master(h, n + g) &&
+             !is_master(h, n + g + 1))
+        ++g;
+    if ((rc = graph_steps(h, g))) return rc;
+    k += g;
   }
   CK(cudaEventRecord(h->e1, h->s));
   CK(cudaEventSynchronize(h->e1));
@@ -1151,6 +1264,7 @@ int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches) {
 void kaos_destroy(kaos_handle *h) {
   if (!h) return;
   if (h->s) cudaStreamSynchronize(h->s);
+  for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
   for (auto e : h->pev) cudaEventDestroy(e);
   for (void *p : h->allocs) cudaFree(p);
   if (h->e0) cudaEventDestroy(h->e0);

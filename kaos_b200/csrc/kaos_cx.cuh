@@ -31,14 +31,16 @@ struct CxArgs {
   int64_t *nena;
   unsigned *cxc;             // [chunk][nq_max] Qindk1 counts (from the push)
   unsigned *cxo;             // [chunk][nq_max] exclusive prefix
-  int *cxneed;               // chunk has conversions
+  unsigned *cxconv;          // per chunk: ions converted in it this step
+  int64_t *cxbase;           // per chunk: ENA slot of its first conversion
   int *cxend;                // per cell (all tubes): chunks >= cxend convert none
   int nqmax, mixed;
   uint32_t *status;
 };
 
 // exclusive scan over the chunks of a tube for one cell (one block per
-// (tube, cell) pair, block-wide scan); flags chunks holding ions to convert.
+// (tube, cell) pair, block-wide scan); adds the conversions of this cell to
+// the per-chunk totals.
 // A cell with no conversion does nothing; the scan of a cell stops after the
 // tile of chunks in which its prefix reaches the conversion count, and
 // cxend records the first chunk without a written prefix.
@@ -69,7 +71,7 @@ __global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
     const unsigned s = base + woff + x - n;  // exclusive prefix
     if (c < c1) {
       a.cxo[(int64_t)c * a.nqmax + k] = s;
-      if (n && s < need) a.cxneed[c] = 1;
+      if (n && s < need) atomicAdd(&a.cxconv[c], min(n, need - s));
     }
     __syncthreads();
     if (threadIdx.x == 0) base += tot;
@@ -80,6 +82,38 @@ __global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
     }
   }
   if (threadIdx.x == 0) a.cxend[blockIdx.x] = c1;
+}
+
+// ENA slots in ion-index order: exclusive scan of the per-chunk conversion
+// totals over the chunks of each tube (one block per tube); the ENA count
+// of the tube advances by the step's total.
+__global__ void k_cx_base(CxArgs a) {
+  const int t = blockIdx.x;
+  const int c0 = a.tube_cx0[t], c1 = a.tube_cx0[t + 1];
+  __shared__ unsigned long long wsum[32];
+  __shared__ unsigned long long base;
+  const int64_t n0 = a.nena[t];
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const int l = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r0 = c0; r0 < c1; r0 += blockDim.x) {
+    const int c = r0 + threadIdx.x;
+    const unsigned long long n = (c < c1) ? a.cxconv[c] : 0ull;
+    unsigned long long x = n;
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (l >= o) x += y;
+    }
+    if (l == 31) wsum[w] = x;
+    __syncthreads();
+    unsigned long long woff = 0, tot = 0;
+    for (int v = 0; v < nw; ++v) { if (v < w) woff += wsum[v]; tot += wsum[v]; }
+    if (c < c1) a.cxbase[c] = n0 + (int64_t)(base + woff + x - n);
+    __syncthreads();
+    if (threadIdx.x == 0) base += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.nena[t] = n0 + (int64_t)base;
 }
 
 // Cartesian unit vectors along B (par), across the shell (p) and in
@@ -95,41 +129,40 @@ __device__ __forceinline__ void dipole_frame(double ct, double st, double cp,
   e_phi[0] = -sp;    e_phi[1] = cp;     e_phi[2] = 0.0;
 }
 
-// in-order conversion of the first need[Q] eligible ions per cell
-// (every block also clears its chunk's count row for the next push)
+// in-order conversion of the first need[Q] eligible ions per cell; the
+// converted ions of a chunk take consecutive ENA slots from cxbase in index
+// order (every block also clears its chunk's count row for the next push)
 __global__ void k_cx_convert(CxArgs a) {
   const int c = blockIdx.x;
   const int t = a.cx_tube[c];
   const TubeD &T = a.tubes[t];
   unsigned *crow = a.cxc + (int64_t)c * a.nqmax;
-  if (!a.cxneed[c]) {
+  const unsigned nconv = a.cxconv[c];
+  if (nconv == 0u) {
     for (int k = threadIdx.x; k < T.nq; k += blockDim.x) crow[k] = 0u;
     return;
   }
   extern __shared__ unsigned sm_[];
   unsigned *need = sm_;                 // remaining conversions per cell
   unsigned *wcnt = sm_ + a.nqmax;       // [8 warps][nq] per-tile counts
-  __shared__ unsigned remaining;
-  if (threadIdx.x == 0) remaining = 0;
-  __syncthreads();
+  __shared__ unsigned done, wconv[32];
+  if (threadIdx.x == 0) done = 0;
   for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
     const double nu = a.ct.nuPoi[T.coff + k];
     unsigned nd = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
     if (nd && c >= a.cxend[T.coff + k]) nd = 0u;  // prefix >= need
     const unsigned o = nd ? a.cxo[(int64_t)c * a.nqmax + k] : 0u;
-    const unsigned cnt = crow[k];
     crow[k] = 0u;
     need[k] = nd > o ? nd - o : 0u;
-    // conversions that can happen in this chunk
-    const unsigned here = need[k] < cnt ? need[k] : cnt;
-    if (here) atomicAdd(&remaining, here);
   }
   __syncthreads();
+  if (threadIdx.x == 0) a.cxconv[c] = 0u;  // every thread has read it
+  const int64_t slot0 = a.cxbase[c];
   const int64_t nl = a.nlive[t];
   const int64_t beg = a.cx_start[c], end = min(beg + (int64_t)CX_CHUNK, nl);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int64_t r0 = beg; r0 < end; r0 += blockDim.x) {
-    if (remaining == 0) break;  // uniform: read after the tile's last sync
+    if (done >= nconv) break;  // uniform: read after the tile's last sync
     const int64_t i = r0 + threadIdx.x;
     int q = -1;
     if (i < end) {
@@ -156,8 +189,16 @@ __global__ void k_cx_convert(CxArgs a) {
       for (int v = 0; v < nw; ++v) tot += wcnt[v * T.nq + k];
       need[k] = need[k] > tot ? need[k] - tot : 0u;
     }
+    // slot of this conversion: rank among the tile's conversions
+    const unsigned bal = __ballot_sync(0xffffffffu, conv);
+    if (l == 0) wconv[w] = __popc(bal);
+    __syncthreads();
+    unsigned woff = 0, ttot = 0;
+    for (int v = 0; v < nw; ++v) { if (v < w) woff += wconv[v]; ttot += wconv[v]; }
+    const int64_t slot = slot0 + done + woff + __popc(bal & ((1u << l) - 1u));
+    __syncthreads();  // every thread has read done and wconv
+    if (threadIdx.x == 0) done += ttot;
     if (conv) {
-      atomicSub(&remaining, 1u);
       const int64_t j = T.off + i;
       // ion position and velocity at the end of the previous step
       double rho, z, vpar, v1, v2, qk4;
@@ -201,7 +242,6 @@ __global__ void k_cx_convert(CxArgs a) {
       dipole_frame(ctk, stk, T.cphi, T.sphi, e4, e4p, e4h);
       const double VN[3] = {vpar * ep[0], vpar * ep[1], vpar * ep[2]};
       const double vp4 = e4[0] * VN[0] + e4[1] * VN[1] + e4[2] * VN[2];
-      const int64_t slot = atomicAdd((unsigned long long *)&a.nena[t], 1ull);
       if (slot < T.ecap) {
         const int64_t e = T.eoff + slot;
         a.ena.x[e] = rho * T.cphi;

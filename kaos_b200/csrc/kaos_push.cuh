@@ -42,6 +42,8 @@ struct PushArgs {
   unsigned *cxc;
   const int *tube_cx0;
   int cx_stride, cx_chunk;
+  // graph replay: the step number is read from device memory
+  const uint32_t *dstep;
 };
 
 // Flush a block's per-cell Qindk1 counts into its selection-chunk row.
@@ -181,9 +183,10 @@ template <typename T> struct HeatC {
 // the coherent branch kicks |Vperp| by sqrt(k1^2+k2^2) G1 with a uniform
 // gyro-angle.  invOm = 1/Omega is passed in (no division needed).
 template <typename T>
-__device__ __forceinline__ void heat(const PushArgs &a, const HeatC<T> &c,
-                                     uint64_t id, T invsumds, T Om, T invOm,
-                                     T vparabs, T &v1, T &v2) {
+__device__ __forceinline__ void heat(const PushArgs &a, uint32_t step,
+                                     const HeatC<T> &c, uint64_t id,
+                                     T invsumds, T Om, T invOm, T vparabs,
+                                     T &v1, T &v2) {
   const bool f64 = sizeof(T) == 8;
   const T x = Om * c.iom0;
   T e1, e2;
@@ -211,18 +214,18 @@ __device__ __forceinline__ void heat(const PushArgs &a, const HeatC<T> &c,
   T G1, G2;
   if (f64) {
     double g1, g2;
-    gauss2_64(a.seed, id, a.step, KAOS_RNG_HEAT, g1, g2);
+    gauss2_64(a.seed, id, step, KAOS_RNG_HEAT, g1, g2);
     G1 = (T)g1;
     G2 = (T)g2;
   } else {
     float g1, g2;
-    gauss2_32(a.seed, id, a.step, KAOS_RNG_HEAT, g1, g2);
+    gauss2_32(a.seed, id, step, KAOS_RNG_HEAT, g1, g2);
     G1 = (T)g1;
     G2 = (T)g2;
   }
   if (a.icrcoh) {
     const T vpn = fabs(sqrt(v1 * v1 + v2 * v2) + sqrt(k1 * k1 + k2 * k2) * G1);
-    kaos_u32x4 r = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), a.step,
+    kaos_u32x4 r = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), step,
                                (KAOS_RNG_HEAT << 24) | 2u, a.seed);
     const T ga = (T)kaos_u01(r.v[0], r.v[1]) * T(2.0 * PI);
     v1 = vpn * cos(ga);
@@ -308,6 +311,7 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   const double h = a.h, hh = 0.5 * a.h, h6 = a.h / 6.0, hsq2 = 0.5 * a.h * a.h;
   const double qs_ms = a.qs / a.ms;
   const double c_invOm = a.ms / (a.qs * MDIP);
+  const uint32_t step = a.dstep ? *a.dstep : a.step;
   const double ipG = 1.0 / T.pG, invsumds = 1.0 / T.sumdsICR;
   Ions I = a.ion;
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
       const double r = 1.0 / g1.ir;
       const double invOm = c_invOm * (r * r * r) * g1.isl;
       const HeatC<double> hc = heat_consts<double>(a.ct, (int64_t)T.coff + qi);
-      heat<double>(a, hc, I.id[j], invsumds, Om, invOm, fabs(vpar), v1n, v2n);
+      heat<double>(a, step, hc, I.id[j], invsumds, Om, invOm, fabs(vpar), v1n, v2n);
     }
     // ---- k2: half step along V_R (KineticUpdateB) -----------------------
     const double VRr = vpar * g1.er, VRz = vpar * g1.ez;
@@ -452,6 +456,7 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
   const int64_t end = min(beg + (int64_t)a.chunk, nl);
   const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
   const float qs_ms = (float)(a.qs / a.ms);
+  const uint32_t step = a.dstep ? *a.dstep : a.step;
   const float c_invOm = (float)(a.ms / (a.qs * MDIP));
   const float invsumds = (float)(1.0 / T.sumdsICR);
   const double ipG = 1.0 / T.pG;
@@ -540,7 +545,7 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
       const float invOm = c_invOm * (rf * rf * rf) * g1.isl;
       const float *hk = HK + 6 * qi;
       const HeatC<float> hc{hk[0], hk[1], hk[2], hk[3], hk[4], hk[5]};
-      heat<float>(a, hc, pid, invsumds, Om, invOm, fabsf(vpar), v1n, v2n);
+      heat<float>(a, step, hc, pid, invsumds, Om, invOm, fabsf(vpar), v1n, v2n);
     }
     const float rf = (float)rho0, zf = (float)z0;
     const float VRr = vpar * g1.er, VRz = vpar * g1.ez;

@@ -16,6 +16,8 @@ struct TubeArgs {
   double ms, qs, h, mNeut, TNeut, dNTe, dNTeEND;
   uint64_t seed;
   uint32_t nn;          // master-step index (reference nn)
+  const uint32_t *dstep;  // graph replay: nn = step / ndatfac + 1 from device
+  int ndatfac;
   int three_d;
   int te_update, have_import, eamb, grav, eapressure, eambsign, eambself,
       momfilter, qexchange, cenpar, cenperp;
@@ -85,8 +87,10 @@ __global__ void k_fields(TubeArgs a) {
   }
   __syncthreads();
   if (a.have_import || !a.eamb) return;  // imported EAmag kept as is
-  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x)
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
     M0f[Q] = a.momfilter ? filter_cell(M0p, nq, Q, a.fpM0) : M0p[Q];
+    c.mom[KAOS_M0FILT * c.ncell_total + T.coff + Q] = M0f[Q];  // M0FiltAvrgRT
+  }
   __syncthreads();
   const double S = T.sgn;  // qGL(1) <= 0 ? +1 : -1
   for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
@@ -201,95 +205,123 @@ __device__ void cell_moments(double w, double cnt, const unsigned *mp,
 }
 
 // ---------------------------------------------------------------------------
+// Warp sum (every lane gets the total).
+__device__ __forceinline__ double warp_sum(double x) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
 // Moments of one master step from the binning marginals (ZerothIonMoment ..
 // SecondParIonMoment _8_6_1-_8_6_6 with the NonUniform2D/3D integrators
-// _8_5_*), then the model-A collision counts (IonNeutralCollision
-// FrequencyASub _8_6_6_1_...:28-301).  One block per tube.
-__global__ void k_moments(TubeArgs a) {
-  extern __shared__ double sm[];
-  const TubeD T = a.tubes[blockIdx.x];
-  const int nq = T.nq;
+// _8_5_*): one warp per cell, lanes over the velocity bins.  Every
+// integrand there is a sum of single-axis terms at the bin centres, so the
+// per-axis marginal counts carry all the information.
+__global__ void __launch_bounds__(256) k_cell_moments(TubeArgs a,
+                                                      const int *cell_tube) {
+  const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   const CellTables &c = a.ct;
   const int64_t NC = c.ncell_total;
-  double *mom = c.mom;
+  if (g >= NC) return;  // whole warp
+  const TubeD &T = a.tubes[cell_tube[g]];
   const double ms = a.ms;
   const int n1 = c_vg.n1, n2 = c_vg.n2, npar = c_vg.npar;
-  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
-    const int64_t g = T.coff + Q;
-    const double w = T.nsnormfac / c.d3xC[g];
-    const double cnt = (double)a.acc.cnt[g];
-    const double NqRT = cnt * w;
-    double M[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const unsigned *mp = a.acc.mpar + g * npar, *m1 = a.acc.m1 + g * n1;
-    double Nin = 0.0;
-    for (int k = 0; k < npar; ++k) Nin += (double)mp[k];
-    if (NqRT != 0.0 && Nin != 0.0) {
-      double M0 = w * Nin;
-      double Sp = 0.0, S1 = 0.0;
-      for (int k = 0; k < npar; ++k) Sp += 0.5 * (c_vg.epar[k] + c_vg.epar[k + 1]) * mp[k];
-      for (int k = 0; k < n1; ++k) S1 += 0.5 * (c_vg.e1[k] + c_vg.e1[k + 1]) * m1[k];
-      const double M1par = (w * Sp) / M0;
-      double Tp = 0.0, Tq = 0.0, T1 = 0.0, T1c = 0.0;
-      // centred integrand; for M2|| a bin whose centred value is exactly
-      // zero falls back to the uncentred one (_8_6_6_SecondParIonMoment
-      // .f90:90-99).  The total-energy integrand also carries the Vperp
-      // terms, so it is never zero and keeps the centred value (Tq).
-      for (int k = 0; k < npar; ++k) {
-        if (!mp[k]) continue;
-        double vc = 0.5 * (c_vg.epar[k] + c_vg.epar[k + 1]);
-        double d = a.cenpar ? (vc - M1par) : vc;
-        double d2 = d * d;
-        Tq += d2 * mp[k];
-        if (d2 == 0.0) d2 = vc * vc;
-        Tp += d2 * mp[k];
-      }
-      const double M1p1 = (w * S1) / M0;
-      for (int k = 0; k < n1; ++k) {
-        if (!m1[k]) continue;
-        double vc = 0.5 * (c_vg.e1[k] + c_vg.e1[k + 1]);
-        T1 += vc * vc * m1[k];
-        double d = vc - M1p1;
-        double d2 = d * d;
-        if (d2 == 0.0) d2 = vc * vc;
-        T1c += d2 * m1[k];
-      }
-      M[KAOS_M0] = M0;
-      M[KAOS_M1PAR] = M1par;
-      M[KAOS_M2PAR] = (ms / 2.0) * ((w * Tp) / M0);
-      if (a.three_d) {
-        const unsigned *m2 = a.acc.m2 + g * n2;
-        double S2 = 0.0, T2 = 0.0, T2c = 0.0;
-        for (int k = 0; k < n2; ++k) S2 += 0.5 * (c_vg.e2[k] + c_vg.e2[k + 1]) * m2[k];
-        const double M1p2 = (w * S2) / M0;
-        for (int k = 0; k < n2; ++k) {
-          if (!m2[k]) continue;
-          double vc = 0.5 * (c_vg.e2[k] + c_vg.e2[k + 1]);
-          T2 += vc * vc * m2[k];
-          double d = vc - M1p2;
-          double d2 = d * d;
-          if (d2 == 0.0) d2 = vc * vc;
-          T2c += d2 * m2[k];
-        }
-        M[KAOS_M1PERP1] = M1p1;
-        M[KAOS_M1PERP2] = M1p2;
-        M[KAOS_M2] = (ms / 2.0) * ((w * (T1 + T2 + Tq)) / M0);
-        M[KAOS_M2PERP1] = (ms / 2.0) * ((w * (a.cenperp ? T1c : T1)) / M0);
-        M[KAOS_M2PERP2] = (ms / 2.0) * ((w * (a.cenperp ? T2c : T2)) / M0);
-      } else {
-        M[KAOS_M1PERP] = M1p1;
-        M[KAOS_M2] = (ms / 2.0) * ((w * (T1 + Tq)) / M0);
-        M[KAOS_M2PERP] = (ms / 2.0) * ((w * (a.cenperp ? T1c : T1)) / M0);
-      }
+  const double w = T.nsnormfac / c.d3xC[g];
+  const double NqRT = (double)a.acc.cnt[g] * w;
+  const unsigned *mp = a.acc.mpar + g * npar, *m1 = a.acc.m1 + g * n1;
+  const unsigned *m2 = a.three_d ? a.acc.m2 + g * n2 : nullptr;
+  double Nin = 0.0, Sp = 0.0, S1 = 0.0, S2 = 0.0;
+  for (int k = lane; k < npar; k += 32) {
+    const double m = (double)mp[k];
+    Nin += m;
+    Sp += 0.5 * (c_vg.epar[k] + c_vg.epar[k + 1]) * m;
+  }
+  for (int k = lane; k < n1; k += 32) S1 += 0.5 * (c_vg.e1[k] + c_vg.e1[k + 1]) * (double)m1[k];
+  if (m2)
+    for (int k = lane; k < n2; k += 32) S2 += 0.5 * (c_vg.e2[k] + c_vg.e2[k + 1]) * (double)m2[k];
+  Nin = warp_sum(Nin);
+  Sp = warp_sum(Sp);
+  S1 = warp_sum(S1);
+  S2 = warp_sum(S2);
+  double M[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (NqRT != 0.0 && Nin != 0.0) {
+    const double M0 = w * Nin;
+    const double M1par = (w * Sp) / M0, M1p1 = (w * S1) / M0, M1p2 = (w * S2) / M0;
+    // centred integrand; for M2|| a bin whose centred value is exactly zero
+    // falls back to the uncentred one (_8_6_6_SecondParIonMoment.f90:90-99).
+    // The total-energy integrand also carries the Vperp terms, so it is
+    // never zero and keeps the centred value (Tq).
+    double Tp = 0.0, Tq = 0.0, T1 = 0.0, T1c = 0.0, T2 = 0.0, T2c = 0.0;
+    for (int k = lane; k < npar; k += 32) {
+      if (!mp[k]) continue;
+      const double vc = 0.5 * (c_vg.epar[k] + c_vg.epar[k + 1]);
+      const double d = a.cenpar ? (vc - M1par) : vc;
+      double d2 = d * d;
+      Tq += d2 * mp[k];
+      if (d2 == 0.0) d2 = vc * vc;
+      Tp += d2 * mp[k];
     }
+    for (int k = lane; k < n1; k += 32) {
+      if (!m1[k]) continue;
+      const double vc = 0.5 * (c_vg.e1[k] + c_vg.e1[k + 1]);
+      T1 += vc * vc * m1[k];
+      const double d = vc - M1p1;
+      double d2 = d * d;
+      if (d2 == 0.0) d2 = vc * vc;
+      T1c += d2 * m1[k];
+    }
+    if (m2)
+      for (int k = lane; k < n2; k += 32) {
+        if (!m2[k]) continue;
+        const double vc = 0.5 * (c_vg.e2[k] + c_vg.e2[k + 1]);
+        T2 += vc * vc * m2[k];
+        const double d = vc - M1p2;
+        double d2 = d * d;
+        if (d2 == 0.0) d2 = vc * vc;
+        T2c += d2 * m2[k];
+      }
+    Tp = warp_sum(Tp);
+    Tq = warp_sum(Tq);
+    T1 = warp_sum(T1);
+    T1c = warp_sum(T1c);
+    T2 = warp_sum(T2);
+    T2c = warp_sum(T2c);
+    M[KAOS_M0] = M0;
+    M[KAOS_M1PAR] = M1par;
+    M[KAOS_M2PAR] = (ms / 2.0) * ((w * Tp) / M0);
+    if (a.three_d) {
+      M[KAOS_M1PERP1] = M1p1;
+      M[KAOS_M1PERP2] = M1p2;
+      M[KAOS_M2] = (ms / 2.0) * ((w * (T1 + T2 + Tq)) / M0);
+      M[KAOS_M2PERP1] = (ms / 2.0) * ((w * (a.cenperp ? T1c : T1)) / M0);
+      M[KAOS_M2PERP2] = (ms / 2.0) * ((w * (a.cenperp ? T2c : T2)) / M0);
+    } else {
+      M[KAOS_M1PERP] = M1p1;
+      M[KAOS_M2] = (ms / 2.0) * ((w * (T1 + Tq)) / M0);
+      M[KAOS_M2PERP] = (ms / 2.0) * ((w * (a.cenperp ? T1c : T1)) / M0);
+    }
+  }
+  if (lane == 0) {
+    double *mom = c.mom;
     for (int k = 0; k < 10; ++k) mom[k * NC + g] = M[k];
     mom[KAOS_NQ * NC + g] = NqRT;
     c.M0prev[g] = M[KAOS_M0];
     mom[KAOS_EAMAG * NC + g] = c.EAmag[g];
     mom[KAOS_EGMAG * NC + g] = c.EG[g];
   }
-  if (!a.qexchange) return;
-  // ---- collision counts per cell (needs filtered moments) ----------------
-  __syncthreads();
+}
+
+// Model-A collision counts of one master step (IonNeutralCollision
+// FrequencyASub _8_6_6_1_...:28-301) from the moments of k_cell_moments.
+// One block per tube.
+__global__ void k_collision_counts(TubeArgs a) {
+  extern __shared__ double sm[];
+  const TubeD T = a.tubes[blockIdx.x];
+  const int nq = T.nq;
+  const CellTables &c = a.ct;
+  const int64_t NC = c.ncell_total;
+  double *mom = c.mom;
+  const uint32_t nn = a.dstep ? *a.dstep / (uint32_t)a.ndatfac + 1u : a.nn;
   double *f1p = sm, *f11 = sm + nq, *f12 = sm + 2 * nq, *f2p = sm + 3 * nq;
   double *s1p = sm + 4 * nq, *s11 = sm + 5 * nq, *s12 = sm + 6 * nq, *s2p = sm + 7 * nq;
   const int m1i = a.three_d ? KAOS_M1PERP1 : KAOS_M1PERP;
@@ -318,7 +350,7 @@ __global__ void k_moments(TubeArgs a) {
       sigma = (l * l) * pow(1.0 - exp(-415.0 / E), 0.8);
     }
     if (M0 != 0.0) {
-      const uint64_t key = ((uint64_t)a.nn << 32) | (uint32_t)Q;
+      const uint64_t key = ((uint64_t)nn << 32) | (uint32_t)Q;
       double G0 = gauss64(a.seed, key, 0u, KAOS_RNG_NEUT, 0);
       double G1 = gauss64(a.seed, key, 0u, KAOS_RNG_NEUT, 1);
       double G2 = gauss64(a.seed, key, 0u, KAOS_RNG_NEUT, 2);
@@ -337,7 +369,7 @@ __global__ void k_moments(TubeArgs a) {
         int64_t k = -1;
         uint32_t it = 0;
         while (prod > e && it < 100000u) {
-          kaos_u32x4 w = kaos_philox((uint32_t)Q, a.nn, it >> 1, (KAOS_RNG_POIS << 24), a.seed);
+          kaos_u32x4 w = kaos_philox((uint32_t)Q, nn, it >> 1, (KAOS_RNG_POIS << 24), a.seed);
           prod *= (it & 1u) ? kaos_u01(w.v[2], w.v[3]) : kaos_u01(w.v[0], w.v[1]);
           ++k;
           ++it;
