@@ -262,6 +262,11 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
   if (timed) CK(cudaEventRecord(h->pev[2 * h->npev], h->s));
   size_t smem = (size_t)(2 * nq + 1) * sizeof(double) + (size_t)nq * sizeof(unsigned);
   if (h->mixed) smem += (size_t)5 * nq * sizeof(double) + (size_t)6 * nq * sizeof(float);
+  smem += (size_t)BIN_WIN * (1 + h->vg.npar + h->vg.n1 + (h->three_d ? h->vg.n2 : 0)) *
+          sizeof(unsigned);  // block-private binning window
+  const void *fn = h->mixed ? (h->three_d ? (const void *)k_push32<true> : (const void *)k_push32<false>)
+                            : (h->three_d ? (const void *)k_push64<true> : (const void *)k_push64<false>);
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (h->mixed) {
     if (h->three_d) k_push32<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
     else k_push32<false><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
@@ -359,7 +364,7 @@ int launch_boundary(kaos_handle *h) {
   BcArgs bc = b;
   bc.nlive = h->d_nlive;  // count reads the live counts
   k_bc_count<<<h->nblk, BC_THREADS, 0, h->s>>>(bc);
-  k_bc_scan<<<h->ntubes, 32, 0, h->s>>>(b);      // writes nlive_new
+  k_bc_scan<<<h->ntubes, 1024, 0, h->s>>>(b);    // writes nlive_new
   k_bc_scatter<<<h->nblk, BC_THREADS, 0, h->s>>>(b, h->d_nlive);
   h->launches += 3;
   CK(cudaGetLastError());
@@ -478,7 +483,7 @@ int launch_boundary_ena(kaos_handle *h) {
   BcArgs bc = b;
   bc.nlive = h->d_nena;
   k_bc_count<<<h->neblk, BC_THREADS, 0, h->s>>>(bc);
-  k_bc_scan<<<h->ntubes, 32, 0, h->s>>>(b);
+  k_bc_scan<<<h->ntubes, 1024, 0, h->s>>>(b);
   k_bc_scatter<<<h->neblk, BC_THREADS, 0, h->s>>>(b, h->d_nena);
   h->launches += 3;
   CK(cudaGetLastError());

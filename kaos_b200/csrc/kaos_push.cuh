@@ -69,6 +69,16 @@ __device__ __forceinline__ void agg_inc(unsigned int *base, int64_t idx) {
 // Qindk1/V*indk1, _8_3_1_IonParticleCounts.f90:63-80, :336-357, :612-632).
 // Only per-cell counts and the per-axis marginals are kept: every moment
 // integrand of _8_6_1.._8_6_6 is a sum of single-axis terms.
+__device__ __forceinline__ void hist_inc(const Accum &acc, const TubeD &T,
+                                         int qi, int b1, int b2, int bp) {
+  const bool d3 = c_vg.three_d;
+  int64_t nv = d3 ? (int64_t)c_vg.n1 * c_vg.n2 * c_vg.npar
+                  : (int64_t)c_vg.n1 * c_vg.npar;
+  int64_t b = d3 ? ((int64_t)b1 * c_vg.n2 + b2) * c_vg.npar + bp
+                 : (int64_t)b1 * c_vg.npar + bp;
+  atomicAdd(acc.hist + T.hoff + (int64_t)qi * nv + b, 1u);
+}
+
 __device__ __forceinline__ void accumulate(const Accum &acc, const TubeD &T,
                                            int qi, int b1, int b2, int bp,
                                            int exporting) {
@@ -80,12 +90,80 @@ __device__ __forceinline__ void accumulate(const Accum &acc, const TubeD &T,
   atomicAdd(acc.mpar + gc * c_vg.npar + bp, 1u);
   atomicAdd(acc.m1 + gc * c_vg.n1 + b1, 1u);
   if (d3) atomicAdd(acc.m2 + gc * c_vg.n2 + b2, 1u);
-  if (exporting) {
-    int64_t nv = d3 ? (int64_t)c_vg.n1 * c_vg.n2 * c_vg.npar
-                    : (int64_t)c_vg.n1 * c_vg.npar;
-    int64_t b = d3 ? ((int64_t)b1 * c_vg.n2 + b2) * c_vg.npar + bp
-                   : (int64_t)b1 * c_vg.npar + bp;
-    atomicAdd(acc.hist + T.hoff + (int64_t)qi * nv + b, 1u);
+  if (exporting) hist_inc(acc, T, qi, b1, b2, bp);
+}
+
+// Block-private binning window: the counters of BIN_WIN consecutive cells
+// starting at the cell of the block's first ion live in shared memory (the
+// ion arrays stay nearly ordered by cell: ions are created cell by cell and
+// move a small fraction of a cell per step); ions outside the window go to
+// the global counters.  The window is flushed once per block.
+constexpr int BIN_WIN = 4;
+
+__device__ __forceinline__ int bin_win_size() {
+  return BIN_WIN * (1 + c_vg.npar + c_vg.n1 + (c_vg.three_d ? c_vg.n2 : 0));
+}
+
+struct BinWin {
+  int lo;
+  unsigned *s;  // [cnt BIN_WIN][mpar BIN_WIN*npar][m1 BIN_WIN*n1][m2 BIN_WIN*n2]
+};
+
+__device__ __forceinline__ BinWin bin_win_init(unsigned *base, int first_cell,
+                                               int nq) {
+  BinWin W;
+  W.lo = max(0, min(first_cell - 1, nq - BIN_WIN));
+  W.s = base;
+  const int n = bin_win_size();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) base[k] = 0u;
+  return W;  // the caller synchronises before the first use
+}
+
+__device__ __forceinline__ void accumulate_win(const Accum &acc, const TubeD &T,
+                                               const BinWin &W, int qi, int b1,
+                                               int b2, int bp, int exporting) {
+  if (qi < 0) return;
+  const int wc = qi - W.lo;
+  if ((unsigned)wc >= (unsigned)BIN_WIN) {
+    accumulate(acc, T, qi, b1, b2, bp, exporting);
+    return;
+  }
+  atomicAdd(W.s + wc, 1u);
+  const bool d3 = c_vg.three_d;
+  if (b1 < 0 || bp < 0 || (d3 && b2 < 0)) return;
+  unsigned *mp = W.s + BIN_WIN, *m1 = mp + BIN_WIN * c_vg.npar,
+           *m2 = m1 + BIN_WIN * c_vg.n1;
+  atomicAdd(mp + wc * c_vg.npar + bp, 1u);
+  atomicAdd(m1 + wc * c_vg.n1 + b1, 1u);
+  if (d3) atomicAdd(m2 + wc * c_vg.n2 + b2, 1u);
+  if (exporting) hist_inc(acc, T, qi, b1, b2, bp);
+}
+
+__device__ __forceinline__ void bin_win_flush(const Accum &acc, const TubeD &T,
+                                              const BinWin &W) {
+  __syncthreads();
+  const int np = c_vg.npar, n1 = c_vg.n1, n2 = c_vg.three_d ? c_vg.n2 : 0;
+  const int n = bin_win_size();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const unsigned v = W.s[k];
+    if (!v) continue;
+    int r = k, wc, b;
+    unsigned *dst;
+    if (r < BIN_WIN) {
+      wc = r;
+      dst = acc.cnt + (T.coff + W.lo + wc);
+    } else if ((r -= BIN_WIN) < BIN_WIN * np) {
+      wc = r / np; b = r - wc * np;
+      dst = acc.mpar + (int64_t)(T.coff + W.lo + wc) * np + b;
+    } else if ((r -= BIN_WIN * np) < BIN_WIN * n1) {
+      wc = r / n1; b = r - wc * n1;
+      dst = acc.m1 + (int64_t)(T.coff + W.lo + wc) * n1 + b;
+    } else {
+      r -= BIN_WIN * n1;
+      wc = r / n2; b = r - wc * n2;
+      dst = acc.m2 + (int64_t)(T.coff + W.lo + wc) * n2 + b;
+    }
+    atomicAdd(dst, v);
   }
 }
 
@@ -304,10 +382,13 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   load_tube_smem(a, t, T, E, Cc);
   if (a.cxc)
     for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
-  __syncthreads();
   const int64_t nl = a.nlive[t];
   const int64_t beg = a.blk_start[blockIdx.x];
   const int64_t end = min(beg + (int64_t)a.chunk, nl);
+  BinWin W{};
+  if (a.bin)
+    W = bin_win_init(HC + nqmax, beg < end ? a.ion.qind[T.off + beg] : 0, T.nq);
+  __syncthreads();
   const double h = a.h, hh = 0.5 * a.h, h6 = a.h / 6.0, hsq2 = 0.5 * a.h * a.h;
   const double qs_ms = a.qs / a.ms;
   const double c_invOm = a.ms / (a.qs * MDIP);
@@ -342,7 +423,7 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
       const int nw = ((b1 + 1) << 16) | (bp + 1);
       if (nw != old && !a.bin_only) I.vb[j] = nw;
     }
-    if (a.bin) accumulate(a.acc, T, qi, b1, b2, bp, a.exporting);
+    if (a.bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
     if (a.bin_only) {
       if (a.write_qind) I.qind[j] = qi;
       continue;
@@ -412,6 +493,7 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
     if (a.write_qind) I.qind[j] = qi;
     if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);
   }
+  if (a.bin) bin_win_flush(a.acc, T, W);
   if (a.cxc) flush_cx_counts(a, t, beg, T.nq, HC);
 }
 
@@ -433,6 +515,11 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
   load_tube_smem(a, t, T, E, Cc);
   if (a.cxc)
     for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
+  BinWin W{};
+  if (a.bin) {
+    const int64_t b0 = a.blk_start[blockIdx.x];
+    W = bin_win_init(HC + nqmax, b0 < a.nlive[t] ? max(a.ion.cell[T.off + b0], 0) : 0, T.nq);
+  }
   for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
     const int64_t g = T.coff + k;
     const double ql = a.ct.qGL[g], qh = a.ct.qGH[g];
@@ -530,7 +617,7 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
       const int nw = ((b1 + 1) << 16) | (bp + 1);
       if (nw != old && !a.bin_only) I.vb[j] = nw;
     }
-    if (a.bin) accumulate(a.acc, T, qi, b1, b2, bp, a.exporting);
+    if (a.bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
     if (a.bin_only) {
       if (a.write_qind) I.qind[j] = qi;
       continue;
@@ -589,6 +676,7 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
     if (a.write_qind) I.qind[j] = qi;
     if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);
   }
+  if (a.bin) bin_win_flush(a.acc, T, W);
   if (a.cxc) flush_cx_counts(a, t, beg, T.nq, HC);
 }
 

@@ -448,17 +448,34 @@ __global__ void k_bc_count(BcArgs a) {
   }
 }
 
+// Exclusive scan of the kept counts over the blocks of one tube (one thread
+// block per tube, block-wide scan in tiles), then the new live count.
 __global__ void k_bc_scan(BcArgs a) {
-  // one block per tube: serial scan by thread 0 over the tube's blocks
-  // (a few thousand entries at most), then publish the new live count.
   const int t = blockIdx.x;
-  if (threadIdx.x != 0) return;
-  int64_t s = 0;
-  for (int b = a.tube_blk0[t]; b < a.tube_blk0[t + 1]; ++b) {
-    a.blkoff[b] = s;
-    s += a.blkcnt[b];
+  const int b0 = a.tube_blk0[t], b1 = a.tube_blk0[t + 1];
+  __shared__ int64_t wsum[32];
+  __shared__ int64_t base;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const int l = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r0 = b0; r0 < b1; r0 += blockDim.x) {
+    const int b = r0 + threadIdx.x;
+    const int64_t n = (b < b1) ? a.blkcnt[b] : 0;
+    int64_t x = n;  // inclusive warp scan
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (l >= o) x += y;
+    }
+    if (l == 31) wsum[w] = x;
+    __syncthreads();
+    int64_t woff = 0, tot = 0;
+    for (int v = 0; v < nw; ++v) { if (v < w) woff += wsum[v]; tot += wsum[v]; }
+    if (b < b1) a.blkoff[b] = base + woff + x - n;
+    __syncthreads();
+    if (threadIdx.x == 0) base += tot;
+    __syncthreads();
   }
-  a.nlive[t] = s;
+  if (threadIdx.x == 0) a.nlive[t] = base;
 }
 
 __global__ void k_bc_scatter(BcArgs a, const int64_t *nlive_old) {
