@@ -144,7 +144,8 @@ def run_ours(args, precision, graph=False, ndatfac=50, steps=None):
     value = nmean * steps / (ms * 1e-3)
     push_ms = pms / max(pl, 1)
     return dict(value=value, ms=ms, launches=launches, n=nmean, push_ms=push_ms,
-                t_load=t_load, solver=s, init=init, tube=tube, mi=mi)
+                t_load=t_load, solver=s, init=init, tube=tube, mi=mi,
+                launch=s.launch())
 
 
 def mixed_moment_error(s32, s64):
@@ -362,6 +363,10 @@ def main():
                                    "master step every 50 steps",
                        "precision": "mixed (FP32 state + RK, FP64 quartic/renormalisation/reductions)",
                        "l2": "inputs > L2 (particle arrays 0.5-1 GB); no flush",
+                       "push_launch": {"ions_per_item": r32["launch"][0],
+                                       "persistent": bool(r32["launch"][1] & 1),
+                                       "registers": 80 if r32["launch"][1] & 2 else 64,
+                                       "chosen_by": "autotuner"},
                        "parallelism": f"tube per GPU x{world}"},
             "fp64": {"value": r64["value"] * world, "ms_per_step": r64["ms"] / args.steps,
                      "push_ms": r64["push_ms"]},

@@ -241,8 +241,21 @@ int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches);
  * _8_KineticSolver.f90:54-239). */
 int kaos_set_graph(kaos_handle *h, int32_t on);
 
-/* Block shape for the push kernel (threads per block; 0 = autotuned). */
-int kaos_set_launch(kaos_handle *h, int32_t threads, int32_t blocks_per_sm);
+/* Launch shape of the particle push: `chunk` ions per work item (1024,
+ * 2048 or 4096; an item is a (tube, chunk of ions) pair) and `mode` bit 0:
+ * 0 = one thread block per item, 1 = a persistent grid (resident blocks per
+ * SM x SMs) striding over the items; bit 1 (mixed precision only): register
+ * budget of the push, 0 = 64 registers (4 blocks of 256 threads per SM),
+ * 1 = 80 registers (3 blocks).  chunk = 0 or mode < 0 re-arms the
+ * autotuner, which is on by default: before the first step after step 1 it
+ * times the push of every candidate on a copy of the ion state and keeps
+ * the fastest.  Results do not depend on the shape.  No reference
+ * counterpart (the reference has one MPI rank per core,
+ * _8_KineticSolver.f90:43-44). */
+int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode);
+
+/* The launch shape in use (after autotuning). */
+int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode);
 
 /* Text of the last error on this handle (static storage; never NULL). */
 const char *kaos_last_error(kaos_handle *h);

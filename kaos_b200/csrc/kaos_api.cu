@@ -26,8 +26,12 @@ namespace {
 constexpr int PUSH_THREADS = 256;
 constexpr int PUSH_ITEMS = 8;
 constexpr int BC_THREADS = 256;
-// a push block's ions lie in one charge-exchange selection chunk
-static_assert(CX_CHUNK % (PUSH_THREADS * PUSH_ITEMS) == 0, "chunk sizes");
+// push work-item sizes the autotuner tries (ions per item); an item's ions
+// lie in one charge-exchange selection chunk
+constexpr int NCHUNKS = 3;
+constexpr int CHUNKS[NCHUNKS] = {1024, 2048, 4096};
+static_assert(CX_CHUNK % 4096 == 0 && CX_CHUNK % (PUSH_THREADS * PUSH_ITEMS) == 0,
+              "chunk sizes");
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0: closed form of the
 // depressed resolvent cubic in hyperbolic form, then Newton polish.
@@ -125,6 +129,20 @@ struct kaos_handle {
     int64_t launches = 0;
   };
   std::map<uint64_t, StepGraph> graphs;
+  // push work items: (tube, chunk of ions) maps, one per candidate chunk
+  struct WorkMap {
+    int chunk = 0, n = 0;
+    int *d_tube = nullptr;
+    int64_t *d_start = nullptr;
+  };
+  WorkMap wmap[NCHUNKS];
+  int wsel = 1;          // chosen map (CHUNKS[wsel] ions per item)
+  int persistent = 0;    // persistent grid striding over the items
+  int tune_pending = 1;  // autotune before the next step
+  int regsel = 0;        // mixed push register budget: 0 = 64, 1 = 80
+  int nsm = 0;
+  int occ[2] = {0, 0};   // resident push blocks per SM per budget (0: unknown)
+  int64_t ion_len = 0;   // length of every ion array (all tubes' capacity)
   double last_ms = 0.0;
   int64_t launches = 0;
   std::vector<cudaEvent_t> pev;  // event pairs around push launches
@@ -186,9 +204,12 @@ int max_nq(const kaos_handle *h) {
 PushArgs push_args(kaos_handle *h) {
   PushArgs a{};
   a.tubes = h->d_tubes;
-  a.blk_tube = h->d_blk_tube;
-  a.blk_start = h->d_blk_start;
-  a.chunk = PUSH_THREADS * PUSH_ITEMS;
+  const kaos_handle::WorkMap &M = h->wmap[h->wsel];
+  a.blk_tube = M.d_tube;
+  a.blk_start = M.d_start;
+  a.nitems = M.n;
+  a.chunk = M.chunk;
+  a.nqs = max_nq(h);
   a.nlive = h->d_nlive;
   a.ion = h->ion[h->cur];
   a.ct = h->ct;
@@ -264,16 +285,28 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
   if (h->mixed) smem += (size_t)5 * nq * sizeof(double) + (size_t)6 * nq * sizeof(float);
   smem += (size_t)BIN_WIN * (1 + h->vg.npar + h->vg.n1 + (h->three_d ? h->vg.n2 : 0)) *
           sizeof(unsigned);  // block-private binning window
-  const void *fn = h->mixed ? (h->three_d ? (const void *)k_push32<true> : (const void *)k_push32<false>)
-                            : (h->three_d ? (const void *)k_push64<true> : (const void *)k_push64<false>);
-  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  if (h->mixed) {
-    if (h->three_d) k_push32<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
-    else k_push32<false><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
-  } else {
-    if (h->three_d) k_push64<true><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
-    else k_push64<false><<<h->nblk, PUSH_THREADS, smem, h->s>>>(a);
+  const int rs = h->mixed ? h->regsel : 0, ps = h->persistent;
+  // kernel variant: [mixed][three_d][register budget][persistent]
+  using KFn = void (*)(PushArgs);
+  static const KFn k32[2][2][2] = {
+      {{k_push32<false, 4, false>, k_push32<false, 4, true>},
+       {k_push32<false, 3, false>, k_push32<false, 3, true>}},
+      {{k_push32<true, 4, false>, k_push32<true, 4, true>},
+       {k_push32<true, 3, false>, k_push32<true, 3, true>}}};
+  static const KFn k64[2][2] = {{k_push64<false, false>, k_push64<false, true>},
+                                {k_push64<true, false>, k_push64<true, true>}};
+  const KFn fn = h->mixed ? k32[h->three_d][rs][ps] : k64[h->three_d][ps];
+  if (smem > 48 * 1024)
+    CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (!h->occ[rs]) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ[rs], (const void *)fn, PUSH_THREADS, smem));
+    h->occ[rs] = std::max(h->occ[rs], 1);
   }
+  const int grid = ps ? std::min(a.nitems, h->nsm * h->occ[rs]) : a.nitems;
+  if (grid > 0) fn<<<grid, PUSH_THREADS, smem, h->s>>>(a);
   if (timed) {
     CK(cudaEventRecord(h->pev[2 * h->npev + 1], h->s));
     h->npev++;
@@ -561,6 +594,61 @@ int step_once(kaos_handle *h) {
   return KAOS_OK;
 }
 
+// Launch-shape autotuner: the live ion state is copied into the spare
+// buffer set and the push of the next step is timed there for every
+// candidate (ions per work item x one block per item or a persistent grid);
+// the fastest is kept.  The simulation state is not touched, and results do
+// not depend on the choice (every ion is pushed by the same code).
+int autotune(kaos_handle *h) {
+  const int other = 1 - h->cur;
+  const Fields F = ion_fields(h, h->cur, other);
+  for (int f = 0; f < F.n; ++f)
+    CK(cudaMemcpyAsync(F.f[f].dst, F.f[f].src, (size_t)h->ion_len * F.f[f].size,
+                       cudaMemcpyDeviceToDevice, h->s));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int bw = h->wsel, bp = h->persistent, br = h->regsel;
+  for (int m = 0; m < NCHUNKS; ++m)
+    for (int pm = 0; pm < 2; ++pm)
+    for (int rs = 0; rs < (h->mixed ? 2 : 1); ++rs) {
+      h->wsel = m;
+      h->persistent = pm;
+      h->regsel = rs;
+      PushArgs a = push_args(h);
+      a.ion = h->ion[other];
+      a.step = (uint32_t)(h->n + 1);
+      a.write_qind = 1;
+      a.write_qk4 = 0;
+      float tmin = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {
+        CK(cudaEventRecord(e0, h->s));
+        const int npev0 = h->npev;
+        const int64_t l0 = h->launches;
+        int rc = launch_push(h, a);
+        h->npev = npev0;   // tuning pushes are not part of the step timing
+        h->launches = l0;
+        if (rc) return rc;
+        CK(cudaEventRecord(e1, h->s));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        tmin = std::min(tmin, ms);
+      }
+      if (tmin < best) { best = tmin; bw = m; bp = pm; br = rs; }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->wsel = bw;
+  h->persistent = bp;
+  h->regsel = br;
+  h->tune_pending = 0;
+  for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+  h->graphs.clear();
+  return KAOS_OK;
+}
+
 // Steps of one kind replayed from a cached CUDA graph.  A graph holds g
 // consecutive steps that share their launch sequence; its key is what the
 // sequence depends on: g, master / next-master step, the current ion and ENA
@@ -783,6 +871,22 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   CK(cudaMemcpy(h->d_blk_tube, bt.data(), bt.size() * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_blk_start, bs.data(), bs.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_tube_blk0, h->tube_blk0.data(), h->tube_blk0.size() * sizeof(int), cudaMemcpyHostToDevice));
+  for (int m = 0; m < NCHUNKS; ++m) {
+    std::vector<int> wt;
+    std::vector<int64_t> ws;
+    for (int t = 0; t < ntubes; ++t)
+      for (int64_t s0 = 0; s0 < h->th[t].cap; s0 += CHUNKS[m]) {
+        wt.push_back(t);
+        ws.push_back(s0);
+      }
+    kaos_handle::WorkMap &M = h->wmap[m];
+    M.chunk = CHUNKS[m];
+    M.n = (int)wt.size();
+    if ((rc = dalloc(h, &M.d_tube, wt.size())) || (rc = dalloc(h, &M.d_start, ws.size())))
+      return rc;
+    CK(cudaMemcpy(M.d_tube, wt.data(), wt.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(M.d_start, ws.data(), ws.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  }
   if ((rc = dalloc(h, &h->d_nlive, ntubes))) return rc;
   if ((rc = dalloc(h, &h->d_nlive_new, ntubes))) return rc;
   if ((rc = dalloc(h, &h->d_next_id, ntubes))) return rc;
@@ -796,6 +900,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   if ((rc = dalloc(h, &h->d_step, 1))) return rc;
   // particle arrays (two buffer sets for the order-preserving compaction)
   const int64_t cap = poff;
+  h->ion_len = cap;
   for (int b = 0; b < 2; ++b) {
     Ions &I = h->ion[b];
     if (h->mixed) {
@@ -1010,10 +1115,30 @@ int kaos_set_graph(kaos_handle *h, int32_t on) {
   return KAOS_OK;
 }
 
-int kaos_set_launch(kaos_handle *h, int32_t threads, int32_t bps) {
+int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode) {
   if (!h) return KAOS_ERR_PARAM;
-  (void)threads;
-  (void)bps;
+  if (chunk == 0 || mode < 0) {
+    h->tune_pending = 1;
+    return KAOS_OK;
+  }
+  int m = -1;
+  for (int k = 0; k < NCHUNKS; ++k)
+    if (CHUNKS[k] == chunk) m = k;
+  if (m < 0 || mode > 3)
+    return fail(h, KAOS_ERR_PARAM, "launch: chunk must be 1024, 2048 or 4096 and mode 0..3");
+  h->wsel = m;
+  h->persistent = mode & 1;
+  h->regsel = (mode >> 1) & 1;
+  h->tune_pending = 0;
+  for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+  h->graphs.clear();
+  return KAOS_OK;
+}
+
+int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode) {
+  if (!h || !chunk || !mode) return KAOS_ERR_PARAM;
+  *chunk = CHUNKS[h->wsel];
+  *mode = h->persistent | (h->regsel << 1);
   return KAOS_OK;
 }
 
@@ -1028,6 +1153,7 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
   for (int64_t k = 0; k < nsteps;) {
     const int64_t n = h->n + 1;
     int rc;
+    if (h->tune_pending && n >= 2 && (rc = autotune(h))) return rc;
     if (!h->graph || n == 1) {
       if ((rc = step_once(h))) return rc;
       h->dstep_valid = 0;

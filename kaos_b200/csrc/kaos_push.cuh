@@ -18,9 +18,11 @@ __constant__ VGridC c_vg;
 
 struct PushArgs {
   const TubeD *tubes;
-  const int *blk_tube;
-  const int64_t *blk_start;
-  int chunk;
+  const int *blk_tube;       // work item -> tube
+  const int64_t *blk_start;  // work item -> first ion (tube-relative)
+  int nitems;                // work items (tube, chunk of ions)
+  int chunk;                 // ions per work item
+  int nqs;                   // cells per tube in the shared-memory layout
   const int64_t *nlive;
   Ions ion;
   CellTables ct;
@@ -371,30 +373,38 @@ __device__ __forceinline__ HeatC<T> heat_consts(const CellTables &c, int64_t g) 
 
 // ---------------------------------------------------------------------------
 // FP64 kernel: ions stored as meridian-plane (rho, z) in FP64.
-template <bool THREE_D>
+template <bool THREE_D, bool PERSIST>
 __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   extern __shared__ double sm[];
-  const int t = a.blk_tube[blockIdx.x];
-  TubeD T;
-  const int nqmax = a.tubes[t].nq;
+  const int nqmax = a.nqs;
   double *E = sm, *Cc = sm + nqmax + 1;
   unsigned *HC = (unsigned *)(Cc + nqmax);
-  load_tube_smem(a, t, T, E, Cc);
-  if (a.cxc)
-    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
-  const int64_t nl = a.nlive[t];
-  const int64_t beg = a.blk_start[blockIdx.x];
-  const int64_t end = min(beg + (int64_t)a.chunk, nl);
-  BinWin W{};
-  if (a.bin)
-    W = bin_win_init(HC + nqmax, beg < end ? a.ion.qind[T.off + beg] : 0, T.nq);
-  __syncthreads();
   const double h = a.h, hh = 0.5 * a.h, h6 = a.h / 6.0, hsq2 = 0.5 * a.h * a.h;
   const double qs_ms = a.qs / a.ms;
   const double c_invOm = a.ms / (a.qs * MDIP);
   const uint32_t step = a.dstep ? *a.dstep : a.step;
-  const double ipG = 1.0 / T.pG, invsumds = 1.0 / T.sumdsICR;
   Ions I = a.ion;
+  TubeD T;
+  int tcur = -1;
+  // one work item per block, or a persistent grid striding over the items
+  for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+  const int t = a.blk_tube[item];
+  const int64_t nl = a.nlive[t];
+  const int64_t beg = a.blk_start[item];
+  if (beg >= nl) continue;  // idle chunk (uniform over the block)
+  const int64_t end = min(beg + (int64_t)a.chunk, nl);
+  __syncthreads();  // the previous item is done with the shared tables
+  if (t != tcur) {
+    load_tube_smem(a, t, T, E, Cc);
+    tcur = t;
+  }
+  if (a.cxc)
+    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
+  BinWin W{};
+  if (a.bin)
+    W = bin_win_init(HC + nqmax, a.ion.qind[T.off + beg], T.nq);
+  __syncthreads();
+  const double ipG = 1.0 / T.pG, invsumds = 1.0 / T.sumdsICR;
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t j = T.off + i;
     const int qprev = I.qind[j];
@@ -495,60 +505,69 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   }
   if (a.bin) bin_win_flush(a.acc, T, W);
   if (a.cxc) flush_cx_counts(a, t, beg, T.nq, HC);
+  if (!PERSIST) break;  // one item per block: no loop-carried state
+  }  // work items
 }
 
 // ---------------------------------------------------------------------------
 // Mixed kernel: position = (cell, FP32 offset in q); FP32 velocities and RK
 // stages; FP64 for the q reconstruction, the quartic root (Newton from a
 // per-cell linear guess) and the renormalised q of the new position.
-template <bool THREE_D>
-__global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
+// MINB = resident blocks per SM the register budget is sized for (4: 64
+// registers, 3: 80); the autotuner picks one.
+template <bool THREE_D, int MINB, bool PERSIST>
+__global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
   extern __shared__ double sm[];
-  const int t = a.blk_tube[blockIdx.x];
-  TubeD T;
-  const int nqmax = a.tubes[t].nq;
+  const int nqmax = a.nqs;
   double *E = sm, *Cc = sm + nqmax + 1;
   double *UL = Cc + nqmax, *UD = UL + nqmax, *QL = UD + nqmax, *IDQ = QL + nqmax,
          *DQ = IDQ + nqmax;
   float *HK = (float *)(DQ + nqmax);  // 6 floats per cell: K1 K2 c1 c2 iom0 lam
   unsigned *HC = (unsigned *)(HK + 6 * nqmax);
-  load_tube_smem(a, t, T, E, Cc);
-  if (a.cxc)
-    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
-  BinWin W{};
-  if (a.bin) {
-    const int64_t b0 = a.blk_start[blockIdx.x];
-    W = bin_win_init(HC + nqmax, b0 < a.nlive[t] ? max(a.ion.cell[T.off + b0], 0) : 0, T.nq);
-  }
-  for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
-    const int64_t g = T.coff + k;
-    const double ql = a.ct.qGL[g], qh = a.ct.qGH[g];
-    QL[k] = ql;
-    DQ[k] = qh - ql;
-    IDQ[k] = 1.0 / (qh - ql);
-    UL[k] = a.ct.uL[g];
-    UD[k] = a.ct.uH[g] - a.ct.uL[g];
-    if (a.icr) {
-      HK[6 * k + 0] = (float)a.ct.hK1[g];
-      HK[6 * k + 1] = (float)a.ct.hK2[g];
-      HK[6 * k + 2] = (float)a.ct.hc1[g];
-      HK[6 * k + 3] = (float)a.ct.hc2[g];
-      HK[6 * k + 4] = (float)a.ct.hiom0[g];
-      HK[6 * k + 5] = (float)a.ct.lambdaPerp[g];
-    }
-  }
-  __syncthreads();
-  const int64_t nl = a.nlive[t];
-  const int64_t beg = a.blk_start[blockIdx.x];
-  const int64_t end = min(beg + (int64_t)a.chunk, nl);
   const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
   const float qs_ms = (float)(a.qs / a.ms);
   const uint32_t step = a.dstep ? *a.dstep : a.step;
   const float c_invOm = (float)(a.ms / (a.qs * MDIP));
-  const float invsumds = (float)(1.0 / T.sumdsICR);
-  const double ipG = 1.0 / T.pG;
   const float fRE = (float)RE;
   Ions I = a.ion;
+  TubeD T;
+  int tcur = -1;
+  // one work item per block, or a persistent grid striding over the items
+  for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+  const int t = a.blk_tube[item];
+  const int64_t nl = a.nlive[t];
+  const int64_t beg = a.blk_start[item];
+  if (beg >= nl) continue;  // idle chunk (uniform over the block)
+  const int64_t end = min(beg + (int64_t)a.chunk, nl);
+  __syncthreads();  // the previous item is done with the shared tables
+  if (t != tcur) {
+    load_tube_smem(a, t, T, E, Cc);
+    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
+      const int64_t g = T.coff + k;
+      const double ql = a.ct.qGL[g], qh = a.ct.qGH[g];
+      QL[k] = ql;
+      DQ[k] = qh - ql;
+      IDQ[k] = 1.0 / (qh - ql);
+      UL[k] = a.ct.uL[g];
+      UD[k] = a.ct.uH[g] - a.ct.uL[g];
+      if (a.icr) {
+        HK[6 * k + 0] = (float)a.ct.hK1[g];
+        HK[6 * k + 1] = (float)a.ct.hK2[g];
+        HK[6 * k + 2] = (float)a.ct.hc1[g];
+        HK[6 * k + 3] = (float)a.ct.hc2[g];
+        HK[6 * k + 4] = (float)a.ct.hiom0[g];
+        HK[6 * k + 5] = (float)a.ct.lambdaPerp[g];
+      }
+    }
+    tcur = t;
+  }
+  if (a.cxc)
+    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
+  BinWin W{};
+  if (a.bin) W = bin_win_init(HC + nqmax, max(a.ion.cell[T.off + beg], 0), T.nq);
+  __syncthreads();
+  const float invsumds = (float)(1.0 / T.sumdsICR);
+  const double ipG = 1.0 / T.pG;
   // Software pipeline: the state of the next ion of this thread is loaded
   // before the current one is pushed, so its HBM latency overlaps the work.
   int n_c = DEAD;
@@ -678,6 +697,8 @@ __global__ void __launch_bounds__(256, 4) k_push32(PushArgs a) {
   }
   if (a.bin) bin_win_flush(a.acc, T, W);
   if (a.cxc) flush_cx_counts(a, t, beg, T.nq, HC);
+  if (!PERSIST) break;  // one item per block: no loop-carried state
+  }  // work items
 }
 
 }  // namespace kaos

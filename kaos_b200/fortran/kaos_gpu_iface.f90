@@ -182,12 +182,19 @@ module kaos_gpu_iface
       integer(c_int32_t), value :: on
     end function kaos_set_graph
 
-    integer(c_int) function kaos_set_launch(h, threads, blocks_per_sm) &
+    integer(c_int) function kaos_set_launch(h, chunk, mode) &
         bind(C, name="kaos_set_launch")
       import :: c_int, c_int32_t, c_ptr
       type(c_ptr), value :: h
-      integer(c_int32_t), value :: threads, blocks_per_sm
+      integer(c_int32_t), value :: chunk, mode
     end function kaos_set_launch
+
+    integer(c_int) function kaos_get_launch(h, chunk, mode) &
+        bind(C, name="kaos_get_launch")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), intent(out) :: chunk, mode
+    end function kaos_get_launch
 
     type(c_ptr) function kaos_last_error(h) bind(C, name="kaos_last_error")
       import :: c_ptr

@@ -27,6 +27,7 @@ EXPORTS = [
     "kaos_get_enas", "kaos_get_boundary", "kaos_get_timing", "kaos_set_graph",
     "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
     "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
+    "kaos_get_launch",
 ]
 
 _lib = None
@@ -64,6 +65,7 @@ def load(path: str = LIBPATH):
                                         vp, vp, i64, vp, vp, vp]
     L.kaos_set_graph.argtypes = [vp, i32]
     L.kaos_set_launch.argtypes = [vp, i32, i32]
+    L.kaos_get_launch.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
     L.kaos_last_error.argtypes = [vp]
     L.kaos_last_error.restype = C.c_char_p
     L.kaos_get_status.argtypes = [vp, C.POINTER(C.c_uint32)]
@@ -182,3 +184,13 @@ class Solver:
 
     def set_graph(self, on):
         self._check(load().kaos_set_graph(self.h, int(on)))
+
+    def set_launch(self, chunk, mode):
+        """chunk ions per work item (1024/2048/4096), mode 0 = block per
+        item, 1 = persistent grid; chunk 0 re-arms the autotuner."""
+        self._check(load().kaos_set_launch(self.h, int(chunk), int(mode)))
+
+    def launch(self):
+        c, m = C.c_int32(), C.c_int32()
+        self._check(load().kaos_get_launch(self.h, C.byref(c), C.byref(m)))
+        return c.value, m.value

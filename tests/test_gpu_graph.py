@@ -66,3 +66,44 @@ def test_graph_replay_with_export():
     np.testing.assert_array_equal(a["h"], b["h"])
     for k in a["p"]:
         np.testing.assert_array_equal(a["p"][k], b["p"][k], err_msg=k)
+
+
+def _run_shape(mixed, shape):
+    mi, spec, tube, vg = grids.config_small(n_particles=9000, three_d=True,
+                                            steps_per_master=4, heating=True,
+                                            collisions=True)
+    if mixed:
+        mi.precision = KAOS_PREC_MIXED
+    tube.nsnormCLB = 30.0
+    init = grids.initial_particles(tube, spec, mi, seed=5)
+    s = Solver(mi, [tube], vg)
+    s.load(0, *init)
+    if shape is not None:
+        s.set_launch(*shape)
+    s.step(13)
+    out = {"p": s.particles(), "e": s.enas(), "cnt": s.counts(),
+           "launch": s.launch()}
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_launch_shapes_bit_identical(mixed):
+    """Every push launch shape (ions per work item, one block per item or a
+    persistent grid, register budget) and the autotuner's choice give the
+    same particles, ENAs and counts."""
+    ref = _run_shape(mixed, (2048, 0))
+    shapes = [(1024, 1), (4096, 0), None]
+    if mixed:
+        shapes += [(1024, 2), (4096, 3)]
+    for sh in shapes:
+        o = _run_shape(mixed, sh)
+        if sh is not None:
+            assert o["launch"] == sh
+        else:
+            assert o["launch"][0] in (1024, 2048, 4096)
+        for k in ref["p"]:
+            np.testing.assert_array_equal(ref["p"][k], o["p"][k], err_msg=f"{sh} {k}")
+        for k in ref["e"]:
+            np.testing.assert_array_equal(ref["e"][k], o["e"][k], err_msg=f"{sh} {k}")
+        np.testing.assert_array_equal(ref["cnt"], o["cnt"])
