@@ -62,7 +62,20 @@ extern "C" {
 #define KAOS_EGMAG 12    /* EGmagRT gravity "field" at cell centres [V/m]   */
 #define KAOS_M0FILT 13   /* M0FiltAvrgRT filtered density used by EAmag     */
 #define KAOS_NUPOI 14    /* nuIonNeutRT Poisson collision counts per cell  */
-#define KAOS_NMOMENTS 15
+/* ENA statistics (charge exchange on), on the ENA velocity grid (Vp, Vq,
+ * Vphi) of kaos_set_ena_grid: ENAParticleCountsSub
+ * (_8_3_2_ENAParticleCounts.f90) and ZerothENAMoment .. SecondPHIENAMoment
+ * (_8_10_1 .. _8_10_8). */
+#define KAOS_ENA_NQ 15     /* NqENART  ENA density from counts [m^-3]      */
+#define KAOS_ENA_M0 16     /* M0phENART    [m^-3]                          */
+#define KAOS_ENA_M1P 17    /* M1PphENART   [m/s]                           */
+#define KAOS_ENA_M1Q 18    /* M1QphENART   [m/s]                           */
+#define KAOS_ENA_M1PHI 19  /* M1PHIphENART [m/s]                           */
+#define KAOS_ENA_M2 20     /* M2phENART    [eV]                            */
+#define KAOS_ENA_M2P 21    /* M2PphENART   [eV]                            */
+#define KAOS_ENA_M2Q 22    /* M2QphENART   [eV]                            */
+#define KAOS_ENA_M2PHI 23  /* M2PHIphENART [eV]                            */
+#define KAOS_NMOMENTS 24
 
 /*
  * Run parameters: the subset of _ModelInput.f90 / FluxTubeT flag fields
@@ -253,6 +266,12 @@ int kaos_set_graph(kaos_handle *h, int32_t on);
  * counterpart (the reference has one MPI rank per core,
  * _8_KineticSolver.f90:43-44). */
 int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode);
+
+/* ENA velocity grid V3CellT (_KineticMainParams.f90:364-399): Vp edges
+ * e1[n1+1], Vphi edges e2[n2+1], Vq (= V||) edges epar[npar+1].  Set before
+ * the first step; without it the ion grid's axes are used (Vp <- Vperp1,
+ * Vq <- Vpar, Vphi <- Vperp2, or Vperp1 on a 2D ion grid). */
+int kaos_set_ena_grid(kaos_handle *h, const kaos_vgrid_c *vg);
 
 /* The launch shape in use (after autotuning). */
 int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode);

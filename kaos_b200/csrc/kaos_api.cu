@@ -78,6 +78,7 @@ struct kaos_handle {
   std::vector<TubeD> th;          // host copy of tube descriptors
   std::vector<std::vector<double>> host_cells;  // for getters
   VGridC vg{};
+  VGridC evg{};  // ENA velocity grid (Vp = 1, Vq = par, Vphi = 2)
   cudaStream_t s = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   // device
@@ -325,6 +326,12 @@ int zero_accum(kaos_handle *h) {
     CK(cudaMemsetAsync(h->acc.m2, 0, nc * h->vg.n2 * sizeof(unsigned), h->s));
   if (h->export_on && h->acc.hist)
     CK(cudaMemsetAsync(h->acc.hist, 0, nc * (int64_t)h->nv * sizeof(unsigned), h->s));
+  if (h->acc.ecnt) {
+    CK(cudaMemsetAsync(h->acc.ecnt, 0, nc * sizeof(unsigned), h->s));
+    CK(cudaMemsetAsync(h->acc.emp, 0, nc * MAXV * sizeof(unsigned), h->s));
+    CK(cudaMemsetAsync(h->acc.emq, 0, nc * MAXV * sizeof(unsigned), h->s));
+    CK(cudaMemsetAsync(h->acc.emph, 0, nc * MAXV * sizeof(unsigned), h->s));
+  }
   return KAOS_OK;
 }
 
@@ -338,6 +345,11 @@ int launch_moments(kaos_handle *h, uint32_t nn) {
     size_t smem = (size_t)8 * max_nq(h) * sizeof(double);
     k_collision_counts<<<h->ntubes, 256, smem, h->s>>>(ta);
     h->launches++;
+    if (nn > 1) {  // ENA statistics from the second master step on
+      k_ena_moments<<<(int)((h->ncell + cells_per_block - 1) / cells_per_block), 256, 0, h->s>>>(
+          h->d_tubes, h->d_cell_tube, h->ct, h->acc, h->P.ms);
+      h->launches++;
+    }
   }
   CK(cudaGetLastError());
   return KAOS_OK;
@@ -471,8 +483,10 @@ int launch_cx(kaos_handle *h) {
   return KAOS_OK;
 }
 
-int launch_push_ena(kaos_handle *h) {
+int launch_push_ena(kaos_handle *h, int bin) {
   EnaArgs a{};
+  a.acc = h->acc;
+  a.bin = bin;
   a.tubes = h->d_tubes;
   a.blk_tube = h->d_eblk_tube;
   a.blk_start = h->d_eblk_start;
@@ -509,7 +523,8 @@ int launch_boundary_ena(kaos_handle *h) {
   F.f[F.n++] = Field{A.z, B.z, 8}; F.f[F.n++] = Field{A.vx, B.vx, 8};
   F.f[F.n++] = Field{A.vy, B.vy, 8}; F.f[F.n++] = Field{A.vz, B.vz, 8};
   F.f[F.n++] = Field{A.vps, B.vps, 8}; F.f[F.n++] = Field{A.vphs, B.vphs, 8};
-  F.f[F.n++] = Field{A.qind, B.qind, 4}; F.f[F.n++] = Field{A.id, B.id, 8};
+  F.f[F.n++] = Field{A.qind, B.qind, 4}; F.f[F.n++] = Field{A.vb, B.vb, 4};
+  F.f[F.n++] = Field{A.id, B.id, 8};
   b.fields = F;
   CK(cudaMemsetAsync(h->d_lbe_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
   CK(cudaMemsetAsync(h->d_ube_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
@@ -584,7 +599,7 @@ int step_once(kaos_handle *h) {
   p.write_qk4 = next_master || qx;
   if (qx) p.cxc = h->d_cxc;
   if ((rc = launch_push(h, p))) return rc;
-  if (qx && (rc = launch_push_ena(h))) return rc;
+  if (qx && (rc = launch_push_ena(h, master))) return rc;
   if (master) {
     if (h->P.LBCONDITIONflag == 1 && (rc = launch_inject(h, 0))) return rc;
     if (h->P.UBCONDITIONflag == 1 && (rc = launch_inject(h, 1))) return rc;
@@ -749,6 +764,14 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   for (int k = 0; k <= vg.npar; ++k) { vg.epar[k] = vgc->epar[k]; vg.fpar[k] = (float)vgc->epar[k]; }
   for (int k = 0; h->three_d && k <= vg.n2; ++k) { vg.e2[k] = vgc->e2[k]; vg.f2[k] = (float)vgc->e2[k]; }
   h->nv = h->three_d ? vg.n1 * vg.n2 * vg.npar : vg.n1 * vg.npar;
+  // ENA grid until kaos_set_ena_grid: Vp <- Vperp1 axis, Vq <- Vpar axis,
+  // Vphi <- Vperp2 axis (Vperp1 on a 2D ion grid)
+  h->evg = vg;
+  h->evg.three_d = 1;
+  if (!h->three_d) {
+    h->evg.n2 = vg.n1;
+    for (int k = 0; k <= vg.n1; ++k) { h->evg.e2[k] = vg.e1[k]; h->evg.f2[k] = vg.f1[k]; }
+  }
 
   // ---- tubes: descriptors, concatenated per-cell tables -----------------
   std::vector<double> qGL, qGH, qGC, hqC, dqC, d3xC, rGC, thC, elC, TeG, TsG,
@@ -949,9 +972,15 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
           (rc = dalloc(h, &E.z, ecap_all)) || (rc = dalloc(h, &E.vx, ecap_all)) ||
           (rc = dalloc(h, &E.vy, ecap_all)) || (rc = dalloc(h, &E.vz, ecap_all)) ||
           (rc = dalloc(h, &E.vps, ecap_all)) || (rc = dalloc(h, &E.vphs, ecap_all)) ||
-          (rc = dalloc(h, &E.qind, ecap_all)) || (rc = dalloc(h, &E.id, ecap_all)))
+          (rc = dalloc(h, &E.qind, ecap_all)) || (rc = dalloc(h, &E.vb, ecap_all)) ||
+          (rc = dalloc(h, &E.id, ecap_all)))
         return rc;
     }
+    if ((rc = dalloc(h, &h->acc.ecnt, (size_t)h->ncell)) ||
+        (rc = dalloc(h, &h->acc.emp, (size_t)h->ncell * MAXV)) ||
+        (rc = dalloc(h, &h->acc.emq, (size_t)h->ncell * MAXV)) ||
+        (rc = dalloc(h, &h->acc.emph, (size_t)h->ncell * MAXV)))
+      return rc;
     std::vector<int> ebt, te0, cxt, tc0;
     std::vector<int64_t> ebs, cxs;
     for (int t = 0; t < ntubes; ++t) {
@@ -1135,6 +1164,23 @@ int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode) {
   return KAOS_OK;
 }
 
+int kaos_set_ena_grid(kaos_handle *h, const kaos_vgrid_c *vg) {
+  if (!h || !vg) return KAOS_ERR_PARAM;
+  if (h->n != 0) return fail(h, KAOS_ERR_STATE, "the ENA grid is set before the first step");
+  if (vg->n1 < 1 || vg->n2 < 1 || vg->npar < 1 || vg->n1 > MAXV || vg->n2 > MAXV ||
+      vg->npar > MAXV || !vg->e1 || !vg->e2 || !vg->epar)
+    return fail(h, KAOS_ERR_PARAM, "ENA grid sizes must be in [1, %d]", MAXV);
+  VGridC &g = h->evg;
+  g.three_d = 1;
+  g.n1 = vg->n1;
+  g.n2 = vg->n2;
+  g.npar = vg->npar;
+  for (int k = 0; k <= g.n1; ++k) { g.e1[k] = vg->e1[k]; g.f1[k] = (float)vg->e1[k]; }
+  for (int k = 0; k <= g.n2; ++k) { g.e2[k] = vg->e2[k]; g.f2[k] = (float)vg->e2[k]; }
+  for (int k = 0; k <= g.npar; ++k) { g.epar[k] = vg->epar[k]; g.fpar[k] = (float)vg->epar[k]; }
+  return KAOS_OK;
+}
+
 int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode) {
   if (!h || !chunk || !mode) return KAOS_ERR_PARAM;
   *chunk = CHUNKS[h->wsel];
@@ -1147,6 +1193,7 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
   if (!h->loaded) return fail(h, KAOS_ERR_STATE, "kaos_step before kaos_load_particles");
   if (nsteps < 0) return fail(h, KAOS_ERR_PARAM, "nsteps < 0");
   CK(cudaMemcpyToSymbolAsync(c_vg, &h->vg, sizeof(VGridC), 0, cudaMemcpyHostToDevice, h->s));
+  CK(cudaMemcpyToSymbolAsync(c_evg, &h->evg, sizeof(VGridC), 0, cudaMemcpyHostToDevice, h->s));
   h->launches = 0;
   h->npev = 0;
   CK(cudaEventRecord(h->e0, h->s));

@@ -77,6 +77,7 @@ struct Ions {
 struct Enas {
   double *x, *y, *z, *vx, *vy, *vz, *vps, *vphs;  // vps/vphs: stale Vp, Vphi
   int32_t *qind;
+  int32_t *vb;   // Vp | Vq << 10 | Vphi << 20 bin indices, 1-based, 0: none
   uint64_t *id;
 };
 
@@ -86,9 +87,17 @@ struct Accum {
   unsigned int *m1, *m2, *mpar;  // marginals [cell][n]
   unsigned int *hist;  // optional full histogram [cell][nv]
   unsigned int *cxc;   // charge-exchange chunk counts
+  // ENAs: per-cell counts and (Vp, Vq, Vphi) marginals [cell][MAXV]
+  unsigned int *ecnt, *emp, *emq, *emph;
 };
 
 // ---- small helpers ------------------------------------------------------
+// Warp sum (every lane gets the total).
+__device__ __forceinline__ double warp_sum(double x) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
 __host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b) {
   return (a + b - 1) / b;
 }

@@ -253,6 +253,7 @@ __global__ void k_cx_convert(CxArgs a) {
         a.ena.vps[e] = 0.0;  // Vp(j), Vphi(j) still hold the ion zeros
         a.ena.vphs[e] = 0.0;
         a.ena.qind[e] = q;
+        a.ena.vb[e] = 0;
         a.ena.id[e] = a.ion.id[j];
       } else {
         atomicOr(a.status, ST_CAP);
@@ -277,9 +278,23 @@ struct EnaArgs {
   const int64_t *nena;
   CellTables ct;
   Enas ena;
+  Accum acc;
   double h, grav_GM;
   int grav;
+  int bin;  // master step: count the ENAs by start-of-step cell and bins
 };
+
+// ENA velocity grid (V3CellT): n1/e1 = Vp, npar/epar = Vq, n2/e2 = Vphi.
+__constant__ VGridC c_evg;
+
+// ENA velocity-bin search (KineticUpdateA _8_1_1_KineticUpdateA.f90:1161-
+// 1230), 1-based; the reference's out-of-grid test can never hold, so a
+// value outside the grid keeps the previous index.
+__device__ __forceinline__ int ena_bin(const double *e, int n, double v,
+                                       int prev) {
+  const int b = vbin(e, n, v);
+  return b >= 0 ? b + 1 : prev;
+}
 
 __device__ __forceinline__ void ena_geo(const double x[3], double &ct,
                                         double &st, double &cp, double &sp,
@@ -327,9 +342,26 @@ __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
     dipole_frame(ct, st, cp, sp, ep, epp, eph);
     const double vpar = ep[0] * V[0] + ep[1] * V[1] + ep[2] * V[2];
     double vps = a.ena.vps[e], vphs = a.ena.vphs[e];
+    const int vb = a.ena.vb[e];
+    int ip = vb & 1023, iq = (vb >> 10) & 1023, iph = (vb >> 20) & 1023;
     if (qi >= 0) {
       vps = fabs(epp[0] * V[0] + epp[1] * V[1] + epp[2] * V[2]);
       vphs = eph[0] * V[0] + eph[1] * V[1];
+      ip = ena_bin(c_evg.e1, c_evg.n1, vps, ip);
+      iq = ena_bin(c_evg.epar, c_evg.npar, vpar, iq);
+      iph = ena_bin(c_evg.e2, c_evg.n2, vphs, iph);
+      const int nvb = ip | (iq << 10) | (iph << 20);
+      if (nvb != vb) a.ena.vb[e] = nvb;
+      // ENAParticleCountsSub (_8_3_2_ENAParticleCounts.f90:45-300)
+      if (a.bin) {
+        const int64_t gc = T.coff + qi;
+        atomicAdd(a.acc.ecnt + gc, 1u);
+        if (ip && iq && iph) {
+          atomicAdd(a.acc.emp + gc * MAXV + (ip - 1), 1u);
+          atomicAdd(a.acc.emq + gc * MAXV + (iq - 1), 1u);
+          atomicAdd(a.acc.emph + gc * MAXV + (iph - 1), 1u);
+        }
+      }
     }
     double VR[3], A1[3], A2[3], A4[3], x2[3], x4[3];
     for (int k = 0; k < 3; ++k) VR[k] = vpar * ep[k] + vps * epp[k] + vphs * eph[k];
@@ -358,6 +390,74 @@ __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
     a.ena.vps[e] = vps;
     a.ena.vphs[e] = vphs;
     a.ena.qind[e] = qi;
+  }
+}
+
+// ENA moments of one master step from the ENA counts and (Vp, Vq, Vphi)
+// marginals (ZerothENAMoment .. SecondPHIENAMoment _8_10_1 .. _8_10_8 with
+// NonUniform3DIntegratorSub _8_9): integrands hVp hVq hVphi F (.) at the
+// bin centres, M1 = MM/M0, M2 = 6.242e18 (ms/2) MM/M0 centred on M1.  One
+// warp per cell.
+__global__ void __launch_bounds__(256) k_ena_moments(const TubeD *tubes,
+                                                     const int *cell_tube,
+                                                     CellTables c, Accum acc,
+                                                     double ms) {
+  const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t NC = c.ncell_total;
+  if (g >= NC) return;  // whole warp
+  const TubeD &T = tubes[cell_tube[g]];
+  const double w = T.nsnormfac / c.d3xC[g];
+  const double NqENA = (double)acc.ecnt[g] * w;
+  const unsigned *mp = acc.emp + g * MAXV, *mq = acc.emq + g * MAXV,
+                 *mph = acc.emph + g * MAXV;
+  const int np = c_evg.n1, nq = c_evg.npar, nph = c_evg.n2;
+  auto centre = [](const double *e, int k) { return 0.5 * (e[k] + e[k + 1]); };
+  double N = 0.0, Sp = 0.0, Sq = 0.0, Sph = 0.0;
+  for (int k = lane; k < np; k += 32) {
+    N += (double)mp[k];
+    Sp += w * centre(c_evg.e1, k) * (double)mp[k];
+  }
+  for (int k = lane; k < nq; k += 32) Sq += w * centre(c_evg.epar, k) * (double)mq[k];
+  for (int k = lane; k < nph; k += 32) Sph += w * centre(c_evg.e2, k) * (double)mph[k];
+  N = warp_sum(N);
+  Sp = warp_sum(Sp);
+  Sq = warp_sum(Sq);
+  Sph = warp_sum(Sph);
+  const double M0 = (NqENA == 0.0) ? 0.0 : w * N;
+  double m1p = 0.0, m1q = 0.0, m1ph = 0.0, tp = 0.0, tq = 0.0, tph = 0.0;
+  if (M0 != 0.0) {
+    m1p = Sp / M0;
+    m1q = Sq / M0;
+    m1ph = Sph / M0;
+    for (int k = lane; k < np; k += 32) {
+      const double d = m1p - centre(c_evg.e1, k);
+      tp += w * fabs(d * d) * (double)mp[k];
+    }
+    for (int k = lane; k < nq; k += 32) {
+      const double d = m1q - centre(c_evg.epar, k);
+      tq += w * fabs(d * d) * (double)mq[k];
+    }
+    for (int k = lane; k < nph; k += 32) {
+      const double d = m1ph - centre(c_evg.e2, k);
+      tph += w * fabs(d * d) * (double)mph[k];
+    }
+    tp = warp_sum(tp);
+    tq = warp_sum(tq);
+    tph = warp_sum(tph);
+  }
+  if (lane == 0) {
+    const double eV = 6.242e18, f = M0 != 0.0 ? eV * (ms / 2.0) / M0 : 0.0;
+    double *mom = c.mom;
+    mom[KAOS_ENA_NQ * NC + g] = NqENA;
+    mom[KAOS_ENA_M0 * NC + g] = M0;
+    mom[KAOS_ENA_M1P * NC + g] = m1p;
+    mom[KAOS_ENA_M1Q * NC + g] = m1q;
+    mom[KAOS_ENA_M1PHI * NC + g] = m1ph;
+    mom[KAOS_ENA_M2 * NC + g] = (tp + tq + tph) * f;
+    mom[KAOS_ENA_M2P * NC + g] = tp * f;
+    mom[KAOS_ENA_M2Q * NC + g] = tq * f;
+    mom[KAOS_ENA_M2PHI * NC + g] = tph * f;
   }
 }
 

@@ -205,12 +205,6 @@ __device__ void cell_moments(double w, double cnt, const unsigned *mp,
 }
 
 // ---------------------------------------------------------------------------
-// Warp sum (every lane gets the total).
-__device__ __forceinline__ double warp_sum(double x) {
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  return x;
-}
-
 // Moments of one master step from the binning marginals (ZerothIonMoment ..
 // SecondParIonMoment _8_6_1-_8_6_6 with the NonUniform2D/3D integrators
 // _8_5_*): one warp per cell, lanes over the velocity bins.  Every

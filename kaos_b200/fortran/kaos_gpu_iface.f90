@@ -20,7 +20,9 @@ module kaos_gpu_iface
     KAOS_M1PERP2 = 2, KAOS_M1PAR = 3, KAOS_M2 = 4, KAOS_M2PERP1 = 5, &
     KAOS_M2PERP2 = 6, KAOS_M2PAR = 7, KAOS_M1PERP = 8, KAOS_M2PERP = 9, &
     KAOS_NQ = 10, KAOS_EAMAG = 11, KAOS_EGMAG = 12, KAOS_M0FILT = 13, &
-    KAOS_NUPOI = 14
+    KAOS_NUPOI = 14, KAOS_ENA_NQ = 15, KAOS_ENA_M0 = 16, KAOS_ENA_M1P = 17, &
+    KAOS_ENA_M1Q = 18, KAOS_ENA_M1PHI = 19, KAOS_ENA_M2 = 20, &
+    KAOS_ENA_M2P = 21, KAOS_ENA_M2Q = 22, KAOS_ENA_M2PHI = 23
 
   ! kaos_params_c
   type, bind(C) :: kaos_params_t
@@ -188,6 +190,12 @@ module kaos_gpu_iface
       type(c_ptr), value :: h
       integer(c_int32_t), value :: chunk, mode
     end function kaos_set_launch
+
+    integer(c_int) function kaos_set_ena_grid(h, vg) bind(C, name="kaos_set_ena_grid")
+      import :: c_int, c_ptr, kaos_vgrid_t
+      type(c_ptr), value :: h
+      type(kaos_vgrid_t), intent(in) :: vg
+    end function kaos_set_ena_grid
 
     integer(c_int) function kaos_get_launch(h, chunk, mode) &
         bind(C, name="kaos_get_launch")

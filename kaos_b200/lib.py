@@ -27,7 +27,7 @@ EXPORTS = [
     "kaos_get_enas", "kaos_get_boundary", "kaos_get_timing", "kaos_set_graph",
     "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
     "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
-    "kaos_get_launch",
+    "kaos_get_launch", "kaos_set_ena_grid",
 ]
 
 _lib = None
@@ -66,6 +66,7 @@ def load(path: str = LIBPATH):
     L.kaos_set_graph.argtypes = [vp, i32]
     L.kaos_set_launch.argtypes = [vp, i32, i32]
     L.kaos_get_launch.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.kaos_set_ena_grid.argtypes = [vp, vp]
     L.kaos_last_error.argtypes = [vp]
     L.kaos_last_error.restype = C.c_char_p
     L.kaos_get_status.argtypes = [vp, C.POINTER(C.c_uint32)]
@@ -184,6 +185,12 @@ class Solver:
 
     def set_graph(self, on):
         self._check(load().kaos_set_graph(self.h, int(on)))
+
+    def set_ena_grid(self, vg):
+        """ENA velocity grid: Vp edges = vg.e1, Vphi = vg.e2, Vq = vg.epar."""
+        self._evg = vg.to_c()
+        self._ekeep = vg
+        self._check(load().kaos_set_ena_grid(self.h, C.addressof(self._evg)))
 
     def set_launch(self, chunk, mode):
         """chunk ions per work item (1024/2048/4096), mode 0 = block per

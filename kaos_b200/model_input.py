@@ -32,6 +32,10 @@ KAOS_PREC_MIXED = 1
 (KAOS_M0, KAOS_M1PERP1, KAOS_M1PERP2, KAOS_M1PAR, KAOS_M2, KAOS_M2PERP1,
  KAOS_M2PERP2, KAOS_M2PAR, KAOS_M1PERP, KAOS_M2PERP, KAOS_NQ, KAOS_EAMAG,
  KAOS_EGMAG, KAOS_M0FILT, KAOS_NUPOI) = range(15)
+# ENA statistics (ENAParticleCounts, ZerothENAMoment .. SecondPHIENAMoment)
+(KAOS_ENA_NQ, KAOS_ENA_M0, KAOS_ENA_M1P, KAOS_ENA_M1Q, KAOS_ENA_M1PHI,
+ KAOS_ENA_M2, KAOS_ENA_M2P, KAOS_ENA_M2Q, KAOS_ENA_M2PHI) = range(15, 24)
+KAOS_NMOMENTS = 24
 MOMENT_NAMES = ["M0", "M1Perp1", "M1Perp2", "M1Par", "M2", "M2Perp1",
                 "M2Perp2", "M2Par", "M1Perp", "M2Perp", "Nq", "EAmag",
                 "EGmag", "M0Filt", "nuPoi"]

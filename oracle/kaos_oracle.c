@@ -51,11 +51,15 @@ typedef struct orc {
   /* velocity grid */
   int n1, n2, npar, nv;
   double *e1, *e2, *epar, *c1, *c2, *cpar, *d3v;
+  /* ENA velocity grid V3CellT (Vp, Vq, Vphi edges) */
+  int nep, neq, neph;
+  double *eep, *eeq, *eeph;
   /* particles */
   int64_t cap, np;
   double *x, *y, *z, *Vx, *Vy, *Vz, *V1, *V2, *Vp, *AEA, *AG, *AEAN, *AGN;
   double *qk4, *rk4, *thk4, *phk4, *ellk4, *Vpe, *Vphe; /* Vpe/Vphe: ENA Vp, Vphi */
   int64_t *Qind, *ipar, *i1, *i2;
+  int64_t *iep, *ieq, *ieph; /* ENA Vpindk1, Vqindk1, Vphiindk1 (0: none) */
   unsigned char *ena;
   uint64_t *id;
   uint64_t next_id;
@@ -353,6 +357,18 @@ static void wave_heating(orc *o, int64_t j, int64_t Qk1, double OmegaGk1,
   }
 }
 
+/* ENA velocity-bin search, KineticUpdateA _8_1_1_KineticUpdateA.f90:1161-
+ * 1230 (1-based): the first cell is [lo,hi], later cells (lo,hi].  The
+ * reference's out-of-grid test (lowest edge > v and v > highest edge) can
+ * never hold, so a value outside the grid keeps the previous index. */
+static int64_t ena_bin(const double *e, int n, double v, int64_t prev) {
+  for (int k = 1; k <= n; ++k) {
+    if (k == 1 ? (e[0] <= v && v <= e[1]) : (e[k - 1] < v && v <= e[k]))
+      return k;
+  }
+  return prev;
+}
+
 /* ------------------------------------------------------------------------ */
 /* KineticRK4UpdateSub _8_1_KineticRK4Update.f90:29-315 for particle j;
  * KineticUpdateA's binning indices (:221-273, :988-1129) are stored. */
@@ -388,6 +404,9 @@ static void push_particle(orc *o, int64_t j) {
       o->Vpe[j] = fabs((1.0 - 3.0 * (ct * ct)) * (o->Vx[j] * cp + o->Vy[j] * sp) / sl +
                        3.0 * o->Vz[j] * ct * st / sl);
       o->Vphe[j] = -o->Vx[j] * sp + o->Vy[j] * cp;
+      o->iep[j] = ena_bin(o->eep, o->nep, o->Vpe[j], o->iep[j]);
+      o->ieq[j] = ena_bin(o->eeq, o->neq, Vpar, o->ieq[j]);
+      o->ieph[j] = ena_bin(o->eeph, o->neph, o->Vphe[j], o->ieph[j]);
     }
     Vpv = o->Vpe[j];
     Vphv = o->Vphe[j];
@@ -914,6 +933,7 @@ static void ensure_cap(orc *o, int64_t need) {
   GROW(AGN, double) GROW(qk4, double) GROW(rk4, double) GROW(thk4, double)
   GROW(phk4, double) GROW(ellk4, double) GROW(Vpe, double) GROW(Vphe, double)
   GROW(Qind, int64_t) GROW(ipar, int64_t) GROW(i1, int64_t) GROW(i2, int64_t)
+  GROW(iep, int64_t) GROW(ieq, int64_t) GROW(ieph, int64_t)
   GROW(ena, unsigned char) GROW(id, uint64_t)
 #undef GROW
   o->cap = nc;
@@ -923,7 +943,7 @@ static void copy_particle(orc *o, int64_t d, int64_t s) {
 #define C(a) o->a[d] = o->a[s];
   C(x) C(y) C(z) C(Vx) C(Vy) C(Vz) C(V1) C(V2) C(Vp) C(AEA) C(AG) C(AEAN)
   C(AGN) C(qk4) C(rk4) C(thk4) C(phk4) C(ellk4) C(Vpe) C(Vphe) C(Qind)
-  C(ipar) C(i1) C(i2) C(ena) C(id)
+  C(ipar) C(i1) C(i2) C(iep) C(ieq) C(ieph) C(ena) C(id)
 #undef C
 }
 
@@ -1052,6 +1072,64 @@ static void charge_exchange(orc *o) {
   }
 }
 
+/* ENAParticleCountsSub (_8_3_2_ENAParticleCounts.f90:26-300, counts by
+ * Qindk1 and Vp/Vq/Vphi indk1, density units nsnormfac/d3x) and the ENA
+ * moments ZerothENAMoment .. SecondPHIENAMoment (_8_10_1 .. _8_10_8):
+ * integrands hVp hVq hVphi F (.) at the V3CellT bin centres, M1 = MM/M0,
+ * M2 = 6.242e18 (ms/2) MM/M0 with the integrand centred on M1.  The bin
+ * sums are taken ENA by ENA (the same terms as the reference's bin loop,
+ * one per ENA).  Noise filter off (ENANOISEflag = 0). */
+static void ena_statistics(orc *o) {
+  const double ms = o->P.ms, eV = 6.242e18;
+  for (int Q = 1; Q <= o->nq; ++Q) {
+    const double w = o->nsnormfac / o->d3xC[Q - 1];
+    int64_t cnt = 0, nval = 0;
+    double sp = 0.0, sq_ = 0.0, sph = 0.0;
+    for (int64_t j = 0; j < o->np; ++j) {
+      if (!o->ena[j] || o->Qind[j] != Q)
+        continue;
+      cnt++;
+      if (o->iep[j] < 1 || o->ieq[j] < 1 || o->ieph[j] < 1)
+        continue;
+      nval++;
+      sp += w * (o->eep[o->iep[j] - 1] + o->eep[o->iep[j]]) / 2.0;
+      sq_ += w * (o->eeq[o->ieq[j] - 1] + o->eeq[o->ieq[j]]) / 2.0;
+      sph += w * (o->eeph[o->ieph[j] - 1] + o->eeph[o->ieph[j]]) / 2.0;
+    }
+    const double NqENA = (double)cnt * w;
+    double M0 = (NqENA == 0.0) ? 0.0 : (double)nval * w;
+    double m1p = 0, m1q = 0, m1ph = 0, t = 0, tp = 0, tq = 0, tph = 0;
+    if (M0 != 0.0) {
+      m1p = sp / M0;
+      m1q = sq_ / M0;
+      m1ph = sph / M0;
+      for (int64_t j = 0; j < o->np; ++j) {
+        if (!o->ena[j] || o->Qind[j] != Q || o->iep[j] < 1 || o->ieq[j] < 1 ||
+            o->ieph[j] < 1)
+          continue;
+        const double cp = (o->eep[o->iep[j] - 1] + o->eep[o->iep[j]]) / 2.0;
+        const double cq = (o->eeq[o->ieq[j] - 1] + o->eeq[o->ieq[j]]) / 2.0;
+        const double cph = (o->eeph[o->ieph[j] - 1] + o->eeph[o->ieph[j]]) / 2.0;
+        const double dp = fabs(sq(m1p - cp)), dq = fabs(sq(m1q - cq)),
+                     dph = fabs(sq(m1ph - cph));
+        t += w * (dp + dq + dph);
+        tp += w * dp;
+        tq += w * dq;
+        tph += w * dph;
+      }
+    }
+    o->mom[KAOS_ENA_NQ][Q - 1] = NqENA;
+    o->mom[KAOS_ENA_M0][Q - 1] = M0;
+    o->mom[KAOS_ENA_M1P][Q - 1] = m1p;
+    o->mom[KAOS_ENA_M1Q][Q - 1] = m1q;
+    o->mom[KAOS_ENA_M1PHI][Q - 1] = m1ph;
+    o->mom[KAOS_ENA_M2][Q - 1] = M0 != 0.0 ? eV * (ms / 2.0) * (t / M0) : 0.0;
+    o->mom[KAOS_ENA_M2P][Q - 1] = M0 != 0.0 ? eV * (ms / 2.0) * (tp / M0) : 0.0;
+    o->mom[KAOS_ENA_M2Q][Q - 1] = M0 != 0.0 ? eV * (ms / 2.0) * (tq / M0) : 0.0;
+    o->mom[KAOS_ENA_M2PHI][Q - 1] = M0 != 0.0 ? eV * (ms / 2.0) * (tph / M0) : 0.0;
+  }
+}
+
 static int is_master(const orc *o, int64_t n) {
   if (n < 2)
     return 0;
@@ -1122,8 +1200,10 @@ static void step_once(orc *o) {
     if (P->UBCONDITIONflag == 1)
       inject(o, 1);
     statistics(o);
-    if (P->QEXCHANGEflag == 1)
+    if (P->QEXCHANGEflag == 1) {
       collision_frequency(o, nn);
+      ena_statistics(o);
+    }
     memcpy(o->M0prev, o->mom[KAOS_M0], sizeof(double) * (size_t)o->nq);
     memcpy(o->mom[KAOS_EAMAG], o->EAmag, sizeof(double) * (size_t)o->nq);
     memcpy(o->mom[KAOS_EGMAG], o->EG, sizeof(double) * (size_t)o->nq);
@@ -1169,6 +1249,14 @@ orc *orc_create(const kaos_params_c *p, const kaos_tube_c *t,
     o->c2[k] = (o->e2[k] + o->e2[k + 1]) / 2.0;
   for (int k = 0; k < vg->npar; ++k)
     o->cpar[k] = (o->epar[k] + o->epar[k + 1]) / 2.0;
+  /* ENA grid: the ion grid's axes until orc_set_ena_grid (Vp <- Vperp1,
+   * Vq <- Vpar, Vphi <- Vperp2, or Vperp1 on a 2D ion grid) */
+  o->nep = vg->n1;
+  o->eep = dup(vg->e1, vg->n1 + 1);
+  o->neq = vg->npar;
+  o->eeq = dup(vg->epar, vg->npar + 1);
+  o->neph = d3 ? vg->n2 : vg->n1;
+  o->eeph = d3 ? dup(vg->e2, vg->n2 + 1) : dup(vg->e1, vg->n1 + 1);
   o->d3v = dup(NULL, o->nv);
   for (int b = 0; b < o->nv; ++b) {
     double v;
@@ -1228,6 +1316,19 @@ int orc_set_fields(orc *o, const double *EA) {
 }
 
 void orc_set_literal(orc *o, int on) { o->literal = on; }
+
+/* ENA velocity grid (Vp edges = e1/n1, Vphi = e2/n2, Vq = epar/npar). */
+void orc_set_ena_grid(orc *o, const kaos_vgrid_c *vg) {
+  free(o->eep);
+  free(o->eeq);
+  free(o->eeph);
+  o->nep = vg->n1;
+  o->eep = dup(vg->e1, vg->n1 + 1);
+  o->neph = vg->n2;
+  o->eeph = dup(vg->e2, vg->n2 + 1);
+  o->neq = vg->npar;
+  o->eeq = dup(vg->epar, vg->npar + 1);
+}
 
 int orc_step(orc *o, int64_t nsteps) {
   for (int64_t k = 0; k < nsteps; ++k)
@@ -1347,7 +1448,7 @@ void orc_destroy(orc *o) {
                    &o->Vz, &o->V1, &o->V2, &o->Vp, &o->AEA, &o->AG, &o->AEAN,
                    &o->AGN, &o->qk4, &o->rk4, &o->thk4, &o->phk4, &o->ellk4,
                    &o->Vpe, &o->Vphe, &o->Te, &o->EAmag, &o->EG, &o->M0prev,
-                   &o->nuPoi, &o->EAimport};
+                   &o->nuPoi, &o->EAimport, &o->eep, &o->eeq, &o->eeph};
   for (size_t k = 0; k < sizeof(ds) / sizeof(ds[0]); ++k)
     free(*ds[k]);
   for (int k = 0; k < KAOS_NMOMENTS; ++k)
@@ -1356,6 +1457,9 @@ void orc_destroy(orc *o) {
   free(o->ipar);
   free(o->i1);
   free(o->i2);
+  free(o->iep);
+  free(o->ieq);
+  free(o->ieph);
   free(o->ena);
   free(o->id);
   free(o->cnt);

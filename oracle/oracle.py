@@ -33,6 +33,7 @@ def lib():
         L.orc_load.argtypes = [vp] + [vp] * 4 + [C.c_int64]
         L.orc_set_fields.argtypes = [vp, vp]
         L.orc_set_literal.argtypes = [vp, C.c_int]
+        L.orc_set_ena_grid.argtypes = [vp, vp]
         L.orc_step.argtypes = [vp, C.c_int64]
         L.orc_count.restype = C.c_int64
         L.orc_count.argtypes = [vp, vp]
@@ -82,6 +83,12 @@ class Oracle:
 
     def set_literal(self, on):
         lib().orc_set_literal(self.h, int(on))
+
+    def set_ena_grid(self, vg):
+        """ENA velocity grid: Vp edges = vg.e1, Vphi = vg.e2, Vq = vg.epar."""
+        self._evg = vg.to_c()
+        self._ekeep = vg
+        lib().orc_set_ena_grid(self.h, C.addressof(self._evg))
 
     def step(self, n):
         lib().orc_step(self.h, int(n))

@@ -119,6 +119,33 @@ def test_mixed_precision_moments_close_to_fp64_oracle():
         assert rel_norm(s.moments(m), o.moments(m)) < 2e-3
 
 
+ENA_MOMENTS = list(range(15, 24))  # KAOS_ENA_NQ .. KAOS_ENA_M2PHI
+
+
+def test_ena_statistics_match_oracle():
+    """ENA counts by start-of-step cell and (Vp, Vq, Vphi) bins and the ENA
+    moments (ZerothENAMoment .. SecondPHIENAMoment) on a separate ENA grid,
+    FP64 path against the oracle."""
+    from kaos_b200.grids import make_vgrid
+    mi, spec, tube, vg = grids.config_small(n_particles=3000, three_d=True,
+                                            steps_per_master=3, collisions=True)
+    evg = make_vgrid(True, 12, 20, 18, 7e3)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=3)
+    o = Oracle(mi, tube, vg)
+    o.set_ena_grid(evg)
+    o.load(q, vpar, v1, v2)
+    s = Solver(mi, [tube], vg)
+    s.set_ena_grid(evg)
+    s.load(0, q, vpar, v1, v2)
+    o.step(16)
+    s.step(16)  # master steps at 3, 6, ..., 15
+    assert s.count() == o.count()
+    assert np.max(o.moments(16)) > 0  # ENAs were binned
+    for m in ENA_MOMENTS:
+        a, b = s.moments(m), o.moments(m)
+        assert rel_norm(a, b) < MOM_TOL, (m, rel_norm(a, b))
+
+
 @pytest.mark.parametrize("mixed", [False, True])
 def test_charge_exchange_and_ena_push(mixed):
     """Ion -> ENA conversion of the first N ions per cell in index order

@@ -208,3 +208,25 @@ def test_mirror_only_invariant():
     i1 = invariant(o.particles())
     scale = 0.5 * (vpar ** 2 + v1 ** 2 + v2 ** 2).mean()
     assert np.max(np.abs(i1 - i0)) / scale < 1e-6
+
+
+def test_ena_moment_consistency():
+    """The reference's ENA moment diagnostics (_8_10_*): M0 <= NqENA, M2 is
+    the sum of its P, Q and PHI parts, M1P >= 0 (Vp is |Vp|); ENAs exist
+    after a few master steps with charge exchange on."""
+    from kaos_b200.model_input import (KAOS_ENA_NQ, KAOS_ENA_M0, KAOS_ENA_M1P,
+                                       KAOS_ENA_M2, KAOS_ENA_M2P, KAOS_ENA_M2Q,
+                                       KAOS_ENA_M2PHI)
+    mi, spec, tube, vg = grids.config_small(n_particles=2000, three_d=True,
+                                            steps_per_master=3, collisions=True)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=3)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    o.step(13)
+    nq, m0 = o.moments(KAOS_ENA_NQ), o.moments(KAOS_ENA_M0)
+    assert np.max(m0) > 0
+    assert np.all(m0 <= nq * (1 + 1e-12))
+    m2 = o.moments(KAOS_ENA_M2)
+    parts = o.moments(KAOS_ENA_M2P) + o.moments(KAOS_ENA_M2Q) + o.moments(KAOS_ENA_M2PHI)
+    np.testing.assert_allclose(m2, parts, rtol=1e-12, atol=0)
+    assert np.all(o.moments(KAOS_ENA_M1P) >= 0)
