@@ -141,6 +141,11 @@ typedef struct kaos_tube_c {
   /* ICR wave-heating tables (_1_SimParameterization.f90:1408-1444)        */
   const double *lambdaPerp, *EtaLH, *XiPerp1, *XiPerp2;
   const double *S0, *OmegaG0, *ChiPerp1, *ChiPerp2;
+  /* species of this entry (SpecieT(s)%msT, qsT); 0 = kaos_params_c ms/qs.
+   * Several species of one flux tube are separate entries: the reference
+   * runs species as independent outermost loops (_8_KineticSolver.f90:43),
+   * each with the ambipolar field of its own density. */
+  double ms, qs;
 } kaos_tube_c;
 
 /*

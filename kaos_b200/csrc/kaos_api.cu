@@ -347,7 +347,7 @@ int launch_moments(kaos_handle *h, uint32_t nn) {
     h->launches++;
     if (nn > 1) {  // ENA statistics from the second master step on
       k_ena_moments<<<(int)((h->ncell + cells_per_block - 1) / cells_per_block), 256, 0, h->s>>>(
-          h->d_tubes, h->d_cell_tube, h->ct, h->acc, h->P.ms);
+          h->d_tubes, h->d_cell_tube, h->ct, h->acc);
       h->launches++;
     }
   }
@@ -805,6 +805,8 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     d.nsnormCLB = T.nsnormCLB;
     d.nsnormCUB = T.nsnormCUB;
     d.sumdsICR = T.sumdsICR;
+    d.ms = T.ms > 0.0 ? T.ms : p->ms;
+    d.qs = T.qs != 0.0 ? T.qs : p->qs;
     d.moff = moff;
     d.hoff = hoff;
     d.ecap = (p->QEXCHANGEflag == 1) ? (int64_t)T.capacity / 4 + 4096 : 0;
@@ -825,7 +827,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     app(chi1, T.ChiPerp1, 0); app(chi2, T.ChiPerp2, 0);
     // wave-heating constants: K_i = h sqrt(q^2 xi_i eta S0 / (2 m^2 pi))
     for (int k = 0; k < T.nq; ++k) {
-      const double pre = (p->qs * p->qs / (2.0 * p->ms * p->ms)) *
+      const double pre = (d.qs * d.qs / (2.0 * d.ms * d.ms)) *
                          (T.S0 ? T.S0[k] : 0.0) * (T.EtaLH ? T.EtaLH[k] : 0.0);
       hK1.push_back(p->h * std::sqrt(pre * (T.XiPerp1 ? T.XiPerp1[k] : 0.0) / PI));
       hK2.push_back(p->h * std::sqrt(pre * (T.XiPerp2 ? T.XiPerp2[k] : 0.0) / PI));

@@ -48,6 +48,7 @@ struct TubeD {
   int64_t moff;            // offset of this tube's marginal counters
   int64_t hoff;            // offset of this tube's full histogram
   double rhoLB, zLB, rhoUB, zUB;     // injection points (cell centres)
+  double ms, qs;                     // species mass [kg] and charge [C]
 };
 
 // Per-cell tables (device pointers, concatenated over tubes).

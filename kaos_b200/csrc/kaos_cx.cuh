@@ -400,13 +400,13 @@ __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
 // warp per cell.
 __global__ void __launch_bounds__(256) k_ena_moments(const TubeD *tubes,
                                                      const int *cell_tube,
-                                                     CellTables c, Accum acc,
-                                                     double ms) {
+                                                     CellTables c, Accum acc) {
   const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t NC = c.ncell_total;
   if (g >= NC) return;  // whole warp
   const TubeD &T = tubes[cell_tube[g]];
+  const double ms = T.ms;
   const double w = T.nsnormfac / c.d3xC[g];
   const double NqENA = (double)acc.ecnt[g] * w;
   const unsigned *mp = acc.emp + g * MAXV, *mq = acc.emq + g * MAXV,

@@ -195,7 +195,7 @@ __device__ __forceinline__ void field_prologue(const PushArgs &a,
                                                const TubeD &T, const double *E,
                                                const double *C, double qk,
                                                double &aea, double &ag) {
-  const double qm = a.qs / a.ms;
+  const double qm = T.qs / T.ms;
   double v;
   if (a.ff.eamb && interp_centres(E, C, a.ct.EAmag + T.coff, a.ct.qGC + T.coff,
                                   T.nq, T.sgn, qk, &v)) {
@@ -380,8 +380,6 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   double *E = sm, *Cc = sm + nqmax + 1;
   unsigned *HC = (unsigned *)(Cc + nqmax);
   const double h = a.h, hh = 0.5 * a.h, h6 = a.h / 6.0, hsq2 = 0.5 * a.h * a.h;
-  const double qs_ms = a.qs / a.ms;
-  const double c_invOm = a.ms / (a.qs * MDIP);
   const uint32_t step = a.dstep ? *a.dstep : a.step;
   Ions I = a.ion;
   TubeD T;
@@ -405,6 +403,8 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
     W = bin_win_init(HC + nqmax, a.ion.qind[T.off + beg], T.nq);
   __syncthreads();
   const double ipG = 1.0 / T.pG, invsumds = 1.0 / T.sumdsICR;
+  const double qs_ms = T.qs / T.ms;
+  const double c_invOm = T.ms / (T.qs * MDIP);
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t j = T.off + i;
     const int qprev = I.qind[j];
@@ -525,9 +525,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
   float *HK = (float *)(DQ + nqmax);  // 6 floats per cell: K1 K2 c1 c2 iom0 lam
   unsigned *HC = (unsigned *)(HK + 6 * nqmax);
   const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
-  const float qs_ms = (float)(a.qs / a.ms);
   const uint32_t step = a.dstep ? *a.dstep : a.step;
-  const float c_invOm = (float)(a.ms / (a.qs * MDIP));
   const float fRE = (float)RE;
   Ions I = a.ion;
   TubeD T;
@@ -568,6 +566,8 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
   __syncthreads();
   const float invsumds = (float)(1.0 / T.sumdsICR);
   const double ipG = 1.0 / T.pG;
+  const float qs_ms = (float)(T.qs / T.ms);
+  const float c_invOm = (float)(T.ms / (T.qs * MDIP));
   // Software pipeline: the state of the next ion of this thread is loaded
   // before the current one is pushed, so its HBM latency overlaps the work.
   int n_c = DEAD;

@@ -81,8 +81,8 @@ __global__ void k_fields(TubeArgs a) {
       if (tn <= a.dNTeEND) c.Te[g] = tn;
     }
     M0p[Q] = c.M0prev[g];
-    c.EG[g] = a.grav ? (-2.0 * GG * ME * a.ms * cos(c.thetaGC[g]) /
-                        (a.qs * (c.rGC[g] * c.rGC[g]) * sqrt(c.ellGC[g])))
+    c.EG[g] = a.grav ? (-2.0 * GG * ME * T.ms * cos(c.thetaGC[g]) /
+                        (T.qs * (c.rGC[g] * c.rGC[g]) * sqrt(c.ellGC[g])))
                      : 0.0;
   }
   __syncthreads();
@@ -98,7 +98,7 @@ __global__ void k_fields(TubeArgs a) {
     double ep = 0.0;
     if (M0p[Q] != 0.0 && a.eapressure) {
       const double *Mn = M0f;
-      double R1 = (1.0 / fabs(c.hqC[g])) * (KB * c.Te[g] / (a.qs * Mn[Q]));
+      double R1 = (1.0 / fabs(c.hqC[g])) * (KB * c.Te[g] / (T.qs * Mn[Q]));
       double st, den;
       if (Q == 0) {
         st = -25.0 * Mn[Q] + 48.0 * Mn[Q + 1] - 36.0 * Mn[Q + 2] +
@@ -130,6 +130,29 @@ __global__ void k_fields(TubeArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// The one occupied bin of a marginal (all the cell's ions share it), or -1.
+// A cell whose ions share one bin of an axis has that bin's centre as its
+// first moment along the axis (the exact value of the ratio of sums), so the
+// centred second-moment integrand of that bin is zero and falls back to the
+// uncentred one (_8_6_6_SecondParIonMoment.f90:90-99) on every path.
+__device__ __forceinline__ int warp_single_bin(const unsigned *m, int n) {
+  int nz = 0, last = -1;
+  for (int k = threadIdx.x & 31; k < n; k += 32)
+    if (m[k]) { ++nz; last = k; }
+  for (int o = 16; o > 0; o >>= 1) {
+    nz += __shfl_xor_sync(0xffffffffu, nz, o);
+    last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+  }
+  return nz == 1 ? last : -1;
+}
+
+__device__ __forceinline__ int single_bin(const unsigned *m, int n) {
+  int nz = 0, last = -1;
+  for (int k = 0; k < n; ++k)
+    if (m[k]) { ++nz; last = k; }
+  return nz == 1 ? last : -1;
+}
+
 // Moments of one cell from its count and binning marginals, for the
 // allocation-free statistics entry point (ZerothIonMoment
 // .. SecondParIonMoment _8_6_1-_8_6_6 with the NonUniform2D/3D integrators
@@ -151,7 +174,8 @@ __device__ void cell_moments(double w, double cnt, const unsigned *mp,
   double Sp = 0.0, S1 = 0.0;
   for (int k = 0; k < npar; ++k) Sp += 0.5 * (epar[k] + epar[k + 1]) * mp[k];
   for (int k = 0; k < n1; ++k) S1 += 0.5 * (e1[k] + e1[k + 1]) * m1[k];
-  const double M1par = (w * Sp) / M0;
+  const int kp = single_bin(mp, npar), k1 = single_bin(m1, n1);
+  const double M1par = kp >= 0 ? 0.5 * (epar[kp] + epar[kp + 1]) : (w * Sp) / M0;
   double Tp = 0.0, Tq = 0.0, T1 = 0.0, T1c = 0.0;
   // centred integrand; for M2|| a bin whose centred value is exactly zero
   // falls back to the uncentred one (_8_6_6_SecondParIonMoment.f90:90-99).
@@ -166,7 +190,7 @@ __device__ void cell_moments(double w, double cnt, const unsigned *mp,
     if (d2 == 0.0) d2 = vc * vc;
     Tp += d2 * mp[k];
   }
-  const double M1p1 = (w * S1) / M0;
+  const double M1p1 = k1 >= 0 ? 0.5 * (e1[k1] + e1[k1 + 1]) : (w * S1) / M0;
   for (int k = 0; k < n1; ++k) {
     if (!m1[k]) continue;
     const double vc = 0.5 * (e1[k] + e1[k + 1]);
@@ -182,7 +206,8 @@ __device__ void cell_moments(double w, double cnt, const unsigned *mp,
   if (three_d) {
     double S2 = 0.0, T2 = 0.0, T2c = 0.0;
     for (int k = 0; k < n2; ++k) S2 += 0.5 * (e2[k] + e2[k + 1]) * m2[k];
-    const double M1p2 = (w * S2) / M0;
+    const int k2 = single_bin(m2, n2);
+    const double M1p2 = k2 >= 0 ? 0.5 * (e2[k2] + e2[k2 + 1]) : (w * S2) / M0;
     for (int k = 0; k < n2; ++k) {
       if (!m2[k]) continue;
       const double vc = 0.5 * (e2[k] + e2[k + 1]);
@@ -218,7 +243,7 @@ __global__ void __launch_bounds__(256) k_cell_moments(TubeArgs a,
   const int64_t NC = c.ncell_total;
   if (g >= NC) return;  // whole warp
   const TubeD &T = a.tubes[cell_tube[g]];
-  const double ms = a.ms;
+  const double ms = T.ms;
   const int n1 = c_vg.n1, n2 = c_vg.n2, npar = c_vg.npar;
   const double w = T.nsnormfac / c.d3xC[g];
   const double NqRT = (double)a.acc.cnt[g] * w;
@@ -237,10 +262,15 @@ __global__ void __launch_bounds__(256) k_cell_moments(TubeArgs a,
   Sp = warp_sum(Sp);
   S1 = warp_sum(S1);
   S2 = warp_sum(S2);
+  // the one occupied bin of each axis, or -1 (see warp_single_bin)
+  const int kp = warp_single_bin(mp, npar), k1 = warp_single_bin(m1, n1);
+  const int k2 = m2 ? warp_single_bin(m2, n2) : -1;
   double M[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (NqRT != 0.0 && Nin != 0.0) {
     const double M0 = w * Nin;
-    const double M1par = (w * Sp) / M0, M1p1 = (w * S1) / M0, M1p2 = (w * S2) / M0;
+    const double M1par = kp >= 0 ? 0.5 * (c_vg.epar[kp] + c_vg.epar[kp + 1]) : (w * Sp) / M0;
+    const double M1p1 = k1 >= 0 ? 0.5 * (c_vg.e1[k1] + c_vg.e1[k1 + 1]) : (w * S1) / M0;
+    const double M1p2 = k2 >= 0 ? 0.5 * (c_vg.e2[k2] + c_vg.e2[k2 + 1]) : (w * S2) / M0;
     // centred integrand; for M2|| a bin whose centred value is exactly zero
     // falls back to the uncentred one (_8_6_6_SecondParIonMoment.f90:90-99).
     // The total-energy integrand also carries the Vperp terms, so it is
@@ -547,8 +577,8 @@ __global__ void k_inject(InjArgs a) {
   const double rho0 = a.ub ? T.rhoUB : T.rhoLB, z0 = a.ub ? T.zUB : T.zLB;
   const double r = sqrt(rho0 * rho0 + z0 * z0);
   const double ct = z0 / r, st = rho0 / r, el = 1.0 + 3.0 * ct * ct, sl = sqrt(el);
-  const double sig = sqrt(KB * a.ct.TsG[g] / a.ms);
-  const double qm = a.qs / a.ms;
+  const double sig = sqrt(KB * a.ct.TsG[g] / T.ms);
+  const double qm = T.qs / T.ms;
   const double aea = fabs(qm * fabs(a.ct.EAmag[g])), ag = fabs(qm * fabs(a.ct.EG[g]));
   const double qc = a.ct.qGC[g];
   const uint64_t id0 = a.next_id[t];

@@ -47,6 +47,7 @@ module kaos_gpu_iface
     type(c_ptr) :: TeG, TsG, nsnormCNeut
     type(c_ptr) :: lambdaPerp, EtaLH, XiPerp1, XiPerp2
     type(c_ptr) :: S0, OmegaG0, ChiPerp1, ChiPerp2
+    real(c_double) :: ms, qs   ! SpecieT(s)%msT, qsT of this entry; 0 = params
   end type kaos_tube_t
 
   ! kaos_vgrid_c: separable velocity-cell edges (n+1 values per axis)

@@ -65,6 +65,8 @@ class TubeSpec:
     heat_rate_eV_s: float = 0.0   # ICR heating rate at the base cell [eV/s]
     chi: float = 1.7              # ICR spectral index
     capacity_factor: float = 1.3
+    ms: float = 0.0               # species mass [kg]; 0 = ModelInput.ms
+    qs: float = 0.0               # species charge [C]; 0 = ModelInput.qs
 
 
 
@@ -97,14 +99,16 @@ def make_tube(spec: TubeSpec, mi: ModelInput) -> Tube:
     # ICR tables: S0 chosen so that the base-cell mean heating rate is
     # heat_rate_eV_s: <d(m v^2/2)/dt> = m (D1 + D2) with
     # D = q^2/(2 m^2) xi eta S0 (Omega/Omega0)^-chi (sigma = 1).
+    ms = spec.ms if spec.ms > 0 else mi.ms
+    qs = spec.qs if spec.qs != 0 else mi.qs
     Bc = 8.06e15 * np.sqrt(ell) / r ** 3
-    Om = mi.qs * Bc / mi.ms
+    Om = qs * Bc / ms
     Om0 = np.full(nq, Om[0])
     xi, eta = 0.5, 0.125
     S0val = 0.0
     if spec.heat_rate_eV_s > 0:
         rate_J = spec.heat_rate_eV_s * 1.602e-19
-        S0val = rate_J / (mi.ms * 2.0 * (mi.qs ** 2 / (2 * mi.ms ** 2)) * xi * eta)
+        S0val = rate_J / (ms * 2.0 * (qs ** 2 / (2 * ms ** 2)) * xi * eta)
     arc = float(np.sum(hq * dq))
     t = Tube(nq=nq, pG=L, phiG=spec.phi, nsnormfac=nsnormfac,
              nsnormCLB=0.0, nsnormCUB=0.0, qGL=qGL, qGH=qGH, qGC=qGC,
@@ -115,13 +119,13 @@ def make_tube(spec: TubeSpec, mi: ModelInput) -> Tube:
              XiPerp1=np.full(nq, xi), XiPerp2=np.full(nq, xi),
              S0=np.full(nq, S0val), OmegaG0=Om0,
              ChiPerp1=np.full(nq, spec.chi), ChiPerp2=np.full(nq, spec.chi),
-             sumdsICR=arc)
+             sumdsICR=arc, ms=spec.ms, qs=spec.qs)
     counts = np.rint(n_c * d3x / nsnormfac).astype(np.int64)
     # LB injection: the LB-cell macro-particle count per master step
     # (_0_1_1_ConfigGridGeneratorB.f90:189), scaled by the ratio of the
     # master-step cadence to the LB-cell transit time (Q0ndatfac,
     # _0_ConfigGridGenerator.f90:664-666) when the cadence is shorter.
-    q0ndatfac = hq[0] * dq[0] * np.sqrt(mi.ms / (KB * Ti[0])) / mi.h
+    q0ndatfac = hq[0] * dq[0] * np.sqrt(ms / (KB * Ti[0])) / mi.h
     frac = min(1.0, mi.ndatfac / q0ndatfac)
     t.nsnormCLB = float(np.rint(counts[0] * frac))
     t.capacity = int(spec.n_particles * spec.capacity_factor) + 1024
@@ -171,7 +175,7 @@ def initial_particles(tube: Tube, spec: TubeSpec, mi: ModelInput, seed: int,
     else:
         f = rng.uniform(0.02, 0.98, size=n)
         q = tube.qGL[cell] + f * (tube.qGH[cell] - tube.qGL[cell])
-    sig = np.sqrt(KB * tube.TsG[cell] / mi.ms)
+    sig = np.sqrt(KB * tube.TsG[cell] / (tube.ms if tube.ms > 0 else mi.ms))
     v = rng.normal(size=(3, n)) * sig
     return q, v[0].copy(), v[1].copy(), v[2].copy()
 

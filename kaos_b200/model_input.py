@@ -77,7 +77,7 @@ class KaosTube(C.Structure):
         ("TeG", _DP), ("TsG", _DP), ("nsnormCNeut", _DP),
         ("lambdaPerp", _DP), ("EtaLH", _DP), ("XiPerp1", _DP),
         ("XiPerp2", _DP), ("S0", _DP), ("OmegaG0", _DP), ("ChiPerp1", _DP),
-        ("ChiPerp2", _DP),
+        ("ChiPerp2", _DP), ("ms", C.c_double), ("qs", C.c_double),
     ]
 
 
@@ -166,13 +166,15 @@ class Tube:
     ChiPerp2: np.ndarray
     sumdsICR: float = 1.0
     capacity: int = 0
+    ms: float = 0.0   # species of this entry; 0 = ModelInput.ms / qs
+    qs: float = 0.0
 
     def to_c(self) -> KaosTube:
         t = KaosTube()
         t.nq = self.nq
         t.capacity = self.capacity
         for k in ("pG", "phiG", "nsnormfac", "nsnormCLB", "nsnormCUB",
-                  "sumdsICR"):
+                  "sumdsICR", "ms", "qs"):
             setattr(t, k, float(getattr(self, k)))
         for k in ("qGL", "qGH", "qGC", "hqC", "dqC", "d3xC", "rGC",
                   "thetaGC", "ellGC", "TeG", "TsG", "nsnormCNeut",

@@ -661,6 +661,23 @@ static void interpolate_particles(orc *o, int use_q0, const double *q0) {
   }
 }
 
+/* The one occupied bin of axis `ax` (0: Vperp1, 1: Vperp2, 2: Vpar) of a
+ * cell's histogram H[(i1*n2 + i2)*npar + ip], or -1 when several are. */
+static int single_bin(const int64_t *H, int n1, int n2, int npar, int ax) {
+  int found = -1;
+  for (int i1 = 0; i1 < n1; ++i1)
+    for (int i2 = 0; i2 < n2; ++i2)
+      for (int ip = 0; ip < npar; ++ip) {
+        if (!H[((int64_t)i1 * n2 + i2) * npar + ip])
+          continue;
+        int k = ax == 0 ? i1 : (ax == 1 ? i2 : ip);
+        if (found >= 0 && found != k)
+          return -1;
+        found = k;
+      }
+  return found;
+}
+
 /* ------------------------------------------------------------------------ */
 /* ParticleCounts / DistributionFunctions / moments for one master step
  * (_8_3_1_IonParticleCounts.f90:26-451, _8_4_1_IonDistributionFunctions
@@ -741,6 +758,16 @@ static void statistics(orc *o) {
       if (M0 == 0.0)
         continue;
       double M1p1 = S1 / M0, M1p2 = S2 / M0, M1par = Sp / M0;
+      /* a cell whose ions share one bin of an axis has that bin's centre as
+       * its first moment along the axis (the exact value of the ratio); the
+       * centred second-moment integrand of that bin is then zero and falls
+       * back to the uncentred one (_8_6_6_SecondParIonMoment.f90:90-99) */
+      int kp = single_bin(H, o->n1, o->n2, o->npar, 2);
+      int k1 = single_bin(H, o->n1, o->n2, o->npar, 0);
+      int k2 = single_bin(H, o->n1, o->n2, o->npar, 1);
+      if (kp >= 0) M1par = o->cpar[kp];
+      if (k1 >= 0) M1p1 = o->c1[k1];
+      if (k2 >= 0) M1p2 = o->c2[k2];
       o->mom[KAOS_M1PERP1][Q] = M1p1;
       o->mom[KAOS_M1PERP2][Q] = M1p2;
       o->mom[KAOS_M1PAR][Q] = M1par;
@@ -805,6 +832,10 @@ static void statistics(orc *o) {
       if (M0 == 0.0)
         continue;
       double M1perp = (2.0 * PI * Sperp) / M0, M1par = (2.0 * PI * Spar) / M0;
+      int kp = single_bin(H, o->n1, 1, o->npar, 2);
+      int k1 = single_bin(H, o->n1, 1, o->npar, 0);
+      if (kp >= 0) M1par = o->cpar[kp];
+      if (k1 >= 0) M1perp = o->c1[k1];
       o->mom[KAOS_M1PERP][Q] = M1perp;
       o->mom[KAOS_M1PAR][Q] = M1par;
       double T = 0, Tperp = 0, Tp = 0;
@@ -1219,6 +1250,10 @@ orc *orc_create(const kaos_params_c *p, const kaos_tube_c *t,
   o->P = *p;
   if (o->P.ndatfac < 1)
     o->P.ndatfac = 1;
+  if (t->ms > 0.0) /* species of this entry (SpecieT(s)%msT, qsT) */
+    o->P.ms = t->ms;
+  if (t->qs != 0.0)
+    o->P.qs = t->qs;
   int nq = t->nq;
   o->nq = nq;
   o->pG = t->pG;

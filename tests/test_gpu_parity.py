@@ -209,3 +209,38 @@ def test_batched_uneven_tubes_one_launch():
         np.testing.assert_array_equal(s.counts(k), o.counts())
         a, b = s.moments(KAOS_M0, k), o.moments(KAOS_M0)
         assert rel_norm(a, b) < MOM_TOL, k
+
+
+def test_two_species_as_separate_entries():
+    """H+ and O+ of one flux tube as two entries of one batched solver (the
+    reference runs species as independent outer loops, each with its own
+    ambipolar field): each matches its own oracle run in FP64, with wave
+    heating and charge exchange on."""
+    from kaos_b200.grids import TubeSpec, make_tube, make_vgrid
+    from kaos_b200.model_input import MH, MO, ModelInput
+    mi = ModelInput(h=0.01, ndatfac=4, ION2VPERPflag=1, ICRflag=1, QEXCHANGEflag=1)
+    vg = make_vgrid(True, 16, 16, 24, 3e4)
+    common = dict(L=4.0, nq=24, q_ub=0.15, H=600e3, heat_rate_eV_s=5.0,
+                  neut_n0=3e18, neut_H=300e3)
+    specs = [TubeSpec(n_particles=800, ms=MH, **common),
+             TubeSpec(n_particles=3200, ms=MO, **common)]
+    tubes = [make_tube(sp, mi) for sp in specs]
+    s = Solver(mi, tubes, vg)
+    inits = []
+    for k, (sp, t) in enumerate(zip(specs, tubes)):
+        inits.append(grids.initial_particles(t, sp, mi, seed=40 + k))
+        s.load(k, *inits[k])
+    s.step(10)
+    for k, (sp, t) in enumerate(zip(specs, tubes)):
+        o = Oracle(mi, t, vg)
+        o.load(*inits[k])
+        o.step(10)
+        assert s.count(k) == o.count(), k
+        po, ps = o.particles(), s.particles(k)
+        for key in ("z", "vpar", "vperp1", "vperp2"):
+            assert rel_norm(ps[key], po[key]) < TRAJ_TOL, (k, key)
+        np.testing.assert_array_equal(s.counts(k), o.counts())
+        for m in moment_list(True):
+            assert rel_norm(s.moments(m, k), o.moments(m)) < MOM_TOL, (k, m)
+    # the species differ: lighter ions are faster
+    assert np.std(s.particles(0)["vpar"]) > 2 * np.std(s.particles(1)["vpar"])

@@ -230,3 +230,22 @@ def test_ena_moment_consistency():
     parts = o.moments(KAOS_ENA_M2P) + o.moments(KAOS_ENA_M2Q) + o.moments(KAOS_ENA_M2PHI)
     np.testing.assert_allclose(m2, parts, rtol=1e-12, atol=0)
     assert np.all(o.moments(KAOS_ENA_M1P) >= 0)
+
+
+def test_single_bin_cell_moments():
+    """A cell whose ions share one V|| bin has that bin's centre as M1|| and,
+    the centred integrand being zero, the uncentred M2|| fallback of
+    _8_6_6_SecondParIonMoment.f90:90-99: M2|| = (m/2) vc^2."""
+    mi, spec, tube, vg = grids.config_small(n_particles=2000, three_d=True)
+    q = np.full(3, 0.5 * (tube.qGL[5] + tube.qGH[5]))
+    ep = np.asarray(vg.epar)
+    vc = 0.5 * (ep[14] + ep[15])
+    vpar = np.array([vc, vc, 0.5 * (vc + ep[15])])   # all in V|| bin 14
+    v1 = np.array([100.0, 900.0, 2000.0])
+    v2 = np.array([-300.0, 50.0, 700.0])
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    o.step(1)  # statistics of the loaded state
+    assert o.moments(KAOS_M1PAR)[5] == vc
+    np.testing.assert_allclose(o.moments(KAOS_M2PAR)[5], (mi.ms / 2.0) * vc * vc,
+                               rtol=1e-13)
