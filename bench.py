@@ -132,6 +132,8 @@ def run_ours(args, precision, graph=False, ndatfac=50, steps=None):
     s.load(0, *init)
     t_load = time.perf_counter() - t0
     s.set_graph(graph)
+    if args.launch:
+        s.set_launch(*(int(x) for x in args.launch.split(",")))
     s.step(args.warmup)
     n0, _ = s.count()
     # --- device-timed region: K steps in one call (CUDA events on the
@@ -293,6 +295,12 @@ def main():
     ap.add_argument("--no-heating", action="store_true")
     ap.add_argument("--no-collisions", dest="collisions", action="store_false")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--only", default="all", choices=["all", "mixed"],
+                    help="mixed: time the mixed path alone (for profiling)")
+    ap.add_argument("--launch", default=None,
+                    help="fixed push launch shape CHUNK,MODE instead of the autotuner "
+                         "(CHUNK ions per work item 1024/2048/4096; MODE bit 0 persistent "
+                         "grid, bit 1 80-register mixed push)")
     args = ap.parse_args()
     if args.impl == "reference":
         line = reference_arm(args)
@@ -310,8 +318,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from kaos_b200.model_input import KAOS_PREC_FP64, KAOS_PREC_MIXED
+    full = args.only == "all"
     # FP64 path first (reported beside the headline)
-    r64 = run_ours(args, KAOS_PREC_FP64)
+    r64 = run_ours(args, KAOS_PREC_FP64) if full else None
     stop = threading.Event()
     samples = []
     th = threading.Thread(target=clocks_sampler, args=(stop, samples), daemon=True)
@@ -324,16 +333,19 @@ def main():
     stop.set()
     # error of every moment of the mixed path against the FP64 path (same
     # particles, same random streams, last master step)
-    moment_error = mixed_moment_error(r32["solver"], r64["solver"])
-    r64["solver"].close()
+    moment_error = mixed_moment_error(r32["solver"], r64["solver"]) if full else None
+    if full:
+        r64["solver"].close()
     r32["solver"].close()
     # the same steps replayed from CUDA graphs, and at cadence 1 (every step
     # a master step: removal/injection, fields, counts and moments each step)
-    rg = run_ours(args, KAOS_PREC_MIXED, graph=True)
-    rg["solver"].close()
-    rc1 = run_ours(args, KAOS_PREC_MIXED, graph=True, ndatfac=1,
-                   steps=min(args.steps, 50))
-    rc1["solver"].close()
+    rg = rc1 = None
+    if full:
+        rg = run_ours(args, KAOS_PREC_MIXED, graph=True)
+        rg["solver"].close()
+        rc1 = run_ours(args, KAOS_PREC_MIXED, graph=True, ndatfac=1,
+                       steps=min(args.steps, 50))
+        rc1["solver"].close()
     ms = r32["ms"]
     if dist is not None:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -344,9 +356,9 @@ def main():
     achieved = mixed_bytes * r32["n"] / (r32["push_ms"] * 1e-3) / 1e9
     peak, peak_kind = peaks()
     e2e = None
-    if not args.skip_e2e:
+    if not args.skip_e2e and full:
         e2e = run_e2e(args, KAOS_PREC_MIXED)
-    cpu = cpu_baseline(args) if (rank == 0 and world == 1) else None
+    cpu = cpu_baseline(args) if (rank == 0 and world == 1 and full) else None
     tpi = profiled_traffic("k_push32_mixed_c2.md")
     traffic = None if tpi is None else tpi * r32["n"]
     if rank == 0:
@@ -366,19 +378,22 @@ def main():
                        "push_launch": {"ions_per_item": r32["launch"][0],
                                        "persistent": bool(r32["launch"][1] & 1),
                                        "registers": 80 if r32["launch"][1] & 2 else 64,
-                                       "chosen_by": "autotuner"},
+                                       "chosen_by": "fixed" if args.launch else "autotuner"},
                        "parallelism": f"tube per GPU x{world}"},
-            "fp64": {"value": r64["value"] * world, "ms_per_step": r64["ms"] / args.steps,
-                     "push_ms": r64["push_ms"]},
-            "mixed_over_fp64": value / (r64["value"] * world),
+            "fp64": None if not full else {
+                "value": r64["value"] * world, "ms_per_step": r64["ms"] / args.steps,
+                "push_ms": r64["push_ms"]},
+            "mixed_over_fp64": value / (r64["value"] * world) if full else None,
             "mixed_push_ms": r32["push_ms"],
             "moment_error_vs_fp64": moment_error,
-            "graph": {"value": rg["value"] * world, "ms_per_step": rg["ms"] / args.steps,
-                      "note": "mixed path, steps replayed from CUDA graphs"},
-            "cadence1": {"value": rc1["value"] * world,
-                         "ms_per_step": rc1["ms"] / min(args.steps, 50),
-                         "steps": min(args.steps, 50),
-                         "note": "mixed path, every step a master step, CUDA graphs"},
+            "graph": None if not full else {
+                "value": rg["value"] * world, "ms_per_step": rg["ms"] / args.steps,
+                "note": "mixed path, steps replayed from CUDA graphs"},
+            "cadence1": None if not full else {
+                "value": rc1["value"] * world,
+                "ms_per_step": rc1["ms"] / min(args.steps, 50),
+                "steps": min(args.steps, 50),
+                "note": "mixed path, every step a master step, CUDA graphs"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
