@@ -442,8 +442,14 @@ int launch_inject(kaos_handle *h, int ub) {
     a.cx_stride = max_nq(h);
     a.cx_chunk = CX_CHUNK;
   }
-  k_inject<<<h->ntubes, 256, 0, h->s>>>(a);
-  h->launches++;
+  // blocks per tube: enough for the largest injection, at most 64
+  int64_t kmax = 0;
+  for (const TubeD &T : h->th)
+    kmax = std::max(kmax, (int64_t)std::llrint(ub ? T.nsnormCUB : T.nsnormCLB));
+  const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (kmax + 255) / 256));
+  k_inject<<<dim3(bx, h->ntubes), 256, 0, h->s>>>(a);
+  k_inject_commit<<<(h->ntubes + 127) / 128, 128, 0, h->s>>>(a, h->ntubes);
+  h->launches += 2;
   CK(cudaGetLastError());
   return KAOS_OK;
 }

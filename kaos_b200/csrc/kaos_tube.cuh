@@ -561,19 +561,24 @@ struct InjArgs {
   int cx_stride, cx_chunk;
 };
 
+// Ions injected by one tube at this master step (capacity-clamped).
+__device__ __forceinline__ int64_t inject_count(const InjArgs &a, const TubeD &T,
+                                                int64_t nl) {
+  const int64_t k = (int64_t)llrint(a.ub ? T.nsnormCUB : T.nsnormCLB);
+  if (k <= 0) return 0;
+  return nl + k > T.cap ? max(T.cap - nl, (int64_t)0) : k;
+}
+
+// grid (blocks per tube, tubes): every block of a tube reads the same live
+// count; k_inject_commit advances it afterwards
 __global__ void k_inject(InjArgs a) {
-  const int t = blockIdx.x;
+  const int t = blockIdx.y;
   const TubeD T = a.tubes[t];
   const int Q = a.ub ? T.nq - 1 : 0;
   const int64_t g = T.coff + Q;
-  int64_t k = (int64_t)llrint(a.ub ? T.nsnormCUB : T.nsnormCLB);
   const int64_t nl = a.nlive[t];
+  const int64_t k = inject_count(a, T, nl);
   if (k <= 0) return;
-  if (nl + k > T.cap) {
-    if (threadIdx.x == 0) atomicOr(a.status, ST_CAP);
-    k = T.cap - nl;
-    if (k <= 0) return;
-  }
   const double rho0 = a.ub ? T.rhoUB : T.rhoLB, z0 = a.ub ? T.zUB : T.zLB;
   const double r = sqrt(rho0 * rho0 + z0 * z0);
   const double ct = z0 / r, st = rho0 / r, el = 1.0 + 3.0 * ct * ct, sl = sqrt(el);
@@ -583,7 +588,8 @@ __global__ void k_inject(InjArgs a) {
   const double qc = a.ct.qGC[g];
   const uint64_t id0 = a.next_id[t];
   const bool d3 = c_vg.three_d;
-  for (int64_t i = threadIdx.x; i < k; i += blockDim.x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k;
+       i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t j = T.off + nl + i;
     const uint64_t id = id0 + (uint64_t)i;
     const double Vx0 = sig * gauss64(a.seed, id, 0u, KAOS_RNG_INJECT, 0);
@@ -623,12 +629,21 @@ __global__ void k_inject(InjArgs a) {
       agg_inc(a.cxc, (int64_t)(a.tube_cx0[t] + (int)((nl + i) / a.cx_chunk)) * a.cx_stride + Q);
     if (a.bin) accumulate(a.acc, T, Q, b1, d3 ? b2 : 0, bp, a.exporting);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    a.nlive[t] = nl + k;
-    a.next_id[t] = id0 + (uint64_t)k;
-    a.n_in[t] = (unsigned long long)k;
-  }
+}
+
+// After k_inject: advance the live counts and ids (one thread per tube) and
+// flag a capacity clamp.
+__global__ void k_inject_commit(InjArgs a, int ntubes) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntubes) return;
+  const TubeD &T = a.tubes[t];
+  const int64_t nl = a.nlive[t];
+  const int64_t want = (int64_t)llrint(a.ub ? T.nsnormCUB : T.nsnormCLB);
+  const int64_t k = inject_count(a, T, nl);
+  if (want > 0 && k < want) atomicOr(a.status, ST_CAP);
+  a.nlive[t] = nl + k;
+  a.next_id[t] += (uint64_t)k;
+  a.n_in[t] = (unsigned long long)k;
 }
 
 }  // namespace kaos
