@@ -178,6 +178,31 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
                         const double *vpar, const double *vperp1,
                         const double *vperp2, int64_t n);
 
+/*
+ * Initial ions generated on the device, in place of kaos_load_particles:
+ * the steps either side of the loop that DensityProfileA1/B, the velocity
+ * distribution and InitialConditions do on the host in the reference
+ * (_2_1_DensityProfileA1.f90, _4_DensityProfileB.f90,
+ * _6_VelocityDistribution.f90, _7_InitialConditions.f90).  counts[k] ions
+ * start in cell k at q uniform over the middle 96 % of the cell; each ion's
+ * velocity (V||, Vperp1, Vperp2) is an isotropic Maxwellian at the cell's
+ * TsG, or, with probability tail_fraction, an isotropic kappa distribution
+ * f ~ (1 + v^2/(kappa theta^2))^-(kappa+1) of temperature tail_T (drawn as
+ * a Student-t vector of 2 kappa - 1 degrees of freedom; 2 kappa - 1 must be
+ * an integer in [3, 63]).  Random numbers: Philox keyed by (seed, ion index,
+ * KAOS_RNG_INIT), the same generator as the CPU oracle's, so both start from
+ * the same ions.  Ions are numbered 0..n-1 in cell order.
+ */
+typedef struct kaos_init_c {
+  const int64_t *counts;   /* ions per cell [nq]                           */
+  double tail_fraction;    /* fraction of ions from the kappa tail, [0, 1] */
+  double kappa;            /* kappa index of the tail                      */
+  double tail_T;           /* tail temperature [K]                         */
+  uint64_t seed;
+} kaos_init_c;
+
+int kaos_init_particles(kaos_handle *h, int32_t tube, const kaos_init_c *init);
+
 /* Set the per-cell ambipolar field EAmagRT (host-imported spin-up
  * profile, _8_7_AmbipolarEfield.f90:1375-1402) used on the first step.
  * NULL resets to "compute from the initial moments". */

@@ -31,6 +31,7 @@
 #define KAOS_RNG_INJECT 2u /* boundary-injection Maxwellian, per particle */
 #define KAOS_RNG_NEUT 3u   /* neutral velocity sample, per cell/master    */
 #define KAOS_RNG_POIS 4u   /* Poisson collision count, per cell/master    */
+#define KAOS_RNG_INIT 5u   /* initial ions (position, population, V)      */
 
 typedef struct {
   uint32_t v[4];

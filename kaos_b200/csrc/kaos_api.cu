@@ -1122,6 +1122,59 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
   return KAOS_OK;
 }
 
+int kaos_init_particles(kaos_handle *h, int32_t tube, const kaos_init_c *in) {
+  if (!h) return KAOS_ERR_PARAM;
+  if (tube < 0 || tube >= h->ntubes) return fail(h, KAOS_ERR_PARAM, "bad tube %d", tube);
+  if (!in || !in->counts) return fail(h, KAOS_ERR_PARAM, "null counts");
+  if (h->n != 0) return fail(h, KAOS_ERR_STATE, "particles must be loaded before the first step");
+  const TubeD &T = h->th[tube];
+  const int nu = (int)std::llround(2.0 * in->kappa - 1.0);
+  if (!(in->tail_fraction >= 0.0 && in->tail_fraction <= 1.0) ||
+      (in->tail_fraction > 0.0 &&
+       (std::fabs(2.0 * in->kappa - 1.0 - nu) > 1e-9 || nu < 3 || nu > 63 || !(in->tail_T > 0.0))))
+    return fail(h, KAOS_ERR_PARAM, "init: tail_fraction in [0,1]; 2 kappa - 1 an integer in [3, 63]; tail_T > 0");
+  std::vector<int64_t> pre(T.nq + 1, 0);
+  for (int k = 0; k < T.nq; ++k) {
+    if (in->counts[k] < 0) return fail(h, KAOS_ERR_PARAM, "negative count in cell %d", k);
+    pre[k + 1] = pre[k] + in->counts[k];
+  }
+  const int64_t n = pre[T.nq];
+  if (n > T.cap) return fail(h, KAOS_ERR_CAPACITY, "tube %d: %lld particles exceed capacity %lld", tube, (long long)n, (long long)T.cap);
+  int64_t *d_pre = nullptr;
+  if (cudaMalloc(&d_pre, pre.size() * sizeof(int64_t)) != cudaSuccess)
+    return fail(h, KAOS_ERR_CUDA, "cudaMalloc of the init prefix failed");
+  InitArgs a{};
+  a.T = T;
+  a.pre = d_pre;
+  a.n = n;
+  a.ion = h->ion[h->cur];
+  a.ct = h->ct;
+  a.tail_fraction = in->tail_fraction;
+  a.nu = nu;
+  a.s_tail = in->tail_fraction > 0.0
+                 ? std::sqrt(KB * in->tail_T / T.ms * (double)(nu - 2) / (double)nu) : 0.0;
+  a.seed = in->seed;
+  a.mixed = h->mixed;
+  cudaError_t e = cudaMemcpy(d_pre, pre.data(), pre.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_vg, &h->vg, sizeof(VGridC));
+  if (e == cudaSuccess && n > 0) {
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 32);
+    k_init<<<grid, 256>>>(a);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(d_pre);
+  if (e != cudaSuccess) return fail(h, KAOS_ERR_CUDA, "init: %s", cudaGetErrorString(e));
+  int64_t nl = n;
+  uint64_t nid = (uint64_t)n;
+  CK(cudaMemcpy(h->d_nlive + tube, &nl, sizeof(int64_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_next_id + tube, &nid, sizeof(uint64_t), cudaMemcpyHostToDevice));
+  if (h->d_cxc)  // the first push starts the selection counts from zero
+    CK(cudaMemset(h->d_cxc, 0, (size_t)h->ncx * max_nq(h) * sizeof(unsigned)));
+  h->loaded = 1;
+  return KAOS_OK;
+}
+
 int kaos_set_fields(kaos_handle *h, int32_t tube, const double *EAmag,
                     int32_t nq) {
   if (!h) return KAOS_ERR_PARAM;

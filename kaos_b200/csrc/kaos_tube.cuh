@@ -646,4 +646,104 @@ __global__ void k_inject_commit(InjArgs a, int ntubes) {
   a.n_in[t] = (unsigned long long)k;
 }
 
+// ---------------------------------------------------------------------------
+// Initial ions on the device (kaos_init_particles): the draws of the CPU
+// oracle's generator (orc_init), then the derived per-ion state that
+// kaos_load_particles computes on the host.  Products and sums of the draws
+// are written with explicit rounding so that no multiply-add is fused.
+struct InitArgs {
+  TubeD T;
+  const int64_t *pre;   // [nq+1] exclusive prefix of the per-cell counts
+  int64_t n;
+  Ions ion;
+  CellTables ct;
+  double tail_fraction, s_tail;
+  int nu;               // Student-t degrees of freedom of the kappa tail
+  uint64_t seed;
+  int mixed;
+};
+
+__device__ __forceinline__ void init_pair(uint64_t seed, uint64_t id,
+                                          uint32_t sub, double &a, double &b) {
+  kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), 0u,
+                             (KAOS_RNG_INIT << 24) | sub, seed);
+  const double u1 = kaos_u01(w.v[0], w.v[1]), u2 = kaos_u01(w.v[2], w.v[3]);
+  const double R = sqrt(__dmul_rn(-2.0, log(u1)));
+  double sn, cs;
+  sincos(__dmul_rn(__dmul_rn(2.0, PI), u2), &sn, &cs);
+  a = __dmul_rn(R, cs);
+  b = __dmul_rn(R, sn);
+}
+
+__global__ void k_init(InitArgs a) {
+  const TubeD &T = a.T;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = T.nq;  // cell: pre[lo] <= j < pre[lo + 1]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (a.pre[mid] <= j) lo = mid; else hi = mid;
+    }
+    const int c = lo;
+    const int64_t g = T.coff + c;
+    kaos_u32x4 w = kaos_philox((uint32_t)j, (uint32_t)((uint64_t)j >> 32), 0u,
+                               (KAOS_RNG_INIT << 24), a.seed);
+    const double upos = kaos_u01(w.v[0], w.v[1]), upop = kaos_u01(w.v[2], w.v[3]);
+    const double qL = a.ct.qGL[g], qH = a.ct.qGH[g];
+    const double q = __dadd_rn(qL, __dmul_rn(__dadd_rn(0.02, __dmul_rn(0.96, upos)),
+                                             __dadd_rn(qH, -qL)));
+    const bool tail = upop < a.tail_fraction;
+    double g0, g1, g2, g3;
+    init_pair(a.seed, (uint64_t)j, 1u, g0, g1);
+    init_pair(a.seed, (uint64_t)j, 2u, g2, g3);
+    double f;
+    if (!tail) {
+      f = sqrt(KB * a.ct.TsG[g] / T.ms);
+    } else {
+      double W = __dmul_rn(g3, g3), x, y;
+      int m = 1;  // normals 3 .. 3+nu-1; g3 is the first
+      for (uint32_t sub = 3; m < a.nu; ++sub) {
+        init_pair(a.seed, (uint64_t)j, sub, x, y);
+        W = __dadd_rn(W, __dmul_rn(x, x));
+        if (++m < a.nu) { W = __dadd_rn(W, __dmul_rn(y, y)); ++m; }
+      }
+      f = a.s_tail / sqrt(W / (double)a.nu);
+    }
+    const double vpar = __dmul_rn(f, g0), v1 = __dmul_rn(f, g1), v2 = __dmul_rn(f, g2);
+    const int64_t k = T.off + j;
+    Ions I = a.ion;
+    I.qind[k] = c;
+    I.id[k] = (uint64_t)j;
+    if (I.vb) {
+      const int bp = vbin(c_vg.epar, c_vg.npar, vpar);
+      const int b1 = vbin(c_vg.e1, c_vg.n1, sqrt(v1 * v1 + v2 * v2));
+      I.vb[k] = ((b1 + 1) << 16) | (bp + 1);
+    }
+    if (a.mixed) {
+      I.cell[k] = c;
+      I.off[k] = (float)((q - qL) / (qH - qL));
+      I.fvpar[k] = (float)vpar;
+      I.fv1[k] = (float)v1;
+      I.fv2[k] = (float)v2;
+      I.fqk4[k] = (float)q;
+    } else {
+      // position on the meridian plane: quartic root by Newton from the
+      // cell's linear guess (converged to FP64 precision)
+      const double fr = (q - qL) / (qH - qL);
+      const double u0 = a.ct.uL[g] + fr * (a.ct.uH[g] - a.ct.uL[g]);
+      const double u = quartic_newton(q, 1.0 / T.pG, u0, 6);
+      const double st = sqrt(u / T.pG), ctv = q * u * u, r = u * RE;
+      double rho = r * st, z = r * ctv;
+      if (fabs(rho) < 1e-6) rho = 0.0;
+      if (fabs(z) < 1e-6) z = 0.0;
+      I.rho[k] = rho;
+      I.z[k] = z;
+      I.vpar[k] = vpar;
+      I.v1[k] = v1;
+      I.v2[k] = v2;
+      I.qk4[k] = q;
+    }
+  }
+}
+
 }  // namespace kaos

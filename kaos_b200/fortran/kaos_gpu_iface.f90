@@ -56,6 +56,13 @@ module kaos_gpu_iface
     type(c_ptr) :: e1, e2, epar
   end type kaos_vgrid_t
 
+  ! kaos_init_c: on-device initial ions
+  type, bind(C) :: kaos_init_t
+    type(c_ptr) :: counts            ! integer(c_int64_t) per cell
+    real(c_double) :: tail_fraction, kappa, tail_T
+    integer(c_int64_t) :: seed
+  end type kaos_init_t
+
   interface
     integer(c_int) function kaos_create(p, tubes, ntubes, vg, h) &
         bind(C, name="kaos_create")
@@ -75,6 +82,14 @@ module kaos_gpu_iface
       real(c_double), intent(in) :: q(*), vpar(*), vperp1(*), vperp2(*)
       integer(c_int64_t), value :: n
     end function kaos_load_particles
+
+    integer(c_int) function kaos_init_particles(h, tube, init) &
+        bind(C, name="kaos_init_particles")
+      import :: c_int, c_int32_t, c_ptr, kaos_init_t
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: tube
+      type(kaos_init_t), intent(in) :: init
+    end function kaos_init_particles
 
     integer(c_int) function kaos_set_fields(h, tube, EAmag, nq) &
         bind(C, name="kaos_set_fields")

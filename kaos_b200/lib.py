@@ -27,7 +27,7 @@ EXPORTS = [
     "kaos_get_enas", "kaos_get_boundary", "kaos_get_timing", "kaos_set_graph",
     "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
     "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
-    "kaos_get_launch", "kaos_set_ena_grid",
+    "kaos_get_launch", "kaos_set_ena_grid", "kaos_init_particles",
 ]
 
 _lib = None
@@ -67,6 +67,7 @@ def load(path: str = LIBPATH):
     L.kaos_set_launch.argtypes = [vp, i32, i32]
     L.kaos_get_launch.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
     L.kaos_set_ena_grid.argtypes = [vp, vp]
+    L.kaos_init_particles.argtypes = [vp, i32, vp]
     L.kaos_last_error.argtypes = [vp]
     L.kaos_last_error.restype = C.c_char_p
     L.kaos_get_status.argtypes = [vp, C.POINTER(C.c_uint32)]
@@ -185,6 +186,18 @@ class Solver:
 
     def set_graph(self, on):
         self._check(load().kaos_set_graph(self.h, int(on)))
+
+    def init_particles(self, tube, counts, tail_fraction=0.0, kappa=3.0,
+                       tail_T=0.0, seed=20261203):
+        """Generate the initial ions of one tube on the device (counts per
+        cell; Maxwellian at TsG, optional kappa tail)."""
+        from .model_input import KaosInit
+        c = np.ascontiguousarray(counts, dtype=np.int64)
+        ini = KaosInit()
+        ini.counts = c.ctypes.data_as(C.POINTER(C.c_int64))
+        ini.tail_fraction, ini.kappa, ini.tail_T, ini.seed = (
+            float(tail_fraction), float(kappa), float(tail_T), int(seed))
+        self._check(load().kaos_init_particles(self.h, int(tube), C.addressof(ini)))
 
     def set_ena_grid(self, vg):
         """ENA velocity grid: Vp edges = vg.e1, Vphi = vg.e2, Vq = vg.epar."""

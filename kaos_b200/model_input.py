@@ -81,6 +81,12 @@ class KaosTube(C.Structure):
     ]
 
 
+class KaosInit(C.Structure):
+    """ctypes mirror of ``kaos_init_c``."""
+    _fields_ = [("counts", C.POINTER(C.c_int64)), ("tail_fraction", C.c_double),
+                ("kappa", C.c_double), ("tail_T", C.c_double), ("seed", C.c_uint64)]
+
+
 class KaosVGrid(C.Structure):
     """ctypes mirror of ``kaos_vgrid_c``."""
     _fields_ = [("n1", C.c_int32), ("n2", C.c_int32), ("npar", C.c_int32),

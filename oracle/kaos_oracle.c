@@ -1340,6 +1340,68 @@ int orc_load(orc *o, const double *q, const double *vpar, const double *v1,
   return 0;
 }
 
+/* Initial-ion generator of kaos_init_particles (test input synthesis, the
+ * same draws as the device generator): counts[k] ions in cell k, q uniform
+ * over the middle 96 % of the cell, isotropic Maxwellian at TsG or, with
+ * probability tail_fraction, an isotropic kappa distribution of temperature
+ * tail_T drawn as a Student-t vector of nu = 2 kappa - 1 degrees of freedom
+ * (covariance nu/(nu-2) s^2 = kT/m).  Philox (seed, ion index, 0,
+ * KAOS_RNG_INIT << 24 | sub): sub 0 = (position, population) uniforms,
+ * sub 1.. = Box-Muller pairs.  Then loaded as orc_load does. */
+static void init_pair(uint64_t seed, uint64_t id, uint32_t sub, double *a,
+                      double *b) {
+  kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), 0u,
+                             (KAOS_RNG_INIT << 24) | sub, seed);
+  double u1 = kaos_u01(w.v[0], w.v[1]), u2 = kaos_u01(w.v[2], w.v[3]);
+  double R = sqrt(-2.0 * log(u1));
+  *a = R * cos(2.0 * PI * u2);
+  *b = R * sin(2.0 * PI * u2);
+}
+
+int orc_init(orc *o, const int64_t *counts, double tail_fraction, double kappa,
+             double tail_T, uint64_t seed) {
+  int64_t n = 0;
+  for (int k = 0; k < o->nq; ++k)
+    n += counts[k];
+  double *q = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+  double *vp = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+  double *v1 = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+  double *v2 = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+  const int nu = (int)llround(2.0 * kappa - 1.0);
+  const double st = sqrt(KB * tail_T / o->P.ms * (double)(nu - 2) / (double)nu);
+  int64_t j = 0;
+  for (int k = 0; k < o->nq; ++k)
+    for (int64_t c = 0; c < counts[k]; ++c, ++j) {
+      kaos_u32x4 w = kaos_philox((uint32_t)j, (uint32_t)((uint64_t)j >> 32), 0u,
+                                 (KAOS_RNG_INIT << 24), seed);
+      double upos = kaos_u01(w.v[0], w.v[1]), upop = kaos_u01(w.v[2], w.v[3]);
+      q[j] = o->qGL[k] + (0.02 + 0.96 * upos) * (o->qGH[k] - o->qGL[k]);
+      int tail = upop < tail_fraction;
+      double g[66];
+      int ng = 3 + (tail ? nu : 0);
+      for (int m = 0; m < ng; m += 2)
+        init_pair(seed, (uint64_t)j, (uint32_t)(1 + m / 2), &g[m], &g[m + 1]);
+      double f;
+      if (!tail) {
+        f = sqrt(KB * o->TsG[k] / o->P.ms);
+      } else {
+        double W = 0.0;
+        for (int m = 0; m < nu; ++m)
+          W = W + g[3 + m] * g[3 + m];
+        f = st / sqrt(W / (double)nu);
+      }
+      vp[j] = f * g[0];
+      v1[j] = f * g[1];
+      v2[j] = f * g[2];
+    }
+  int rc = orc_load(o, q, vp, v1, v2, n);
+  free(q);
+  free(vp);
+  free(v1);
+  free(v2);
+  return rc;
+}
+
 int orc_set_fields(orc *o, const double *EA) {
   if (!EA) {
     o->have_import = 0;

@@ -34,6 +34,7 @@ def lib():
         L.orc_set_fields.argtypes = [vp, vp]
         L.orc_set_literal.argtypes = [vp, C.c_int]
         L.orc_set_ena_grid.argtypes = [vp, vp]
+        L.orc_init.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, C.c_uint64]
         L.orc_step.argtypes = [vp, C.c_int64]
         L.orc_count.restype = C.c_int64
         L.orc_count.argtypes = [vp, vp]
@@ -76,6 +77,12 @@ class Oracle:
     def load(self, q, vpar, v1, v2):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (q, vpar, v1, v2)]
         lib().orc_load(self.h, *[_p(a) for a in arrs], len(arrs[0]))
+
+    def init(self, counts, tail_fraction=0.0, kappa=3.0, tail_T=0.0, seed=20261203):
+        """The initial-ion generator of kaos_init_particles, then load."""
+        c = np.ascontiguousarray(counts, dtype=np.int64)
+        lib().orc_init(self.h, _p(c), float(tail_fraction), float(kappa),
+                       float(tail_T), int(seed))
 
     def set_fields(self, EA):
         self._EA = None if EA is None else np.ascontiguousarray(EA, dtype=np.float64)

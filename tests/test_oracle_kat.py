@@ -249,3 +249,29 @@ def test_single_bin_cell_moments():
     assert o.moments(KAOS_M1PAR)[5] == vc
     np.testing.assert_allclose(o.moments(KAOS_M2PAR)[5], (mi.ms / 2.0) * vc * vc,
                                rtol=1e-13)
+
+
+def test_initial_ion_generator_distributions():
+    """The initial-ion generator (shared draws with kaos_init_particles):
+    per-cell counts, positions inside their cells, a Maxwellian core at TsG
+    and a kappa tail whose variance is kT/m with heavier tails than a
+    Gaussian."""
+    from kaos_b200.model_input import MO
+    mi, spec, tube, vg = grids.config_small(n_particles=30000, three_d=True)
+    counts = tube._counts
+    T_tail = 5.0 * 1.602e-19 / KB
+    o = Oracle(mi, tube, vg)
+    o.init(counts, tail_fraction=0.0, seed=11)
+    p = o.particles()
+    assert len(p["q"]) == counts.sum()
+    # every ion inside the cell it was generated for, in cell order
+    np.testing.assert_array_equal(p["qind"], np.repeat(np.arange(tube.nq), counts))
+    var = KB * tube.TsG[0] / MO
+    for k in ("vpar", "vperp1", "vperp2"):
+        assert abs(np.var(p[k]) / var - 1) < 0.03, k
+    o2 = Oracle(mi, tube, vg)
+    o2.init(counts, tail_fraction=1.0, kappa=3.0, tail_T=T_tail, seed=11)
+    v = o2.particles()["vpar"]
+    assert abs(np.var(v) / (KB * T_tail / MO) - 1) < 0.15
+    kurt = np.mean(v ** 4) / np.var(v) ** 2
+    assert kurt > 4.0  # Student-t with 5 dof: kurtosis 9; Gaussian: 3
