@@ -150,6 +150,26 @@ def run_ours(args, precision, graph=False, ndatfac=50, steps=None):
                 launch=s.launch())
 
 
+def run_large(args, precision, steps):
+    """The large single tube (L=6, 512 cells, 64x64x96, 1e8 O+ with a kappa
+    tail, generated on the device), mixed path from CUDA graphs or FP64."""
+    from kaos_b200 import grids
+    from kaos_b200.lib import Solver
+    from kaos_b200.model_input import KAOS_PREC_MIXED
+    mi, spec, tube, vg = grids.config_c3(args.large_particles, precision=precision)
+    s = Solver(mi, [tube], vg)
+    s.init_particles(0, tube._counts, seed=20261203, **grids.C3_TAIL)
+    s.set_graph(precision == KAOS_PREC_MIXED)
+    s.step(args.warmup)
+    n0, _ = s.count()
+    s.step(steps)
+    ms, _ = s.timing()
+    n1, _ = s.count()
+    s.close()
+    n = 0.5 * (n0 + n1)
+    return dict(value=n * steps / (ms * 1e-3), ms=ms / steps, n=n)
+
+
 def mixed_moment_error(s32, s64):
     """Norm-wise relative difference max|m32 - m64| / max|m64| per moment."""
     from kaos_b200 import model_input as M
@@ -186,7 +206,7 @@ def run_e2e(args, precision):
         s.step(1)
         for m in range(8):
             d2h += s.moments(m).nbytes
-    p = s.particles()
+    p = s.state()
     d2h += sum(v.nbytes for v in p.values())
     dt = time.perf_counter() - t0
     n = len(p["q"])
@@ -295,6 +315,8 @@ def main():
     ap.add_argument("--no-heating", action="store_true")
     ap.add_argument("--no-collisions", dest="collisions", action="store_false")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--large-particles", type=int, default=100_000_000,
+                    help="ions of the large single-tube line (0: skip it)")
     ap.add_argument("--only", default="all", choices=["all", "mixed"],
                     help="mixed: time the mixed path alone (for profiling)")
     ap.add_argument("--launch", default=None,
@@ -356,6 +378,20 @@ def main():
     achieved = mixed_bytes * r32["n"] / (r32["push_ms"] * 1e-3) / 1e9
     peak, peak_kind = peaks()
     e2e = None
+    large = None
+    if full and args.large_particles > 0:
+        lsteps = min(args.steps, 100)
+        l32 = run_large(args, KAOS_PREC_MIXED, lsteps)
+        l64 = run_large(args, KAOS_PREC_FP64, lsteps)
+        large = {"workload": "large single tube: L=6, 512 cells 800 km to the equator, "
+                             f"3D grid 64x64x96, {int(l32['n'])} O+ (90 % 0.3 eV Maxwellian "
+                             "+ 10 % kappa=3 5 eV tail, generated on the device), heating "
+                             "and collisions on, LB injection, dt 5 ms",
+                 "steps": lsteps, "mixed": l32["value"] * world,
+                 "mixed_ms_per_step": l32["ms"], "fp64": l64["value"] * world,
+                 "fp64_ms_per_step": l64["ms"],
+                 "mixed_over_fp64": l32["value"] / l64["value"],
+                 "note": "mixed path replayed from CUDA graphs"}
     if not args.skip_e2e and full:
         e2e = run_e2e(args, KAOS_PREC_MIXED)
     cpu = cpu_baseline(args) if (rank == 0 and world == 1 and full) else None
@@ -385,6 +421,7 @@ def main():
                 "push_ms": r64["push_ms"]},
             "mixed_over_fp64": value / (r64["value"] * world) if full else None,
             "mixed_push_ms": r32["push_ms"],
+            "large": large,
             "moment_error_vs_fp64": moment_error,
             "graph": None if not full else {
                 "value": rg["value"] * world, "ms_per_step": rg["ms"] / args.steps,

@@ -1046,72 +1046,37 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
   if (h->n != 0) return fail(h, KAOS_ERR_STATE, "particles must be loaded before the first step");
   const TubeD &T = h->th[tube];
   if (n > T.cap) return fail(h, KAOS_ERR_CAPACITY, "tube %d: %lld particles exceed capacity %lld", tube, (long long)n, (long long)T.cap);
-  const double *qGL = h->host_cells[0].data() + T.coff;
-  const double *qGH = h->host_cells[1].data() + T.coff;
-  std::vector<double> E(T.nq + 1);
-  for (int k = 0; k < T.nq; ++k) E[k] = T.sgn * qGL[k];
-  E[T.nq] = T.sgn * qGH[T.nq - 1];
-  std::vector<int32_t> qind(n), vb(n), cell(n);
-  std::vector<double> a(n), b(n), qq(n);
-  std::vector<float> fo(n), f1(n), f2(n), f3(n), fq(n);
-  std::vector<uint64_t> id(n);
-  for (int64_t j = 0; j < n; ++j) {
-    double qj = q[j];
-    // KineticSolverASub q clamp (_8_0_0_1_KineticSolverA.f90:55-65)
-    if (T.sgn * qj <= E[0]) qj = qGL[0];
-    else if (T.sgn * qj > E[T.nq]) qj = qGH[T.nq - 1];
-    qq[j] = qj;
-    double s = T.sgn * qj;
-    int c;
-    if (s < E[0]) c = BELOW;
-    else if (s > E[T.nq]) c = ABOVE;
-    else c = (int)(std::lower_bound(E.begin() + 1, E.end(), s) - E.begin()) - 1;
-    qind[j] = c;
-    id[j] = (uint64_t)j;
-    double v1 = vperp1[j], v2 = vperp2 ? vperp2[j] : 0.0;
-    auto bin = [](const double *e, int nb, double v) {
-      if (!(v >= e[0] && v <= e[nb])) return -1;
-      return (int)(std::lower_bound(e + 1, e + nb + 1, v) - (e + 1));
-    };
-    int bp = bin(h->vg.epar, h->vg.npar, vpar[j]);
-    int b1 = bin(h->vg.e1, h->vg.n1, std::sqrt(v1 * v1 + v2 * v2));
-    vb[j] = ((b1 + 1) << 16) | (bp + 1);
-    if (h->mixed) {
-      int cp = c >= 0 ? c : (c == BELOW ? 0 : T.nq - 1);
-      cell[j] = cp;
-      fo[j] = (float)((qj - qGL[cp]) / (qGH[cp] - qGL[cp]));
-      f1[j] = (float)vpar[j];
-      f2[j] = (float)v1;
-      f3[j] = (float)v2;
-      fq[j] = (float)qj;
-    } else {
-      host_rho_z(qj, T.pG, &a[j], &b[j]);
+  if (n > 0) {
+    // the caller's arrays go to a device staging area; k_load derives the
+    // per-ion state there (clamp, cell search, bins, positions)
+    const int na = vperp2 ? 4 : 3;
+    double *stage = nullptr;
+    if (cudaMalloc(&stage, (size_t)na * n * sizeof(double)) != cudaSuccess)
+      return fail(h, KAOS_ERR_CUDA, "cudaMalloc of the load staging area failed");
+    const double *src[4] = {q, vpar, vperp1, vperp2};
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < na && e == cudaSuccess; ++k)
+      e = cudaMemcpy(stage + (size_t)k * n, src[k], n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_vg, &h->vg, sizeof(VGridC));
+    if (e == cudaSuccess) {
+      LoadArgs a{};
+      a.T = T;
+      a.q = stage;
+      a.vpar = stage + n;
+      a.v1 = stage + 2 * n;
+      a.v2 = vperp2 ? stage + 3 * n : nullptr;
+      a.n = n;
+      a.ion = h->ion[h->cur];
+      a.ct = h->ct;
+      a.mixed = h->mixed;
+      const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 32);
+      k_load<<<grid, 256, (size_t)(T.nq + 1) * sizeof(double)>>>(a);
+      e = cudaGetLastError();
     }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(stage);
+    if (e != cudaSuccess) return fail(h, KAOS_ERR_CUDA, "load: %s", cudaGetErrorString(e));
   }
-  Ions &I = h->ion[h->cur];
-  const int64_t o = T.off;
-#define H2D(dst, src, T_) CK(cudaMemcpy((dst) + o, (src), n * sizeof(T_), cudaMemcpyHostToDevice))
-  if (h->mixed) {
-    H2D(I.cell, cell.data(), int32_t);
-    H2D(I.off, fo.data(), float);
-    H2D(I.fvpar, f1.data(), float);
-    H2D(I.fv1, f2.data(), float);
-    H2D(I.fv2, f3.data(), float);
-    H2D(I.fqk4, fq.data(), float);
-  } else {
-    std::vector<double> v2v(n);
-    for (int64_t j = 0; j < n; ++j) v2v[j] = vperp2 ? vperp2[j] : 0.0;
-    H2D(I.rho, a.data(), double);
-    H2D(I.z, b.data(), double);
-    H2D(I.vpar, vpar, double);
-    H2D(I.v1, vperp1, double);
-    H2D(I.v2, v2v.data(), double);
-    H2D(I.qk4, qq.data(), double);
-  }
-  H2D(I.qind, qind.data(), int32_t);
-  if (I.vb) H2D(I.vb, vb.data(), int32_t);
-  H2D(I.id, id.data(), uint64_t);
-#undef H2D
   int64_t nl = n;
   uint64_t nid = (uint64_t)n;
   CK(cudaMemcpy(h->d_nlive + tube, &nl, sizeof(int64_t), cudaMemcpyHostToDevice));

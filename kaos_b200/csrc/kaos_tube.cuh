@@ -663,6 +663,47 @@ struct InitArgs {
   int mixed;
 };
 
+// One new ion j of tube T in cell c at q with field-aligned velocity: the
+// per-ion state every path starts from (Qindk1, id, 2D bins; mixed: cell,
+// offset and FP32 velocities; FP64: meridian-plane position from the
+// quartic root by Newton from the cell's linear guess, converged to FP64).
+__device__ __forceinline__ void store_ion(const Ions &I, const TubeD &T,
+                                          const CellTables &ct, int64_t j,
+                                          int c, double q, double vpar,
+                                          double v1, double v2, int mixed) {
+  const int64_t k = T.off + j, g = T.coff + c;
+  const double qL = ct.qGL[g], qH = ct.qGH[g];
+  I.qind[k] = c;
+  I.id[k] = (uint64_t)j;
+  if (I.vb) {
+    const int bp = vbin(c_vg.epar, c_vg.npar, vpar);
+    const int b1 = vbin(c_vg.e1, c_vg.n1, sqrt(v1 * v1 + v2 * v2));
+    I.vb[k] = ((b1 + 1) << 16) | (bp + 1);
+  }
+  if (mixed) {
+    I.cell[k] = c;
+    I.off[k] = (float)((q - qL) / (qH - qL));
+    I.fvpar[k] = (float)vpar;
+    I.fv1[k] = (float)v1;
+    I.fv2[k] = (float)v2;
+    I.fqk4[k] = (float)q;
+  } else {
+    const double fr = (q - qL) / (qH - qL);
+    const double u0 = ct.uL[g] + fr * (ct.uH[g] - ct.uL[g]);
+    const double u = quartic_newton(q, 1.0 / T.pG, u0, 6);
+    const double st = sqrt(u / T.pG), ctv = q * u * u, r = u * RE;
+    double rho = r * st, z = r * ctv;
+    if (fabs(rho) < 1e-6) rho = 0.0;
+    if (fabs(z) < 1e-6) z = 0.0;
+    I.rho[k] = rho;
+    I.z[k] = z;
+    I.vpar[k] = vpar;
+    I.v1[k] = v1;
+    I.v2[k] = v2;
+    I.qk4[k] = q;
+  }
+}
+
 __device__ __forceinline__ void init_pair(uint64_t seed, uint64_t id,
                                           uint32_t sub, double &a, double &b) {
   kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), 0u,
@@ -686,10 +727,10 @@ __global__ void k_init(InitArgs a) {
     }
     const int c = lo;
     const int64_t g = T.coff + c;
+    const double qL = a.ct.qGL[g], qH = a.ct.qGH[g];
     kaos_u32x4 w = kaos_philox((uint32_t)j, (uint32_t)((uint64_t)j >> 32), 0u,
                                (KAOS_RNG_INIT << 24), a.seed);
     const double upos = kaos_u01(w.v[0], w.v[1]), upop = kaos_u01(w.v[2], w.v[3]);
-    const double qL = a.ct.qGL[g], qH = a.ct.qGH[g];
     const double q = __dadd_rn(qL, __dmul_rn(__dadd_rn(0.02, __dmul_rn(0.96, upos)),
                                              __dadd_rn(qH, -qL)));
     const bool tail = upop < a.tail_fraction;
@@ -710,39 +751,39 @@ __global__ void k_init(InitArgs a) {
       f = a.s_tail / sqrt(W / (double)a.nu);
     }
     const double vpar = __dmul_rn(f, g0), v1 = __dmul_rn(f, g1), v2 = __dmul_rn(f, g2);
-    const int64_t k = T.off + j;
-    Ions I = a.ion;
-    I.qind[k] = c;
-    I.id[k] = (uint64_t)j;
-    if (I.vb) {
-      const int bp = vbin(c_vg.epar, c_vg.npar, vpar);
-      const int b1 = vbin(c_vg.e1, c_vg.n1, sqrt(v1 * v1 + v2 * v2));
-      I.vb[k] = ((b1 + 1) << 16) | (bp + 1);
-    }
-    if (a.mixed) {
-      I.cell[k] = c;
-      I.off[k] = (float)((q - qL) / (qH - qL));
-      I.fvpar[k] = (float)vpar;
-      I.fv1[k] = (float)v1;
-      I.fv2[k] = (float)v2;
-      I.fqk4[k] = (float)q;
-    } else {
-      // position on the meridian plane: quartic root by Newton from the
-      // cell's linear guess (converged to FP64 precision)
-      const double fr = (q - qL) / (qH - qL);
-      const double u0 = a.ct.uL[g] + fr * (a.ct.uH[g] - a.ct.uL[g]);
-      const double u = quartic_newton(q, 1.0 / T.pG, u0, 6);
-      const double st = sqrt(u / T.pG), ctv = q * u * u, r = u * RE;
-      double rho = r * st, z = r * ctv;
-      if (fabs(rho) < 1e-6) rho = 0.0;
-      if (fabs(z) < 1e-6) z = 0.0;
-      I.rho[k] = rho;
-      I.z[k] = z;
-      I.vpar[k] = vpar;
-      I.v1[k] = v1;
-      I.v2[k] = v2;
-      I.qk4[k] = q;
-    }
+    store_ion(a.ion, T, a.ct, j, c, q, vpar, v1, v2, a.mixed);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// kaos_load_particles on the device: the KineticSolverASub q clamp
+// (_8_0_0_1_KineticSolverA.f90:55-65), the cell of each ion and its derived
+// state, from the caller's (q, V||, Vperp1, Vperp2) copied to the device.
+struct LoadArgs {
+  TubeD T;
+  const double *q, *vpar, *v1, *v2;  // v2 may be null (2D grid)
+  int64_t n;
+  Ions ion;
+  CellTables ct;
+  int mixed;
+};
+
+__global__ void k_load(LoadArgs a) {
+  extern __shared__ double E[];  // oriented cell edges [nq + 1]
+  const TubeD &T = a.T;
+  const double *qGL = a.ct.qGL + T.coff, *qGH = a.ct.qGH + T.coff;
+  for (int k = threadIdx.x; k <= T.nq; k += blockDim.x)
+    E[k] = (k < T.nq) ? T.sgn * qGL[k] : T.sgn * qGH[T.nq - 1];
+  __syncthreads();
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    double q = a.q[j];
+    const double s = T.sgn * q;
+    if (s <= E[0]) q = qGL[0];
+    else if (s > E[T.nq]) q = qGH[T.nq - 1];
+    const int c = cell_search(E, T.nq, T.sgn * q);
+    store_ion(a.ion, T, a.ct, j, c, q, a.vpar[j], a.v1[j], a.v2 ? a.v2[j] : 0.0,
+              a.mixed);
   }
 }
 

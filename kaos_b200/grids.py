@@ -16,7 +16,7 @@ import dataclasses
 import numpy as np
 
 from .model_input import (KB, MO, PI, RE, GG, ME, ModelInput, Tube, VGrid,
-                          KAOS_PREC_FP64)
+                          KAOS_PREC_FP64, KAOS_PREC_MIXED)
 
 
 def dipole_q_to_rtheta(q, p):
@@ -224,4 +224,24 @@ def config_c2(n_particles=10_000_000, heating=True, collisions=True,
                     neut_n0=1e14 if collisions else 0.0, neut_H=60e3)
     tube = make_tube(spec, mi)
     vg = make_vgrid(True, 48, 48, 64, 30e3)
+    return mi, spec, tube, vg
+
+
+# kappa tail of the large single-tube workload
+C3_TAIL = dict(tail_fraction=0.1, kappa=3.0, tail_T=5.0 * 1.602e-19 / KB)
+
+
+def config_c3(n_particles=100_000_000, precision=KAOS_PREC_MIXED, ndatfac=50):
+    """Large single tube: L=6, 512 cells from 800 km to the equator
+    (|q| >= 1e-3), 3D grid 64x64x96, 1e8 O+ (90 % 0.3 eV Maxwellian core +
+    10 % kappa = 3, 5 eV tail: C3_TAIL with kaos_init_particles), heating
+    (chi 1.7, 1e-3 eV/s at the base) and O neutrals (1e14 m^-3, H 60 km) on,
+    LB injection, UB outflow removal, dt 0.005 s."""
+    mi = ModelInput(h=0.005, ndatfac=ndatfac, ION2VPERPflag=1, ICRflag=1,
+                    QEXCHANGEflag=1, precision=precision)
+    spec = TubeSpec(L=6.0, nq=512, alt_lb=800e3, n_particles=n_particles,
+                    q_ub=1e-3, heat_rate_eV_s=1e-3, chi=1.7, neut_n0=1e14,
+                    neut_H=60e3)
+    tube = make_tube(spec, mi)
+    vg = make_vgrid(True, 64, 64, 96, 40e3)
     return mi, spec, tube, vg

@@ -153,6 +153,15 @@ class Solver:
         self._check(load().kaos_get_counts(self.h, tube, _p(out), n))
         return out
 
+    def state(self, tube=0):
+        """The ions' field-line state: q, V||, Vperp1, Vperp2, Qindk1."""
+        ni, _ = self.count(tube)
+        q, vp, v1, v2 = (np.zeros(ni) for _ in range(4))
+        qi = np.zeros(ni, dtype=np.int32)
+        self._check(load().kaos_get_particles(self.h, tube, _p(q), _p(vp), _p(v1),
+                                              _p(v2), _p(qi), ni))
+        return dict(q=q, vpar=vp, vperp1=v1, vperp2=v2, qind=qi)
+
     def particles(self, tube=0):
         ni, _ = self.count(tube)
         q, vp, v1, v2 = (np.zeros(ni) for _ in range(4))
