@@ -124,7 +124,7 @@ typedef struct kaos_params_c {
  * kaos_create.  Optional tables may be NULL (zeros are used).
  */
 typedef struct kaos_tube_c {
-  int32_t nq;              /* NqUB - NqLB + 1                              */
+  int32_t nq;              /* NqUB - NqLB + 1, in [6, 2048]                */
   int32_t capacity;        /* max particles (incl. injection headroom)     */
   double pG;               /* pGCGT  (field-line p = L shell) [RE]         */
   double phiG;             /* phiGCGT longitude [rad]                      */

@@ -26,6 +26,9 @@ namespace {
 constexpr int PUSH_THREADS = 256;
 constexpr int PUSH_ITEMS = 8;
 constexpr int BC_THREADS = 256;
+// cells per tube: the per-cell tables of a tube live in shared memory (the
+// mixed push holds 84 bytes per cell, the collision-count kernel 64)
+constexpr int MAX_CELLS = 2048;
 // push work-item sizes the autotuner tries (ions per item); an item's ions
 // lie in one charge-exchange selection chunk
 constexpr int NCHUNKS = 3;
@@ -786,11 +789,11 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   int64_t poff = 0, coff = 0, moff = 0, hoff = 0, eoff = 0;
   for (int t = 0; t < ntubes; ++t) {
     const kaos_tube_c &T = tubes[t];
-    if (T.nq < 6 || T.nq > 4096 || T.capacity < 1 || !T.qGL || !T.qGH ||
+    if (T.nq < 6 || T.nq > MAX_CELLS || T.capacity < 1 || !T.qGL || !T.qGH ||
         !T.qGC || !T.hqC || !T.dqC || !T.d3xC || !T.rGC || !T.thetaGC ||
         !T.ellGC || !T.TeG || !T.TsG) {
       *out = h;
-      return fail(h, KAOS_ERR_PARAM, "tube %d: nq must be in [6, 4096], capacity > 0, tables non-NULL", t);
+      return fail(h, KAOS_ERR_PARAM, "tube %d: nq must be in [6, %d], capacity > 0, tables non-NULL", t, MAX_CELLS);
     }
     for (int k = 0; k + 1 < T.nq; ++k)
       if (T.qGH[k] != T.qGL[k + 1]) {
@@ -1032,6 +1035,19 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
         (rc = dalloc(h, &h->d_cxc, cxt.size() * (size_t)max_nq(h))) ||
         (rc = dalloc(h, &h->d_cxo, cxt.size() * (size_t)max_nq(h))))
       return rc;
+  }
+  // kernels whose per-tube shared tables may exceed the default 48 KB
+  {
+    const size_t nq = (size_t)max_nq(h);
+    const std::pair<const void *, size_t> big[] = {
+        {(const void *)k_collision_counts, 8 * nq * sizeof(double)},
+        {(const void *)k_cx_convert, 9 * nq * sizeof(unsigned)},
+        {(const void *)k_fields, 3 * nq * sizeof(double)},
+        {(const void *)k_push_ena, (nq + 1) * sizeof(double)},
+        {(const void *)k_load, (nq + 1) * sizeof(double)}};
+    for (const auto &b : big)
+      if (b.second > 48 * 1024)
+        CK(cudaFuncSetAttribute(b.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.second));
   }
   CK(cudaDeviceSynchronize());
   return KAOS_OK;

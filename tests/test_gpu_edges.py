@@ -1,0 +1,112 @@
+"""Edge cases of the CUDA path against the oracle: the largest tube (2048
+cells) and velocity grid (128 bins per axis) the library accepts, and
+batches holding an empty entry and a single-ion entry (injection fills
+the empty one)."""
+import numpy as np
+import pytest
+
+from kaos_b200 import build as kbuild
+from kaos_b200 import grids
+from kaos_b200.grids import TubeSpec, make_tube, make_vgrid
+from kaos_b200.lib import KaosError, Solver
+from kaos_b200.model_input import (KAOS_M0, KAOS_M1PAR, KAOS_M2, KAOS_M2PAR,
+                                   KAOS_PREC_MIXED, ModelInput)
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TRAJ_TOL = 1e-12
+MOM_TOL = 1e-10
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _build():
+    kbuild.build()
+
+
+def rel_norm(a, b):
+    scale = max(np.max(np.abs(b)), 1e-300)
+    return np.max(np.abs(a - b)) / scale
+
+
+def _compare(s, k, o):
+    assert s.count(k) == o.count(), k
+    po, ps = o.particles(), s.particles(k)
+    for key in ("z", "vpar", "vperp1", "vperp2"):
+        if len(po[key]):
+            assert rel_norm(ps[key], po[key]) < TRAJ_TOL, (k, key)
+    np.testing.assert_array_equal(s.counts(k), o.counts())
+    for m in (KAOS_M0, KAOS_M1PAR, KAOS_M2, KAOS_M2PAR):
+        assert rel_norm(s.moments(m, k), o.moments(m)) < MOM_TOL, (k, m)
+
+
+def _run_one(mi, spec, vg, steps, seed=1):
+    t = make_tube(spec, mi)
+    init = grids.initial_particles(t, spec, mi, seed=seed)
+    s = Solver(mi, [t], vg)
+    s.load(0, *init)
+    s.step(steps)
+    o = Oracle(mi, t, vg)
+    o.load(*init)
+    o.step(steps)
+    return s, o
+
+
+def test_largest_tube_2048_cells():
+    mi = ModelInput(h=0.01, ndatfac=3, ION2VPERPflag=1, ICRflag=1, QEXCHANGEflag=1)
+    spec = TubeSpec(L=4.0, nq=2048, n_particles=20000, q_ub=1e-3, H=900e3,
+                    heat_rate_eV_s=5.0, neut_n0=3e18, neut_H=300e3)
+    vg = make_vgrid(True, 16, 16, 24, 8e3)
+    s, o = _run_one(mi, spec, vg, 7)
+    _compare(s, 0, o)
+    # the mixed path runs the same tube (shared tables of 2048 cells)
+    mi.precision = KAOS_PREC_MIXED
+    t = make_tube(spec, mi)
+    init = grids.initial_particles(t, spec, mi, seed=1)
+    m = Solver(mi, [t], vg)
+    m.load(0, *init)
+    m.step(7)
+    assert rel_norm(m.moments(KAOS_M0), o.moments(KAOS_M0)) < 2e-2
+
+
+def test_largest_velocity_grid_128_bins():
+    mi = ModelInput(h=0.01, ndatfac=3, ION2VPERPflag=1)
+    spec = TubeSpec(L=4.0, nq=8, n_particles=5000, q_ub=0.3, H=600e3)
+    vg = make_vgrid(True, 128, 128, 128, 6e3)
+    s, o = _run_one(mi, spec, vg, 7)
+    _compare(s, 0, o)
+
+
+def test_limits_rejected():
+    mi = ModelInput(h=0.01, ndatfac=3, ION2VPERPflag=1)
+    vg = make_vgrid(True, 16, 16, 24, 8e3)
+    t = make_tube(TubeSpec(nq=2049, n_particles=1000, q_ub=1e-3), mi)
+    with pytest.raises(KaosError):
+        Solver(mi, [t], vg)
+    t = make_tube(TubeSpec(nq=16, n_particles=1000, q_ub=0.2), mi)
+    with pytest.raises(KaosError):
+        Solver(mi, [t], make_vgrid(True, 130, 16, 24, 8e3))
+
+
+def test_empty_and_single_ion_entries():
+    mi = ModelInput(h=0.01, ndatfac=3, ION2VPERPflag=1, ICRflag=1, QEXCHANGEflag=1)
+    vg = make_vgrid(True, 16, 16, 24, 8e3)
+    common = dict(L=4.0, nq=20, q_ub=0.15, H=600e3, heat_rate_eV_s=5.0,
+                  neut_n0=3e18, neut_H=300e3)
+    specs = [TubeSpec(n_particles=600, **common), TubeSpec(n_particles=600, **common),
+             TubeSpec(n_particles=600, **common)]
+    tubes = [make_tube(sp, mi) for sp in specs]
+    tubes[0].nsnormCLB = 12.0  # the empty entry fills by injection
+    full = grids.initial_particles(tubes[2], specs[2], mi, seed=3)
+    inits = [tuple(np.zeros(0) for _ in range(4)),
+             tuple(a[:1].copy() for a in full), full]
+    s = Solver(mi, tubes, vg)
+    for k in range(3):
+        s.load(k, *inits[k])
+    s.step(10)
+    for k in range(3):
+        o = Oracle(mi, tubes[k], vg)
+        o.load(*inits[k])
+        o.step(10)
+        _compare(s, k, o)
+    assert s.count(0)[0] > 0
