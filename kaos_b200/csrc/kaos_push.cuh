@@ -230,7 +230,7 @@ __device__ __forceinline__ void gauss2_32(uint64_t seed, uint64_t id,
   kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), step,
                              stream << 24, seed);
   float u1 = kaos_u01f(w.v[0]), u2 = kaos_u01f(w.v[2]);
-  float R = sqrtf(-2.0f * __logf(u1)), sn, cs;
+  float R = sqrtf(fmaxf(-2.0f * __logf(u1), 0.0f)), sn, cs;
   __sincosf(6.2831853071795865f * u2, &sn, &cs);
   g1 = R * cs;
   g2 = R * sn;
@@ -316,6 +316,53 @@ __device__ __forceinline__ void heat(const PushArgs &a, uint32_t step,
     v1 = v1 + k1 * G1;
     v2 = v2 + k2 * G2;
   }
+}
+
+// Hardware base-2 logarithm and exponential (MUFU, flush-to-zero).
+__device__ __forceinline__ float lg2f(float x) {
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float ex2f(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// The stochastic WaveHeatingSub kick in the mixed push, in log form: the
+// product K_i x^(-c_i) (Om s)^(1/2) of heat() is one base-2 exponential,
+//   kick_i = K_i G_i 2^(-c_i log2(Om/Om0) + log2(Om |V||| / sum ds)/4 - pen),
+// the branch test h Om s <= 2 pi becomes Om |V||| / sum ds <= (2 pi/h)^2 and
+// Sigma^(-3/2) for lambda != 0 becomes pen = 1.5 log2 Sigma when Sigma >= 1.
+// The Gaussians are the same Box-Muller pair of one Philox draw as
+// gauss2_32.  hk: K1 K2 c1 c2 log2(1/Om0) lambda.
+__device__ __forceinline__ void heat32(const PushArgs &a, uint32_t step,
+                                       const float *hk, uint64_t id,
+                                       float invsumds, float ylim, float Om,
+                                       float vabs, float &v1, float &v2) {
+  const float y = Om * vabs * invsumds;  // (Om s)^2
+  if (!(y <= ylim)) return;
+  const float LOm = lg2f(Om);
+  float b = 0.25f * lg2f(y);
+  if (hk[5] != 0.0f) {  // Sigma = 2 pi |Vperp| / (Om lambda)
+    const float ls = lg2f(6.2831853f * sqrtf(v1 * v1 + v2 * v2) / hk[5]) - LOm;
+    if (ls >= 0.0f) b -= 1.5f * ls;
+  }
+  const float lx = LOm + hk[4];
+  const float e1 = ex2f(fmaf(-hk[2], lx, b));
+  const float e2 = (hk[3] == hk[2]) ? e1 : ex2f(fmaf(-hk[3], lx, b));
+  kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), step,
+                             KAOS_RNG_HEAT << 24, a.seed);
+  const float u1 = kaos_u01f(w.v[0]), u2 = kaos_u01f(w.v[2]);
+  // -2 ln u1 > 0; the hardware logarithm's absolute error (~2^-22) can give
+  // a tiny negative value for u1 just below 1
+  const float t = fmaxf(-1.38629436f * lg2f(u1), 1e-30f);
+  const float R = t * rsqrtf(t);
+  float sn, cs;
+  __sincosf(6.2831853f * u2, &sn, &cs);
+  v1 = fmaf(hk[0] * e1 * R, cs, v1);
+  v2 = fmaf(hk[1] * e2 * R, sn, v2);
 }
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0 by Newton from u0 (the
@@ -553,7 +600,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
         HK[6 * k + 1] = (float)a.ct.hK2[g];
         HK[6 * k + 2] = (float)a.ct.hc1[g];
         HK[6 * k + 3] = (float)a.ct.hc2[g];
-        HK[6 * k + 4] = (float)a.ct.hiom0[g];
+        HK[6 * k + 4] = a.icrcoh ? (float)a.ct.hiom0[g] : lg2f((float)a.ct.hiom0[g]);
         HK[6 * k + 5] = (float)a.ct.lambdaPerp[g];
       }
     }
@@ -568,6 +615,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
   const double ipG = 1.0 / T.pG;
   const float qs_ms = (float)(T.qs / T.ms);
   const float c_invOm = (float)(T.ms / (T.qs * MDIP));
+  const float ylim = (float)((2.0 * PI / a.h) * (2.0 * PI / a.h));
   // Software pipeline: the state of the next ion of this thread is loaded
   // before the current one is pushed, so its HBM latency overlaps the work.
   int n_c = DEAD;
@@ -650,8 +698,12 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
       const float Om = qs_ms * (float)MDIP * sl * ir3;
       const float invOm = c_invOm * (rf * rf * rf) * g1.isl;
       const float *hk = HK + 6 * qi;
-      const HeatC<float> hc{hk[0], hk[1], hk[2], hk[3], hk[4], hk[5]};
-      heat<float>(a, step, hc, pid, invsumds, Om, invOm, fabsf(vpar), v1n, v2n);
+      if (!a.icrcoh) {
+        heat32(a, step, hk, pid, invsumds, ylim, Om, fabsf(vpar), v1n, v2n);
+      } else {
+        const HeatC<float> hc{hk[0], hk[1], hk[2], hk[3], hk[4], hk[5]};
+        heat<float>(a, step, hc, pid, invsumds, Om, invOm, fabsf(vpar), v1n, v2n);
+      }
     }
     const float rf = (float)rho0, zf = (float)z0;
     const float VRr = vpar * g1.er, VRz = vpar * g1.ez;
