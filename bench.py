@@ -425,6 +425,7 @@ def main():
             "moment_error_vs_fp64": moment_error,
             "graph": None if not full else {
                 "value": rg["value"] * world, "ms_per_step": rg["ms"] / args.steps,
+                "push_launch": rg["launch"],
                 "note": "mixed path, steps replayed from CUDA graphs"},
             "cadence1": None if not full else {
                 "value": rc1["value"] * world,

@@ -303,6 +303,35 @@ int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode);
  * Vq <- Vpar, Vphi <- Vperp2, or Vperp1 on a 2D ion grid). */
 int kaos_set_ena_grid(kaos_handle *h, const kaos_vgrid_c *vg);
 
+/*
+ * One tube split across ranks (MPI ranks of the reference, one GPU each
+ * here): each rank holds a handle with the tube's full tables and its own
+ * share of the ions.  The reference sums every per-cell and per-bin count
+ * over the ranks (MPIReduceSumSub _9_MPIReduceSum.f90:25-55, called per bin
+ * from _8_3_1_IonParticleCounts.f90:396-407, :675-680) before the moments;
+ * here the handle calls `fn(ctx, buf, count, stream)` once per statistics
+ * step with ALL its binning accumulators in one device block of `count`
+ * uint32 counters (ion and ENA counts and marginals), after synchronising
+ * its stream.  The hook sums `buf` over the ranks in place (an NCCL
+ * all-reduce, kaos_b200/shard.py) and returns 0 when done.  While a hook is
+ * set, steps run without CUDA graphs.  fn = NULL removes it.
+ */
+typedef int (*kaos_reduce_fn)(void *ctx, uint32_t *buf, int64_t count,
+                              void *stream);
+int kaos_set_reduce(kaos_handle *h, kaos_reduce_fn fn, void *ctx);
+
+/* Rank `rank` of `nranks` holding a share of a split tube: of the
+ * nint(nuIonNeutPoiT) ions a cell converts to ENAs at a step (IonNeutral
+ * CollisionFrequencyBSub splits the count over ranks,
+ * _8_6_6_2_IonNeutralCollisionFrequencyB.f90), this rank converts
+ * floor((N + rank) / nranks), its first ones in index order. */
+int kaos_set_rank(kaos_handle *h, int32_t rank, int32_t nranks);
+
+/* Id of the first ion loaded into `tube` (default 0): ids key the random
+ * streams of each ion, so the shares of a split tube take disjoint ranges
+ * and draw the same numbers as the unsplit tube.  Set before loading. */
+int kaos_set_id_base(kaos_handle *h, int32_t tube, uint64_t base);
+
 /* The launch shape in use (after autotuning). */
 int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode);
 

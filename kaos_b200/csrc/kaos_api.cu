@@ -133,6 +133,13 @@ struct kaos_handle {
     int64_t launches = 0;
   };
   std::map<uint64_t, StepGraph> graphs;
+  // all binning accumulators in one block; optional cross-rank reduction
+  unsigned *acc_base = nullptr;
+  int64_t acc_len = 0;
+  kaos_reduce_fn reduce_fn = nullptr;
+  void *reduce_ctx = nullptr;
+  int rank = 0, nranks = 1;          // share of the charge-exchange counts
+  std::vector<uint64_t> id_base;     // first ion id per tube
   // push work items: (tube, chunk of ions) maps, one per candidate chunk
   struct WorkMap {
     int chunk = 0, n = 0;
@@ -322,19 +329,19 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
 
 int zero_accum(kaos_handle *h) {
   const int64_t nc = h->ncell;
-  CK(cudaMemsetAsync(h->acc.cnt, 0, nc * sizeof(unsigned), h->s));
-  CK(cudaMemsetAsync(h->acc.mpar, 0, nc * h->vg.npar * sizeof(unsigned), h->s));
-  CK(cudaMemsetAsync(h->acc.m1, 0, nc * h->vg.n1 * sizeof(unsigned), h->s));
-  if (h->three_d)
-    CK(cudaMemsetAsync(h->acc.m2, 0, nc * h->vg.n2 * sizeof(unsigned), h->s));
+  CK(cudaMemsetAsync(h->acc_base, 0, (size_t)h->acc_len * sizeof(unsigned), h->s));
   if (h->export_on && h->acc.hist)
     CK(cudaMemsetAsync(h->acc.hist, 0, nc * (int64_t)h->nv * sizeof(unsigned), h->s));
-  if (h->acc.ecnt) {
-    CK(cudaMemsetAsync(h->acc.ecnt, 0, nc * sizeof(unsigned), h->s));
-    CK(cudaMemsetAsync(h->acc.emp, 0, nc * MAXV * sizeof(unsigned), h->s));
-    CK(cudaMemsetAsync(h->acc.emq, 0, nc * MAXV * sizeof(unsigned), h->s));
-    CK(cudaMemsetAsync(h->acc.emph, 0, nc * MAXV * sizeof(unsigned), h->s));
-  }
+  return KAOS_OK;
+}
+
+// A tube split across ranks: the caller's hook sums the binning
+// accumulators of all ranks in place before the moments are taken.
+int reduce_accum(kaos_handle *h) {
+  if (!h->reduce_fn) return KAOS_OK;
+  CK(cudaStreamSynchronize(h->s));
+  const int rc = h->reduce_fn(h->reduce_ctx, h->acc_base, h->acc_len, (void *)h->s);
+  if (rc) return fail(h, KAOS_ERR_CUDA, "accumulator reduction hook returned %d", rc);
   return KAOS_OK;
 }
 
@@ -473,6 +480,8 @@ CxArgs cx_args(kaos_handle *h) {
   a.cxconv = h->d_cxconv;
   a.cxbase = h->d_cxbase;
   a.cxend = h->d_cxend;
+  a.rank = h->rank;
+  a.nranks = h->nranks;
   a.nqmax = max_nq(h);
   a.mixed = h->mixed;
   a.status = h->d_status;
@@ -572,7 +581,7 @@ int step_once(kaos_handle *h) {
     a.bin_only = 1;
     a.write_qind = 1;
     if ((rc = launch_push(h, a))) return rc;
-    if ((rc = launch_moments(h, 1))) return rc;
+    if ((rc = reduce_accum(h)) || (rc = launch_moments(h, 1))) return rc;
     if (!h->have_import) {
       if ((rc = launch_fields(h, 0))) return rc;
     } else {
@@ -612,7 +621,7 @@ int step_once(kaos_handle *h) {
   if (master) {
     if (h->P.LBCONDITIONflag == 1 && (rc = launch_inject(h, 0))) return rc;
     if (h->P.UBCONDITIONflag == 1 && (rc = launch_inject(h, 1))) return rc;
-    if ((rc = launch_moments(h, nn))) return rc;
+    if ((rc = reduce_accum(h)) || (rc = launch_moments(h, nn))) return rc;
   }
   h->n = n;
   return KAOS_OK;
@@ -646,7 +655,7 @@ int autotune(kaos_handle *h) {
       a.write_qind = 1;
       a.write_qk4 = 0;
       float tmin = 1e30f;
-      for (int rep = 0; rep < 2; ++rep) {
+      for (int rep = 0; rep < 3; ++rep) {  // the first is a warm-up
         CK(cudaEventRecord(e0, h->s));
         const int npev0 = h->npev;
         const int64_t l0 = h->launches;
@@ -658,7 +667,7 @@ int autotune(kaos_handle *h) {
         CK(cudaEventSynchronize(e1));
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e0, e1));
-        tmin = std::min(tmin, ms);
+        if (rep > 0) tmin = std::min(tmin, ms);
       }
       if (tmin < best) { best = tmin; bw = m; bp = pm; br = rs; }
     }
@@ -758,6 +767,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   h->mixed = p->precision == KAOS_PREC_MIXED;
   h->three_d = p->ION2VPERPflag == 1;
   h->ntubes = ntubes;
+  h->id_base.assign(ntubes, 0);
   VGridC &vg = h->vg;
   vg.three_d = h->three_d;
   vg.n1 = vgc->n1;
@@ -879,11 +889,27 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   if ((rc = dalloc(h, &c.nuPoi, coff))) return rc;
   if ((rc = dalloc(h, &c.mom, coff * KAOS_NMOMENTS))) return rc;
   h->host_cells = {qGL, qGH, qGC};
-  // accumulators
-  if ((rc = dalloc(h, &h->acc.cnt, coff))) return rc;
-  if ((rc = dalloc(h, &h->acc.mpar, coff * vg.npar))) return rc;
-  if ((rc = dalloc(h, &h->acc.m1, coff * vg.n1))) return rc;
-  if ((rc = dalloc(h, &h->acc.m2, coff * std::max(vg.n2, 1)))) return rc;
+  // binning accumulators, ions then ENAs, in one block (one reduction
+  // covers them all when a tube is split across ranks)
+  {
+    const size_t nc = (size_t)coff;
+    const size_t ion_n = nc * (1 + vg.npar + vg.n1 + std::max(vg.n2, 1));
+    const size_t ena_n = p->QEXCHANGEflag == 1 ? nc * (1 + 3 * (size_t)MAXV) : 0;
+    unsigned *base = nullptr;
+    if ((rc = dalloc(h, &base, ion_n + ena_n))) return rc;
+    h->acc_base = base;
+    h->acc_len = (int64_t)(ion_n + ena_n);
+    h->acc.cnt = base;
+    h->acc.mpar = base + nc;
+    h->acc.m1 = h->acc.mpar + nc * vg.npar;
+    h->acc.m2 = h->acc.m1 + nc * vg.n1;
+    if (ena_n) {
+      h->acc.ecnt = base + ion_n;
+      h->acc.emp = h->acc.ecnt + nc;
+      h->acc.emq = h->acc.emp + nc * MAXV;
+      h->acc.emph = h->acc.emq + nc * MAXV;
+    }
+  }
   // tube descriptors and the static block -> (tube, chunk) map
   std::vector<int> bt;
   std::vector<int64_t> bs;
@@ -987,11 +1013,6 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
           (rc = dalloc(h, &E.id, ecap_all)))
         return rc;
     }
-    if ((rc = dalloc(h, &h->acc.ecnt, (size_t)h->ncell)) ||
-        (rc = dalloc(h, &h->acc.emp, (size_t)h->ncell * MAXV)) ||
-        (rc = dalloc(h, &h->acc.emq, (size_t)h->ncell * MAXV)) ||
-        (rc = dalloc(h, &h->acc.emph, (size_t)h->ncell * MAXV)))
-      return rc;
     std::vector<int> ebt, te0, cxt, tc0;
     std::vector<int64_t> ebs, cxs;
     for (int t = 0; t < ntubes; ++t) {
@@ -1082,6 +1103,7 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
       a.v1 = stage + 2 * n;
       a.v2 = vperp2 ? stage + 3 * n : nullptr;
       a.n = n;
+      a.id0 = h->id_base[tube];
       a.ion = h->ion[h->cur];
       a.ct = h->ct;
       a.mixed = h->mixed;
@@ -1094,7 +1116,7 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
     if (e != cudaSuccess) return fail(h, KAOS_ERR_CUDA, "load: %s", cudaGetErrorString(e));
   }
   int64_t nl = n;
-  uint64_t nid = (uint64_t)n;
+  uint64_t nid = h->id_base[tube] + (uint64_t)n;
   CK(cudaMemcpy(h->d_nlive + tube, &nl, sizeof(int64_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_next_id + tube, &nid, sizeof(uint64_t), cudaMemcpyHostToDevice));
   if (h->d_cxc)  // the first push starts the selection counts from zero
@@ -1128,6 +1150,7 @@ int kaos_init_particles(kaos_handle *h, int32_t tube, const kaos_init_c *in) {
   a.T = T;
   a.pre = d_pre;
   a.n = n;
+  a.id0 = h->id_base[tube];
   a.ion = h->ion[h->cur];
   a.ct = h->ct;
   a.tail_fraction = in->tail_fraction;
@@ -1147,7 +1170,7 @@ int kaos_init_particles(kaos_handle *h, int32_t tube, const kaos_init_c *in) {
   cudaFree(d_pre);
   if (e != cudaSuccess) return fail(h, KAOS_ERR_CUDA, "init: %s", cudaGetErrorString(e));
   int64_t nl = n;
-  uint64_t nid = (uint64_t)n;
+  uint64_t nid = h->id_base[tube] + (uint64_t)n;
   CK(cudaMemcpy(h->d_nlive + tube, &nl, sizeof(int64_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_next_id + tube, &nid, sizeof(uint64_t), cudaMemcpyHostToDevice));
   if (h->d_cxc)  // the first push starts the selection counts from zero
@@ -1223,6 +1246,29 @@ int kaos_set_ena_grid(kaos_handle *h, const kaos_vgrid_c *vg) {
   return KAOS_OK;
 }
 
+int kaos_set_reduce(kaos_handle *h, kaos_reduce_fn fn, void *ctx) {
+  if (!h) return KAOS_ERR_PARAM;
+  h->reduce_fn = fn;
+  h->reduce_ctx = ctx;
+  return KAOS_OK;
+}
+
+int kaos_set_rank(kaos_handle *h, int32_t rank, int32_t nranks) {
+  if (!h) return KAOS_ERR_PARAM;
+  if (nranks < 1 || rank < 0 || rank >= nranks)
+    return fail(h, KAOS_ERR_PARAM, "rank %d of %d", rank, nranks);
+  h->rank = rank;
+  h->nranks = nranks;
+  return KAOS_OK;
+}
+
+int kaos_set_id_base(kaos_handle *h, int32_t tube, uint64_t base) {
+  if (!h || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  if (h->n != 0) return fail(h, KAOS_ERR_STATE, "ids are set before the first step");
+  h->id_base[tube] = base;
+  return KAOS_OK;
+}
+
 int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode) {
   if (!h || !chunk || !mode) return KAOS_ERR_PARAM;
   *chunk = CHUNKS[h->wsel];
@@ -1243,7 +1289,7 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
     const int64_t n = h->n + 1;
     int rc;
     if (h->tune_pending && n >= 2 && (rc = autotune(h))) return rc;
-    if (!h->graph || n == 1) {
+    if (!h->graph || n == 1 || h->reduce_fn) {  // a host hook runs between kernels
       if ((rc = step_once(h))) return rc;
       h->dstep_valid = 0;
       ++k;

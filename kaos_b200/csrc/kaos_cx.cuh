@@ -35,8 +35,16 @@ struct CxArgs {
   int64_t *cxbase;           // per chunk: ENA slot of its first conversion
   int *cxend;                // per cell (all tubes): chunks >= cxend convert none
   int nqmax, mixed;
+  int rank, nranks;          // this rank's share of a split tube's conversions
   uint32_t *status;
 };
+
+// Ions a cell converts at this step on this rank: its share of
+// nint(nuIonNeutPoiT) when the tube is split over nranks.
+__device__ __forceinline__ unsigned cx_need(const CxArgs &a, double nu) {
+  const unsigned n = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
+  return a.nranks > 1 ? (n + (unsigned)a.rank) / (unsigned)a.nranks : n;
+}
 
 // exclusive scan over the chunks of a tube for one cell (one block per
 // (tube, cell) pair, block-wide scan); adds the conversions of this cell to
@@ -47,8 +55,7 @@ struct CxArgs {
 __global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
   const int t = cell_tube[blockIdx.x], k = cell_q[blockIdx.x];
   const TubeD &T = a.tubes[t];
-  const double nu = a.ct.nuPoi[T.coff + k];
-  const unsigned need = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
+  const unsigned need = cx_need(a, a.ct.nuPoi[T.coff + k]);
   if (need == 0u) return;
   const int c0 = a.tube_cx0[t], c1 = a.tube_cx0[t + 1];
   __shared__ unsigned wsum[32];
@@ -148,8 +155,7 @@ __global__ void k_cx_convert(CxArgs a) {
   __shared__ unsigned done, wconv[32];
   if (threadIdx.x == 0) done = 0;
   for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
-    const double nu = a.ct.nuPoi[T.coff + k];
-    unsigned nd = nu > 0.0 ? (unsigned)llrint(nu) : 0u;
+    unsigned nd = cx_need(a, a.ct.nuPoi[T.coff + k]);
     if (nd && c >= a.cxend[T.coff + k]) nd = 0u;  // prefix >= need
     const unsigned o = nd ? a.cxo[(int64_t)c * a.nqmax + k] : 0u;
     crow[k] = 0u;

@@ -655,6 +655,7 @@ struct InitArgs {
   TubeD T;
   const int64_t *pre;   // [nq+1] exclusive prefix of the per-cell counts
   int64_t n;
+  uint64_t id0;         // id of ion 0 (keys its draws)
   Ions ion;
   CellTables ct;
   double tail_fraction, s_tail;
@@ -669,12 +670,13 @@ struct InitArgs {
 // quartic root by Newton from the cell's linear guess, converged to FP64).
 __device__ __forceinline__ void store_ion(const Ions &I, const TubeD &T,
                                           const CellTables &ct, int64_t j,
-                                          int c, double q, double vpar,
-                                          double v1, double v2, int mixed) {
+                                          uint64_t id, int c, double q,
+                                          double vpar, double v1, double v2,
+                                          int mixed) {
   const int64_t k = T.off + j, g = T.coff + c;
   const double qL = ct.qGL[g], qH = ct.qGH[g];
   I.qind[k] = c;
-  I.id[k] = (uint64_t)j;
+  I.id[k] = id;
   if (I.vb) {
     const int bp = vbin(c_vg.epar, c_vg.npar, vpar);
     const int b1 = vbin(c_vg.e1, c_vg.n1, sqrt(v1 * v1 + v2 * v2));
@@ -728,15 +730,16 @@ __global__ void k_init(InitArgs a) {
     const int c = lo;
     const int64_t g = T.coff + c;
     const double qL = a.ct.qGL[g], qH = a.ct.qGH[g];
-    kaos_u32x4 w = kaos_philox((uint32_t)j, (uint32_t)((uint64_t)j >> 32), 0u,
+    const uint64_t id = a.id0 + (uint64_t)j;
+    kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), 0u,
                                (KAOS_RNG_INIT << 24), a.seed);
     const double upos = kaos_u01(w.v[0], w.v[1]), upop = kaos_u01(w.v[2], w.v[3]);
     const double q = __dadd_rn(qL, __dmul_rn(__dadd_rn(0.02, __dmul_rn(0.96, upos)),
                                              __dadd_rn(qH, -qL)));
     const bool tail = upop < a.tail_fraction;
     double g0, g1, g2, g3;
-    init_pair(a.seed, (uint64_t)j, 1u, g0, g1);
-    init_pair(a.seed, (uint64_t)j, 2u, g2, g3);
+    init_pair(a.seed, id, 1u, g0, g1);
+    init_pair(a.seed, id, 2u, g2, g3);
     double f;
     if (!tail) {
       f = sqrt(KB * a.ct.TsG[g] / T.ms);
@@ -744,14 +747,14 @@ __global__ void k_init(InitArgs a) {
       double W = __dmul_rn(g3, g3), x, y;
       int m = 1;  // normals 3 .. 3+nu-1; g3 is the first
       for (uint32_t sub = 3; m < a.nu; ++sub) {
-        init_pair(a.seed, (uint64_t)j, sub, x, y);
+        init_pair(a.seed, id, sub, x, y);
         W = __dadd_rn(W, __dmul_rn(x, x));
         if (++m < a.nu) { W = __dadd_rn(W, __dmul_rn(y, y)); ++m; }
       }
       f = a.s_tail / sqrt(W / (double)a.nu);
     }
     const double vpar = __dmul_rn(f, g0), v1 = __dmul_rn(f, g1), v2 = __dmul_rn(f, g2);
-    store_ion(a.ion, T, a.ct, j, c, q, vpar, v1, v2, a.mixed);
+    store_ion(a.ion, T, a.ct, j, id, c, q, vpar, v1, v2, a.mixed);
   }
 }
 
@@ -763,6 +766,7 @@ struct LoadArgs {
   TubeD T;
   const double *q, *vpar, *v1, *v2;  // v2 may be null (2D grid)
   int64_t n;
+  uint64_t id0;
   Ions ion;
   CellTables ct;
   int mixed;
@@ -782,7 +786,8 @@ __global__ void k_load(LoadArgs a) {
     if (s <= E[0]) q = qGL[0];
     else if (s > E[T.nq]) q = qGH[T.nq - 1];
     const int c = cell_search(E, T.nq, T.sgn * q);
-    store_ion(a.ion, T, a.ct, j, c, q, a.vpar[j], a.v1[j], a.v2 ? a.v2[j] : 0.0,
+    store_ion(a.ion, T, a.ct, j, a.id0 + (uint64_t)j, c, q, a.vpar[j], a.v1[j],
+              a.v2 ? a.v2[j] : 0.0,
               a.mixed);
   }
 }

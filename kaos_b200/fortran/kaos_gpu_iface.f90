@@ -213,6 +213,26 @@ module kaos_gpu_iface
       type(kaos_vgrid_t), intent(in) :: vg
     end function kaos_set_ena_grid
 
+    integer(c_int) function kaos_set_reduce(h, fn, ctx) bind(C, name="kaos_set_reduce")
+      import :: c_int, c_ptr, c_funptr
+      type(c_ptr), value :: h
+      type(c_funptr), value :: fn
+      type(c_ptr), value :: ctx
+    end function kaos_set_reduce
+
+    integer(c_int) function kaos_set_rank(h, rank, nranks) bind(C, name="kaos_set_rank")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: rank, nranks
+    end function kaos_set_rank
+
+    integer(c_int) function kaos_set_id_base(h, tube, base) bind(C, name="kaos_set_id_base")
+      import :: c_int, c_int32_t, c_int64_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: tube
+      integer(c_int64_t), value :: base
+    end function kaos_set_id_base
+
     integer(c_int) function kaos_get_launch(h, chunk, mode) &
         bind(C, name="kaos_get_launch")
       import :: c_int, c_int32_t, c_ptr

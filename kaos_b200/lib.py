@@ -28,7 +28,11 @@ EXPORTS = [
     "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
     "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
     "kaos_get_launch", "kaos_set_ena_grid", "kaos_init_particles",
+    "kaos_set_reduce", "kaos_set_rank", "kaos_set_id_base",
 ]
+
+# int fn(void *ctx, uint32_t *buf, int64_t count, void *stream)
+REDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)
 
 _lib = None
 
@@ -68,6 +72,9 @@ def load(path: str = LIBPATH):
     L.kaos_get_launch.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
     L.kaos_set_ena_grid.argtypes = [vp, vp]
     L.kaos_init_particles.argtypes = [vp, i32, vp]
+    L.kaos_set_reduce.argtypes = [vp, REDUCE_FN, vp]
+    L.kaos_set_rank.argtypes = [vp, i32, i32]
+    L.kaos_set_id_base.argtypes = [vp, i32, C.c_uint64]
     L.kaos_last_error.argtypes = [vp]
     L.kaos_last_error.restype = C.c_char_p
     L.kaos_get_status.argtypes = [vp, C.POINTER(C.c_uint32)]
@@ -195,6 +202,23 @@ class Solver:
 
     def set_graph(self, on):
         self._check(load().kaos_set_graph(self.h, int(on)))
+
+    def set_reduce(self, fn):
+        """Cross-rank sum of the binning accumulators of a split tube:
+        fn(buf_ptr, count, stream_ptr) -> 0 sums `count` uint32 counters at
+        device address buf_ptr over the ranks in place; None removes it."""
+        if fn is None:
+            self._reduce = None
+            self._check(load().kaos_set_reduce(self.h, REDUCE_FN(), None))
+            return
+        self._reduce = REDUCE_FN(lambda ctx, buf, count, stream: int(fn(buf, count, stream)))
+        self._check(load().kaos_set_reduce(self.h, self._reduce, None))
+
+    def set_rank(self, rank, nranks):
+        self._check(load().kaos_set_rank(self.h, int(rank), int(nranks)))
+
+    def set_id_base(self, tube, base):
+        self._check(load().kaos_set_id_base(self.h, int(tube), int(base)))
 
     def init_particles(self, tube, counts, tail_fraction=0.0, kappa=3.0,
                        tail_T=0.0, seed=20261203):

@@ -1,10 +1,17 @@
-"""Tube sharding across ranks (one process per GPU).
+"""Tube sharding across ranks (one process per GPU), and a tube split.
 
 Flux tubes never interact in the reference -- species and tubes are the
 outermost sequential loops around the time loop (_8_KineticSolver.f90:43-44)
 -- so a multi-GPU run gives each rank a set of whole tubes and needs no
 collective on the data path.  Only the results are gathered (per-tube moments
 and counts to rank 0) and the timing is reduced as the maximum over ranks.
+
+A tube larger than one GPU is split instead, as the reference's MPI ranks
+split a tube's particles: every rank holds the tube's tables and a share of
+its ions (`split_ions`), and the per-cell binning accumulators are summed
+over the ranks before each set of moments (MPIReduceSumSub,
+_9_MPIReduceSum.f90:25-55), here by one NCCL all-reduce of the handle's
+accumulator block (`nccl_reduce_hook`, given to Solver.set_reduce).
 """
 from __future__ import annotations
 
@@ -53,3 +60,39 @@ def max_over_ranks(value: float, dist, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def split_ions(n: int, world: int) -> List[range]:
+    """Contiguous shares of n ions over `world` ranks (the first n % world
+    ranks hold one more); rank r's ions keep their global ids."""
+    base, extra = divmod(n, world)
+    out, start = [], 0
+    for r in range(world):
+        m = base + (1 if r < extra else 0)
+        out.append(range(start, start + m))
+        start += m
+    return out
+
+
+class _DeviceCounters:
+    """A device buffer of int32 counters seen through the CUDA array
+    interface (the accumulators are uint32; every count fits in int32)."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<i4",
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def nccl_reduce_hook(group=None):
+    """A Solver.set_reduce hook: in-place sum of the accumulator block over
+    the process group (NCCL on GPUs), then wait for it."""
+    import torch
+    import torch.distributed as dist
+
+    def hook(buf: int, count: int, stream: int) -> int:
+        t = torch.as_tensor(_DeviceCounters(buf, count), device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        torch.cuda.current_stream().synchronize()
+        return 0
+
+    return hook

@@ -94,3 +94,15 @@ def test_two_ranks_gloo_match_single_process():
         np.testing.assert_array_equal(merged[k]["counts"], ref["counts"])
         np.testing.assert_array_equal(merged[k]["M0"], ref["M0"])
         assert merged[k]["n"] == ref["n"]
+
+
+def test_split_ions_and_conversion_shares():
+    """A split tube: contiguous shares that cover every ion once, and the
+    per-rank shares floor((N + r) / R) of a cell's conversions sum to N."""
+    from kaos_b200.shard import split_ions
+    for n, world in ((10, 3), (7, 7), (5, 8), (123457, 4)):
+        sh = split_ions(n, world)
+        assert sum(len(s) for s in sh) == n
+        assert [i for s in sh for i in s] == list(range(n))
+        for N in (0, 1, 2, 5, 17, 1000):
+            assert sum((N + r) // world for r in range(world)) == N
