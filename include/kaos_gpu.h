@@ -166,7 +166,11 @@ typedef struct kaos_handle kaos_handle;
 
 /* Create a solver for `ntubes` independent tubes on the current device.
  * Replaces the allocation and parameter copy of DataTypeAllocBSub /
- * SimParameterizationSub (_8_KineticSolver.f90:50). */
+ * SimParameterizationSub (_8_KineticSolver.f90:50).  With
+ * MOMENTFILTERflag = 1 every moving-average window must be odd, >= 3 and at
+ * most the tube's cell count (MomentFilterSub reads that many cells around
+ * each cell; the reference's guard, NqICT >= (Pt-1)/2, lets shorter tubes
+ * read outside the array). */
 int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
                 int32_t ntubes, const kaos_vgrid_c *vg, kaos_handle **out);
 

@@ -805,6 +805,19 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
       *out = h;
       return fail(h, KAOS_ERR_PARAM, "tube %d: nq must be in [6, %d], capacity > 0, tables non-NULL", t, MAX_CELLS);
     }
+    // MomentFilterSub (_8_7_1_MomentFilter.f90:30-142) reads Pt cells around
+    // each cell; a tube shorter than the window would read outside it
+    if (p->MOMENTFILTERflag == 1) {
+      const int pts[5] = {p->M0MAfilterPt, p->M1ParMAfilterPt, p->M1Perp1MAfilterPt,
+                          p->M1Perp2MAfilterPt, p->M2ParMAfilterPt};
+      for (int w : pts)
+        if (w < 3 || w % 2 == 0 || T.nq < w) {
+          *out = h;
+          return fail(h, KAOS_ERR_PARAM,
+                      "tube %d: moving-average windows must be odd, >= 3 and at most nq (%d): got %d",
+                      t, T.nq, w);
+        }
+    }
     for (int k = 0; k + 1 < T.nq; ++k)
       if (T.qGH[k] != T.qGL[k + 1]) {
         *out = h;

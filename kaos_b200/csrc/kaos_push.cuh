@@ -170,40 +170,56 @@ __device__ __forceinline__ void bin_win_flush(const Accum &acc, const TubeD &T,
 }
 
 // Field magnitude at q by linear interpolation between cell centres with
-// constant half cells at both ends (_8_7_AmbipolarEfield.f90:1453-2722);
-// returns false outside the grid (the particle keeps its value).
-__device__ __forceinline__ bool interp_centres(const double *E, const double *C,
-                                               const double *Eg,
-                                               const double *qC, int nq,
-                                               double sgn, double q,
-                                               double *out) {
-  double s = sgn * q;
-  if (s < E[0] || s > E[nq]) return false;
-  if (s <= C[0]) { *out = Eg[0]; return true; }
-  if (s >= C[nq - 1]) { *out = Eg[nq - 1]; return true; }
-  int lo = 1, hi = nq - 1;  // smallest k with s <= C[k]
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (s <= C[mid]) hi = mid; else lo = mid + 1;
-  }
-  double x1 = qC[lo - 1], x2 = qC[lo];
-  *out = Eg[lo - 1] + (((q - x1) / (x2 - x1)) * (Eg[lo] - Eg[lo - 1]));
-  return true;
+// constant half cells at both ends (_8_7_AmbipolarEfield.f90:1453-2722).
+// centre_segment gives the segment of s = sgn*q: 0 below the first centre,
+// nq above the last, else the smallest k in [1, nq-1] with s <= C[k] (the
+// same k as a bisection), found by walking from the ion's cell since q_k4
+// lies within a cell or two of it; -1 outside the grid (the ion keeps its
+// field values).
+__device__ __forceinline__ int centre_segment(const double *E, const double *C,
+                                              int nq, double s, int guess) {
+  if (s < E[0] || s > E[nq]) return -1;
+  if (s <= C[0]) return 0;
+  if (s >= C[nq - 1]) return nq;
+  int k = min(max(guess, 1), nq - 1);
+  while (k > 1 && s <= C[k - 1]) --k;
+  while (k < nq - 1 && s > C[k]) ++k;
+  return k;
+}
+
+// y1 + ((q - x1) / (x2 - x1)) (y2 - y1) (LinInterpsub, _KineticMainParams
+// .f90:810-815) on segment k; frac = (q - x1) / (x2 - x1) is shared by the
+// fields interpolated at the same q.
+__device__ __forceinline__ double interp_frac(int k, const double *qC, int nq,
+                                              double q) {
+  if (k == 0 || k == nq) return 0.0;
+  const double x1 = qC[k - 1], x2 = qC[k];
+  return (q - x1) / (x2 - x1);
+}
+
+__device__ __forceinline__ double interp_at(int k, const double *Eg, int nq,
+                                            double frac) {
+  if (k == 0) return Eg[0];
+  if (k == nq) return Eg[nq - 1];
+  return Eg[k - 1] + (frac * (Eg[k] - Eg[k - 1]));
 }
 
 __device__ __forceinline__ void field_prologue(const PushArgs &a,
                                                const TubeD &T, const double *E,
                                                const double *C, double qk,
-                                               double &aea, double &ag) {
+                                               int guess, double &aea,
+                                               double &ag) {
+  const int k = centre_segment(E, C, T.nq, T.sgn * qk, guess);
+  if (k < 0) return;
   const double qm = T.qs / T.ms;
-  double v;
-  if (a.ff.eamb && interp_centres(E, C, a.ct.EAmag + T.coff, a.ct.qGC + T.coff,
-                                  T.nq, T.sgn, qk, &v)) {
+  const double frac = interp_frac(k, a.ct.qGC + T.coff, T.nq, qk);
+  if (a.ff.eamb) {
+    const double v = interp_at(k, a.ct.EAmag + T.coff, T.nq, frac);
     double e = a.ff.eambsign ? v : fabs(v);
     aea = (e == 0.0) ? 0.0 : (a.ff.eambsign ? qm * e : fabs(qm * e));
   }
-  if (a.ff.grav && interp_centres(E, C, a.ct.EG + T.coff, a.ct.qGC + T.coff,
-                                  T.nq, T.sgn, qk, &v)) {
+  if (a.ff.grav) {
+    const double v = interp_at(k, a.ct.EG + T.coff, T.nq, frac);
     double e = fabs(v);
     ag = (e == 0.0) ? 0.0 : fabs(qm * e);
   }
@@ -393,6 +409,18 @@ __device__ __forceinline__ int cell_search_from(const double *E, int nq,
   return cell_search(E, nq, s);
 }
 
+// Copy the velocity-cell edges of the three axes into shared memory.
+template <typename T>
+__device__ __forceinline__ void load_vgrid_smem(const T *e1, const T *e2,
+                                                const T *ep, T *s1, T *s2,
+                                                T *sp) {
+  for (int k = threadIdx.x; k <= MAXV; k += blockDim.x) {
+    s1[k] = e1[k];
+    s2[k] = e2[k];
+    sp[k] = ep[k];
+  }
+}
+
 // Load this block's tube and its oriented cell edges / centres into smem.
 __device__ __forceinline__ void load_tube_smem(const PushArgs &a, int t,
                                                TubeD &T, double *E,
@@ -431,6 +459,10 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   Ions I = a.ion;
   TubeD T;
   int tcur = -1;
+  // velocity-cell edges for the bin searches: shared memory serves the
+  // threads' different addresses in parallel (constant memory serialises)
+  __shared__ double VE1[MAXV + 1], VE2[MAXV + 1], VEP[MAXV + 1];
+  if (a.bin || !THREE_D) load_vgrid_smem(c_vg.e1, c_vg.e2, c_vg.epar, VE1, VE2, VEP);
   // one work item per block, or a persistent grid striding over the items
   for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
   const int t = a.blk_tube[item];
@@ -459,7 +491,7 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
     const double rho = I.rho[j], z = I.z[j], vpar = I.vpar[j];
     double v1 = I.v1[j], v2 = I.v2[j];
     double aea = I.aea[j], ag = I.ag[j];
-    if (a.prologue) field_prologue(a, T, E, Cc, I.qk4[j], aea, ag);
+    if (a.prologue) field_prologue(a, T, E, Cc, I.qk4[j], qprev, aea, ag);
     const double vp2 = v1 * v1 + v2 * v2;
     // ---- k1: KineticUpdateA -------------------------------------------
     const Geo<double> g1 = geo(rho, z);
@@ -467,14 +499,14 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
     int b1 = -1, b2 = -1, bp = -1;
     if (THREE_D) {
       if (a.bin) {
-        bp = vbin(c_vg.epar, c_vg.npar, vpar);
-        b1 = vbin(c_vg.e1, c_vg.n1, v1);
-        b2 = vbin(c_vg.e2, c_vg.n2, v2);
+        bp = vbin(VEP, c_vg.npar, vpar);
+        b1 = vbin(VE1, c_vg.n1, v1);
+        b2 = vbin(VE2, c_vg.n2, v2);
       }
     } else {  // 2D grid: an out-of-grid speed keeps its previous bin
       const int old = I.vb[j];
-      const int np_ = vbin(c_vg.epar, c_vg.npar, vpar);
-      const int n1_ = vbin(c_vg.e1, c_vg.n1, sqrt(vp2));
+      const int np_ = vbin(VEP, c_vg.npar, vpar);
+      const int n1_ = vbin(VE1, c_vg.n1, sqrt(vp2));
       bp = np_ >= 0 ? np_ : (old & 0xffff) - 1;
       b1 = n1_ >= 0 ? n1_ : (old >> 16) - 1;
       const int nw = ((b1 + 1) << 16) | (bp + 1);
@@ -577,6 +609,9 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
   Ions I = a.ion;
   TubeD T;
   int tcur = -1;
+  // velocity-cell edges for the bin searches in shared memory
+  __shared__ float VE1[MAXV + 1], VE2[MAXV + 1], VEP[MAXV + 1];
+  if (a.bin || !THREE_D) load_vgrid_smem(c_vg.f1, c_vg.f2, c_vg.fpar, VE1, VE2, VEP);
   // one work item per block, or a persistent grid striding over the items
   for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
   const int t = a.blk_tube[item];
@@ -644,7 +679,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
     if (c0 == DEAD) continue;
     if (a.prologue) {
       double da = aea, dg = ag;
-      field_prologue(a, T, E, Cc, (double)I.fqk4[j], da, dg);
+      field_prologue(a, T, E, Cc, (double)I.fqk4[j], c0, da, dg);
       aea = (float)da;
       ag = (float)dg;
     }
@@ -671,14 +706,14 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
     int b1 = -1, b2 = -1, bp = -1;
     if (THREE_D) {
       if (a.bin) {
-        bp = vbin(c_vg.fpar, c_vg.npar, vpar);
-        b1 = vbin(c_vg.f1, c_vg.n1, v1);
-        b2 = vbin(c_vg.f2, c_vg.n2, v2);
+        bp = vbin(VEP, c_vg.npar, vpar);
+        b1 = vbin(VE1, c_vg.n1, v1);
+        b2 = vbin(VE2, c_vg.n2, v2);
       }
     } else {
       const int old = I.vb[j];
-      const int np_ = vbin(c_vg.fpar, c_vg.npar, vpar);
-      const int n1_ = vbin(c_vg.f1, c_vg.n1, sqrtf(vp2));
+      const int np_ = vbin(VEP, c_vg.npar, vpar);
+      const int n1_ = vbin(VE1, c_vg.n1, sqrtf(vp2));
       bp = np_ >= 0 ? np_ : (old & 0xffff) - 1;
       b1 = n1_ >= 0 ? n1_ : (old >> 16) - 1;
       const int nw = ((b1 + 1) << 16) | (bp + 1);

@@ -1246,6 +1246,15 @@ static void step_once(orc *o) {
 
 orc *orc_create(const kaos_params_c *p, const kaos_tube_c *t,
                 const kaos_vgrid_c *vg) {
+  /* MomentFilterSub reads Pt cells around each cell: a tube shorter than a
+   * window would read outside the arrays (the library rejects it too) */
+  if (p->MOMENTFILTERflag == 1) {
+    const int pts[5] = {p->M0MAfilterPt, p->M1ParMAfilterPt, p->M1Perp1MAfilterPt,
+                        p->M1Perp2MAfilterPt, p->M2ParMAfilterPt};
+    for (int k = 0; k < 5; ++k)
+      if (pts[k] < 3 || pts[k] % 2 == 0 || t->nq < pts[k])
+        return NULL;
+  }
   orc *o = (orc *)calloc(1, sizeof(orc));
   o->P = *p;
   if (o->P.ndatfac < 1)

@@ -68,6 +68,9 @@ class Oracle:
         self.nbins = vg.nbins(self.three_d)
         self.h = lib().orc_create(C.addressof(self._mi), C.addressof(self._tube),
                                   C.addressof(self._vg))
+        if not self.h:
+            raise ValueError("oracle: moving-average windows must be odd, >= 3 and "
+                             "at most the tube's cell count")
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -19,7 +19,7 @@ class _OracleAsSolver:
 
 
 def test_export_layout_roundtrip(tmp_path):
-    mi, spec, tube, vg = grids.config_small(n_particles=1500, three_d=True, nq=10)
+    mi, spec, tube, vg = grids.config_small(n_particles=1500, three_d=True, nq=12)
     o = Oracle(mi, tube, vg)
     o.load(*grids.initial_particles(tube, spec, mi, seed=4))
     o.step(1)

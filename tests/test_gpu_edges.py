@@ -71,7 +71,7 @@ def test_largest_tube_2048_cells():
 
 def test_largest_velocity_grid_128_bins():
     mi = ModelInput(h=0.01, ndatfac=3, ION2VPERPflag=1)
-    spec = TubeSpec(L=4.0, nq=8, n_particles=5000, q_ub=0.3, H=600e3)
+    spec = TubeSpec(L=4.0, nq=12, n_particles=5000, q_ub=0.3, H=600e3)
     vg = make_vgrid(True, 128, 128, 128, 6e3)
     s, o = _run_one(mi, spec, vg, 7)
     _compare(s, 0, o)
@@ -86,6 +86,10 @@ def test_limits_rejected():
     t = make_tube(TubeSpec(nq=16, n_particles=1000, q_ub=0.2), mi)
     with pytest.raises(KaosError):
         Solver(mi, [t], make_vgrid(True, 130, 16, 24, 8e3))
+    # a tube shorter than the moment filter's window (11 cells)
+    t = make_tube(TubeSpec(nq=10, n_particles=1000, q_ub=0.2), mi)
+    with pytest.raises(KaosError):
+        Solver(mi, [t], vg)
 
 
 def test_empty_and_single_ion_entries():

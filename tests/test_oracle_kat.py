@@ -157,7 +157,7 @@ def test_particle_number_conservation_and_F_d3v():
 def test_moments_of_drifting_maxwellian():
     """Bin-centre moments of a drifting Maxwellian approach the analytic
     drift and temperature (first-step statistics, before any push)."""
-    mi, spec, tube, vg = grids.config_small(n_particles=200000, nq=8, three_d=True)
+    mi, spec, tube, vg = grids.config_small(n_particles=200000, nq=12, three_d=True)
     vg = grids.make_vgrid(True, 64, 64, 96, 8e3)
     n = int(tube._counts.sum())
     rng = np.random.default_rng(11)
