@@ -114,7 +114,12 @@ typedef struct kaos_params_c {
   int32_t M1Perp1MAfilterPt;
   int32_t M1Perp2MAfilterPt;
   int32_t M2ParMAfilterPt;
-  int32_t reserved[4];
+  int32_t FLUXINJECTIONflag;  /* 1: injected V|| drawn from the Maxwellian
+                                 flux through the boundary (directed into the
+                                 tube) instead of the plain Maxwellian of
+                                 _8_0_0_2_KineticSolverB.f90:317-335; an
+                                 extension, 0 in the reference's runs      */
+  int32_t reserved[3];
 } kaos_params_c;
 
 /*

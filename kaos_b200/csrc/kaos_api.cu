@@ -446,6 +446,8 @@ int launch_inject(kaos_handle *h, int ub) {
   a.qs = h->P.qs;
   a.seed = h->P.seed;
   a.status = h->d_status;
+  a.flux = h->P.FLUXINJECTIONflag == 1;
+  a.stat = h->P.STATICINJECTIONflag == 1;
   if (h->P.QEXCHANGEflag == 1) {  // injected ions join the next selection
     a.cxc = h->d_cxc;
     a.tube_cx0 = h->d_tube_cx0;

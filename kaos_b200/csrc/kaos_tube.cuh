@@ -553,6 +553,7 @@ struct InjArgs {
   uint64_t *next_id;
   unsigned long long *n_in;  // per tube injected count (LB, UB)
   int mixed, ub, bin, exporting;
+  int flux, stat;  // FLUXINJECTIONflag, STATICINJECTIONflag
   double ms, qs;
   uint64_t seed;
   uint32_t *status;
@@ -599,6 +600,13 @@ __global__ void k_inject(InjArgs a) {
     double v1 = ((1.0 - 3.0 * ct * ct) / sl) * h_ + ((3.0 * Vz0 * ct * st) / sl);
     double vpar = ((3.0 * ct * st) / sl) * h_ + ((Vz0 * (3.0 * ct * ct - 1.0)) / sl);
     double v2 = -Vx0 * T.sphi + Vy0 * T.cphi;
+    if (a.flux) {  // V|| of the Maxwellian flux into the tube (Rayleigh)
+      kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), 0u,
+                                 (KAOS_RNG_INJECT << 24) | 3u, a.seed);
+      const double r = sig * sqrt(-2.0 * log(kaos_u01(w.v[0], w.v[1])));
+      vpar = a.ub ? -r : r;
+    }
+    if (a.stat) v1 = v2 = vpar = 0.0;  // STATICINJECTIONflag
     const double vp = sqrt(v1 * v1 + v2 * v2);
     int bp = vbin(c_vg.epar, c_vg.npar, vpar);
     int b1 = vbin(c_vg.e1, c_vg.n1, d3 ? v1 : vp);

@@ -35,7 +35,8 @@ module kaos_gpu_iface
       PHASEENERGYPARIONMOMENTCENTERflag, PHASEENERGYPERPIONMOMENTCENTERflag, &
       M0MAfilterPt, M1ParMAfilterPt, M1Perp1MAfilterPt, M1Perp2MAfilterPt, &
       M2ParMAfilterPt
-    integer(c_int32_t) :: reserved(4)
+    integer(c_int32_t) :: FLUXINJECTIONflag
+    integer(c_int32_t) :: reserved(3)
   end type kaos_params_t
 
   ! kaos_tube_c: pointers are c_loc() of the FluxTubeT per-cell tables

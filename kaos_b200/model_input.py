@@ -61,7 +61,8 @@ class KaosParams(C.Structure):
         ("PHASEENERGYPERPIONMOMENTCENTERflag", C.c_int32),
         ("M0MAfilterPt", C.c_int32), ("M1ParMAfilterPt", C.c_int32),
         ("M1Perp1MAfilterPt", C.c_int32), ("M1Perp2MAfilterPt", C.c_int32),
-        ("M2ParMAfilterPt", C.c_int32), ("reserved", C.c_int32 * 4),
+        ("M2ParMAfilterPt", C.c_int32), ("FLUXINJECTIONflag", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -127,6 +128,7 @@ class ModelInput:
     M1Perp1MAfilterPt: int = 11
     M1Perp2MAfilterPt: int = 11
     M2ParMAfilterPt: int = 11
+    FLUXINJECTIONflag: int = 0    # extension: flux-weighted V|| at injection
 
     def to_c(self) -> KaosParams:
         p = KaosParams()

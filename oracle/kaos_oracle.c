@@ -1035,6 +1035,12 @@ static void inject(orc *o, int ub) {
                  ((Vz0 * (3.0 * (ct * ct) - 1.0)) / sqrt(ell));
     double Vph0 = -Vx0 * sp + Vy0 * cp;
     double v1 = Vp0, v2 = Vph0, vpar = Vq0;
+    if (P->FLUXINJECTIONflag == 1) { /* Maxwellian flux into the tube */
+      kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), 0u,
+                                 (KAOS_RNG_INJECT << 24) | 3u, P->seed);
+      double r = sig * sqrt(-2.0 * log(kaos_u01(w.v[0], w.v[1])));
+      vpar = ub ? -r : r;
+    }
     if (P->STATICINJECTIONflag == 1)
       v1 = v2 = vpar = 0.0;
     place_ion(o, j, o->qGC[Q], vpar, v1, v2);

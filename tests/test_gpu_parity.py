@@ -277,3 +277,20 @@ def test_device_initial_ions_match_oracle(mixed):
     for k in ("z", "vpar", "vperp1", "vperp2"):
         assert rel_norm(ps[k], po[k]) < TRAJ_TOL, k
     np.testing.assert_array_equal(s.counts(), o.counts())
+
+
+@pytest.mark.parametrize("flux,static", [(1, 0), (0, 1)])
+def test_injection_variants(flux, static):
+    """Flux-weighted injection (extension) and STATICINJECTIONflag at both
+    boundaries match the oracle (FP64, 1e-12; counts exact)."""
+    mi, spec, tube, vg = grids.config_small(n_particles=3000, three_d=True,
+                                            steps_per_master=3)
+    mi.FLUXINJECTIONflag, mi.STATICINJECTIONflag, mi.UBCONDITIONflag = flux, static, 1
+    tube.nsnormCLB, tube.nsnormCUB = 40.0, 15.0
+    o, s = run_pair(mi, spec, tube, vg, 13)
+    assert o.count() == s.count()
+    np.testing.assert_array_equal(s.boundary(), o.boundary())
+    po, ps = o.particles(), s.particles()
+    for k in ("z", "vpar", "vperp1", "vperp2"):
+        assert rel_norm(ps[k], po[k]) < TRAJ_TOL, k
+    np.testing.assert_array_equal(s.counts(), o.counts())

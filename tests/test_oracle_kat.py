@@ -275,3 +275,26 @@ def test_initial_ion_generator_distributions():
     assert abs(np.var(v) / (KB * T_tail / MO) - 1) < 0.15
     kurt = np.mean(v ** 4) / np.var(v) ** 2
     assert kurt > 4.0  # Student-t with 5 dof: kurtosis 9; Gaussian: 3
+
+
+def test_flux_weighted_injection():
+    """FLUXINJECTIONflag: ions injected at the lower boundary move into the
+    tube with V|| from the Maxwellian flux, mean sigma sqrt(pi/2); without
+    it V|| is the plain Maxwellian component (both signs)."""
+    from kaos_b200.model_input import MO
+    mi, spec, tube, vg = grids.config_small(n_particles=2000, three_d=True,
+                                            steps_per_master=2)
+    tube.nsnormCLB = 4000.0
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=4)
+    sig = np.sqrt(KB * tube.TsG[0] / MO)
+    for flux in (1, 0):
+        mi.FLUXINJECTIONflag = flux
+        o = Oracle(mi, tube, vg)
+        o.load(q, vpar, v1, v2)
+        o.step(2)  # master step 2 injects after the push
+        vin = o.particles()["vpar"][-4000:]
+        if flux:
+            assert np.all(vin > 0)
+            assert abs(np.mean(vin) / (sig * np.sqrt(np.pi / 2)) - 1) < 0.04
+        else:
+            assert np.mean(vin < 0) > 0.4
