@@ -341,6 +341,19 @@ int kaos_set_rank(kaos_handle *h, int32_t rank, int32_t nranks);
  * and draw the same numbers as the unsplit tube.  Set before loading. */
 int kaos_set_id_base(kaos_handle *h, int32_t tube, uint64_t base);
 
+/*
+ * Convection of a tube to a new L-shell (ConvectionSub, _8_11_Convection
+ * .f90:135-258; the reference's E x B L-shell update is a stub adding 0,
+ * :107, and its grid keeps the q boundaries qGA/qGB).  `t` holds the tube's
+ * tables regenerated for the new pG (and phiG) on the same q grid (same nq,
+ * qGL, qGH).  At the next master step, before anything else, every ion keeps
+ * its q and V|| and moves to the new field line, its magnetic moment kept:
+ * both Vperp components scale by sqrt(B_new/B_old); then the new tables
+ * replace the old.  ENAs are neutral and stay where they are.  The tube's
+ * evolving Te is kept.
+ */
+int kaos_update_tube(kaos_handle *h, int32_t tube, const kaos_tube_c *t);
+
 /* The launch shape in use (after autotuning). */
 int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode);
 

@@ -140,6 +140,13 @@ struct kaos_handle {
   void *reduce_ctx = nullptr;
   int rank = 0, nranks = 1;          // share of the charge-exchange counts
   std::vector<uint64_t> id_base;     // first ion id per tube
+  // tube moves (kaos_update_tube) applied at the next master step
+  struct PendingTube {
+    int tube;
+    TubeD d;
+    std::vector<std::vector<double>> tables;  // in CONV_TABLES order
+  };
+  std::vector<PendingTube> pending, applied;
   // push work items: (tube, chunk of ions) maps, one per candidate chunk
   struct WorkMap {
     int chunk = 0, n = 0;
@@ -332,6 +339,72 @@ int zero_accum(kaos_handle *h) {
   CK(cudaMemsetAsync(h->acc_base, 0, (size_t)h->acc_len * sizeof(unsigned), h->s));
   if (h->export_on && h->acc.hist)
     CK(cudaMemsetAsync(h->acc.hist, 0, nc * (int64_t)h->nv * sizeof(unsigned), h->s));
+  return KAOS_OK;
+}
+
+// The per-cell tables of one tube, in the order of CellTables' pointers
+// listed by conv_table_ptr (the same values kaos_create builds).
+constexpr int CONV_TABLES = 27;
+std::vector<std::vector<double>> tube_tables(const kaos_tube_c &T, const TubeD &d,
+                                             const kaos_params_c &p) {
+  std::vector<std::vector<double>> v(CONV_TABLES);
+  auto app = [&](int k, const double *src, double dflt) {
+    for (int c = 0; c < T.nq; ++c) v[k].push_back(src ? src[c] : dflt);
+  };
+  app(0, T.qGL, 0); app(1, T.qGH, 0); app(2, T.qGC, 0); app(3, T.hqC, 0);
+  app(4, T.dqC, 0); app(5, T.d3xC, 1); app(6, T.rGC, 0); app(7, T.thetaGC, 0);
+  app(8, T.ellGC, 1); app(9, T.TeG, 0); app(10, T.TsG, 0); app(11, T.nsnormCNeut, 0);
+  app(12, T.lambdaPerp, 0); app(13, T.EtaLH, 0); app(14, T.XiPerp1, 0);
+  app(15, T.XiPerp2, 0); app(16, T.S0, 0); app(17, T.OmegaG0, 1);
+  app(18, T.ChiPerp1, 0); app(19, T.ChiPerp2, 0);
+  for (int c = 0; c < T.nq; ++c) {
+    v[20].push_back(host_quartic_u(T.qGL[c], T.pG));
+    v[21].push_back(host_quartic_u(T.qGH[c], T.pG));
+    const double pre = (d.qs * d.qs / (2.0 * d.ms * d.ms)) *
+                       (T.S0 ? T.S0[c] : 0.0) * (T.EtaLH ? T.EtaLH[c] : 0.0);
+    v[22].push_back(p.h * std::sqrt(pre * (T.XiPerp1 ? T.XiPerp1[c] : 0.0) / PI));
+    v[23].push_back(p.h * std::sqrt(pre * (T.XiPerp2 ? T.XiPerp2[c] : 0.0) / PI));
+    v[24].push_back(0.5 * (T.ChiPerp1 ? T.ChiPerp1[c] : 0.0));
+    v[25].push_back(0.5 * (T.ChiPerp2 ? T.ChiPerp2[c] : 0.0));
+    v[26].push_back(T.OmegaG0 && T.OmegaG0[c] != 0.0 ? 1.0 / T.OmegaG0[c] : 0.0);
+  }
+  return v;
+}
+
+const double *conv_table_ptr(const CellTables &c, int k) {
+  const double *p[CONV_TABLES] = {c.qGL, c.qGH, c.qGC, c.hqC, c.dqC, c.d3xC, c.rGC,
+                                  c.thetaGC, c.ellGC, c.TeG, c.TsG, c.nsnormCNeut,
+                                  c.lambdaPerp, c.EtaLH, c.XiPerp1, c.XiPerp2, c.S0,
+                                  c.OmegaG0, c.ChiPerp1, c.ChiPerp2, c.uL, c.uH,
+                                  c.hK1, c.hK2, c.hc1, c.hc2, c.hiom0};
+  return p[k];
+}
+
+// Move the tubes given to kaos_update_tube: re-project their ions with the
+// old tables (k_convect), then copy the new tables and descriptor in.  The
+// host copies are asynchronous from the handle's pending vectors, which stay
+// alive until the end of the kaos_step call.
+int apply_pending_tubes(kaos_handle *h) {
+  for (auto &pt : h->pending) {
+    TubeD &old = h->th[pt.tube];
+    ConvArgs ca{};
+    ca.T = old;
+    ca.p_new = pt.d.pG;
+    ca.nlive = h->d_nlive;
+    ca.tube = pt.tube;
+    ca.ion = h->ion[h->cur];
+    ca.ct = h->ct;
+    ca.mixed = h->mixed;
+    const int grid = (int)std::min<int64_t>((old.cap + 255) / 256, 148 * 16);
+    k_convect<<<grid, 256, 0, h->s>>>(ca);
+    h->launches++;
+    CK(cudaGetLastError());
+    for (int k = 0; k < CONV_TABLES; ++k)
+      CK(cudaMemcpyAsync((void *)(conv_table_ptr(h->ct, k) + old.coff), pt.tables[k].data(),
+                         old.nq * sizeof(double), cudaMemcpyHostToDevice, h->s));
+    old = pt.d;
+    CK(cudaMemcpyAsync(h->d_tubes + pt.tube, &old, sizeof(TubeD), cudaMemcpyHostToDevice, h->s));
+  }
   return KAOS_OK;
 }
 
@@ -604,6 +677,12 @@ int step_once(kaos_handle *h) {
   }
   const bool master = is_master(h, n);
   const uint32_t nn = (uint32_t)(n / h->P.ndatfac + 1);
+  // ConvectionSub runs first on a master step (_8_KineticSolver.f90:62)
+  if (master && !h->pending.empty()) {
+    if ((rc = apply_pending_tubes(h))) return rc;
+    for (auto &pt : h->pending) h->applied.push_back(std::move(pt));
+    h->pending.clear();
+  }
   if (qx && (rc = launch_cx(h))) return rc;
   if (master) {
     if ((rc = launch_boundary(h))) return rc;
@@ -1261,6 +1340,40 @@ int kaos_set_ena_grid(kaos_handle *h, const kaos_vgrid_c *vg) {
   return KAOS_OK;
 }
 
+int kaos_update_tube(kaos_handle *h, int32_t tube, const kaos_tube_c *T) {
+  if (!h || !T || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  const TubeD &cur = h->th[tube];
+  if (T->nq != cur.nq || !T->qGL || !T->qGH || !T->qGC || !T->hqC || !T->dqC ||
+      !T->d3xC || !T->rGC || !T->thetaGC || !T->ellGC || !T->TeG || !T->TsG)
+    return fail(h, KAOS_ERR_PARAM, "tube %d: update needs the same nq and non-NULL tables", tube);
+  const double *qGL = h->host_cells[0].data() + cur.coff;
+  const double *qGH = h->host_cells[1].data() + cur.coff;
+  for (int k = 0; k < cur.nq; ++k)
+    if (T->qGL[k] != qGL[k] || T->qGH[k] != qGH[k])
+      return fail(h, KAOS_ERR_PARAM, "tube %d: the q grid must stay the same (cell %d)", tube, k);
+  kaos_handle::PendingTube pt;
+  pt.tube = tube;
+  pt.d = cur;
+  pt.d.pG = T->pG;
+  pt.d.phiG = T->phiG;
+  pt.d.cphi = std::cos(T->phiG);
+  pt.d.sphi = std::sin(T->phiG);
+  pt.d.nsnormfac = T->nsnormfac;
+  pt.d.nsnormCLB = T->nsnormCLB;
+  pt.d.nsnormCUB = T->nsnormCUB;
+  pt.d.sumdsICR = T->sumdsICR;
+  host_rho_z(T->qGC[0], T->pG, &pt.d.rhoLB, &pt.d.zLB);
+  host_rho_z(T->qGC[T->nq - 1], T->pG, &pt.d.rhoUB, &pt.d.zUB);
+  pt.tables = tube_tables(*T, pt.d, h->P);
+  for (auto &q : h->pending)
+    if (q.tube == tube) {
+      q = std::move(pt);
+      return KAOS_OK;
+    }
+  h->pending.push_back(std::move(pt));
+  return KAOS_OK;
+}
+
 int kaos_set_reduce(kaos_handle *h, kaos_reduce_fn fn, void *ctx) {
   if (!h) return KAOS_ERR_PARAM;
   h->reduce_fn = fn;
@@ -1304,7 +1417,8 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
     const int64_t n = h->n + 1;
     int rc;
     if (h->tune_pending && n >= 2 && (rc = autotune(h))) return rc;
-    if (!h->graph || n == 1 || h->reduce_fn) {  // a host hook runs between kernels
+    if (!h->graph || n == 1 || h->reduce_fn ||
+        (!h->pending.empty() && is_master(h, n))) {  // host work between kernels
       if ((rc = step_once(h))) return rc;
       h->dstep_valid = 0;
       ++k;
@@ -1320,6 +1434,7 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
   }
   CK(cudaEventRecord(h->e1, h->s));
   CK(cudaEventSynchronize(h->e1));
+  h->applied.clear();  // their host tables have been copied
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, h->e0, h->e1));
   h->last_ms = ms;

@@ -800,4 +800,67 @@ __global__ void k_load(LoadArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// ConvectionSub (_8_11_Convection.f90:135-258): on a master step the tube's
+// field line moves to L-shell p_new (the E x B drift); every ion keeps its q
+// and its V||, is placed on the new field line (RK4DipolePolynomialSolverSub
+// at (q, p_new)), and its magnetic moment mu = m Vperp^2 / (2 B) is kept, so
+// both Vperp components (same gyro-angle) scale by sqrt(B_new / B_old).
+// Runs with the tube's old tables, before the new ones are copied in.
+struct ConvArgs {
+  TubeD T;               // the tube before the move
+  double p_new;
+  const int64_t *nlive;
+  int tube;
+  Ions ion;
+  CellTables ct;
+  int mixed;
+};
+
+// |B| / B0 at (q, u = r/RE) on any field line: sqrt(1 + 3 cos^2) / u^3.
+__device__ __forceinline__ double bnorm(double q, double u) {
+  const double ct = q * u * u;
+  return sqrt(1.0 + 3.0 * ct * ct) / (u * u * u);
+}
+
+__global__ void k_convect(ConvArgs a) {
+  const TubeD &T = a.T;
+  const int64_t nl = a.nlive[a.tube];
+  const double ip_old = 1.0 / T.pG, ip_new = 1.0 / a.p_new;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nl;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = T.off + i;
+    if (a.ion.qind[j] == DEAD) continue;
+    double q, u_old;
+    if (a.mixed) {
+      const int c = a.ion.cell[j];
+      if (c == DEAD) continue;
+      const int64_t g = T.coff + c;
+      const double o = (double)a.ion.off[j];
+      q = a.ct.qGL[g] + o * (a.ct.qGH[g] - a.ct.qGL[g]);
+      u_old = quartic_newton(q, ip_old, a.ct.uL[g] + o * (a.ct.uH[g] - a.ct.uL[g]), 4);
+    } else {
+      const double rho = a.ion.rho[j], z = a.ion.z[j];
+      const double r2 = rho * rho + z * z, r = sqrt(r2);
+      q = (RE * RE) * (z / r) / r2;
+      u_old = r / RE;
+    }
+    const double u_new = quartic_newton(q, ip_new, u_old, 6);
+    const double f = sqrt(bnorm(q, u_new) / bnorm(q, u_old));
+    if (a.mixed) {
+      a.ion.fv1[j] = (float)(f * (double)a.ion.fv1[j]);
+      a.ion.fv2[j] = (float)(f * (double)a.ion.fv2[j]);
+    } else {
+      const double rr = u_new * RE, st = sqrt(u_new * ip_new), ctv = q * u_new * u_new;
+      double rho = rr * st, z = rr * ctv;
+      if (fabs(rho) < 1e-6) rho = 0.0;
+      if (fabs(z) < 1e-6) z = 0.0;
+      a.ion.rho[j] = rho;
+      a.ion.z[j] = z;
+      a.ion.v1[j] = f * a.ion.v1[j];
+      a.ion.v2[j] = f * a.ion.v2[j];
+    }
+  }
+}
+
 }  // namespace kaos

@@ -221,6 +221,13 @@ module kaos_gpu_iface
       type(c_ptr), value :: ctx
     end function kaos_set_reduce
 
+    integer(c_int) function kaos_update_tube(h, tube, t) bind(C, name="kaos_update_tube")
+      import :: c_int, c_int32_t, c_ptr, kaos_tube_t
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: tube
+      type(kaos_tube_t), intent(in) :: t
+    end function kaos_update_tube
+
     integer(c_int) function kaos_set_rank(h, rank, nranks) bind(C, name="kaos_set_rank")
       import :: c_int, c_int32_t, c_ptr
       type(c_ptr), value :: h

@@ -70,15 +70,20 @@ class TubeSpec:
 
 
 
-def make_tube(spec: TubeSpec, mi: ModelInput) -> Tube:
-    """Build the per-cell tables of one tube (NMH: q decreases upward)."""
+def make_tube(spec: TubeSpec, mi: ModelInput, q_edges=None) -> Tube:
+    """Build the per-cell tables of one tube (NMH: q decreases upward);
+    q_edges (nq + 1 values) keeps a given q grid, as a convected tube does
+    (its q boundaries qGA/qGB are held, _8_11_Convection.f90:64-66)."""
     L, nq = spec.L, spec.nq
-    qa = q_of_altitude(spec.alt_lb, L)
-    qb = spec.q_ub
-    # uniform q edges, _0_ConfigGridGenerator.f90:299-310
-    k = np.arange(nq + 1, dtype=np.float64)
-    qe = qa - k * (abs(qb - qa) / nq)
-    qe[-1] = qb
+    if q_edges is not None:
+        qe = np.array(q_edges, dtype=np.float64)
+    else:
+        qa = q_of_altitude(spec.alt_lb, L)
+        qb = spec.q_ub
+        # uniform q edges, _0_ConfigGridGenerator.f90:299-310
+        k = np.arange(nq + 1, dtype=np.float64)
+        qe = qa - k * (abs(qb - qa) / nq)
+        qe[-1] = qb
     qGL, qGH = qe[:-1].copy(), qe[1:].copy()
     qGC = (qGL + qGH) / 2.0
     r, th = dipole_q_to_rtheta(qGC, L)
@@ -225,6 +230,18 @@ def config_c2(n_particles=10_000_000, heating=True, collisions=True,
     tube = make_tube(spec, mi)
     vg = make_vgrid(True, 48, 48, 64, 30e3)
     return mi, spec, tube, vg
+
+
+def moved_tube(spec: TubeSpec, mi: ModelInput, tube: Tube, L_new: float) -> Tube:
+    """The tables of `tube` regenerated on a new L-shell for ConvectionSub:
+    same q grid and macro-particle weight, geometry of the new field line."""
+    import dataclasses
+    sp = dataclasses.replace(spec, L=L_new)
+    t = make_tube(sp, mi, q_edges=np.concatenate([tube.qGL, tube.qGH[-1:]]))
+    t.nsnormfac = tube.nsnormfac
+    t.nsnormCLB, t.nsnormCUB = tube.nsnormCLB, tube.nsnormCUB
+    t.capacity = tube.capacity
+    return t
 
 
 # kappa tail of the large single-tube workload

@@ -28,7 +28,7 @@ EXPORTS = [
     "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
     "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
     "kaos_get_launch", "kaos_set_ena_grid", "kaos_init_particles",
-    "kaos_set_reduce", "kaos_set_rank", "kaos_set_id_base",
+    "kaos_set_reduce", "kaos_set_rank", "kaos_set_id_base", "kaos_update_tube",
 ]
 
 # int fn(void *ctx, uint32_t *buf, int64_t count, void *stream)
@@ -75,6 +75,7 @@ def load(path: str = LIBPATH):
     L.kaos_set_reduce.argtypes = [vp, REDUCE_FN, vp]
     L.kaos_set_rank.argtypes = [vp, i32, i32]
     L.kaos_set_id_base.argtypes = [vp, i32, C.c_uint64]
+    L.kaos_update_tube.argtypes = [vp, i32, vp]
     L.kaos_last_error.argtypes = [vp]
     L.kaos_last_error.restype = C.c_char_p
     L.kaos_get_status.argtypes = [vp, C.POINTER(C.c_uint32)]
@@ -213,6 +214,13 @@ class Solver:
             return
         self._reduce = REDUCE_FN(lambda ctx, buf, count, stream: int(fn(buf, count, stream)))
         self._check(load().kaos_set_reduce(self.h, self._reduce, None))
+
+    def update_tube(self, tube, t):
+        """Move tube `tube` to the tables of Tube `t` (new L-shell, same q
+        grid) at the next master step (ConvectionSub)."""
+        tc = t.to_c()
+        self._check(load().kaos_update_tube(self.h, int(tube), C.addressof(tc)))
+        self._tubes[tube] = t
 
     def set_rank(self, rank, nranks):
         self._check(load().kaos_set_rank(self.h, int(rank), int(nranks)))

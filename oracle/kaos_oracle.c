@@ -71,8 +71,12 @@ typedef struct orc {
   double *EAimport;
   int64_t n; /* computational steps taken */
   int64_t lb_out, ub_out, lb_in, ub_in;
+  kaos_tube_c *pending; /* orc_update_tube: applied at the next master step */
+  double GAconv;        /* gyro-angle carried between ions as in the reference */
   char err[256];
 } orc;
+
+static void free_tube(kaos_tube_c *c);
 
 /* ------------------------------------------------------------------------ */
 /* helpers from _KineticMainParams.f90:568-815                              */
@@ -1167,6 +1171,91 @@ static void ena_statistics(orc *o) {
   }
 }
 
+/* ConvectionSub _8_11_Convection.f90:135-258 for a move of the tube to
+ * o->pending (new pG/phiG, same q grid): every ion keeps q, moves to the new
+ * field line (RK4DipolePolynomialSolverSub at (q, pN, phiN)), keeps its
+ * magnetic moment (musub, :146-147, :184-185) and gyro-angle (:168-182,
+ * :188-214, the angle of the previous ion kept when a component is exactly
+ * zero), and its velocity is rebuilt along the new field direction from
+ * VparConvSign |V| (:229-255).  ENAs are left in place (the reference's ENA
+ * branch uses the theta and ell of the previous ion, :232-238).  Then the
+ * tube's tables are replaced, its evolving Te kept. */
+static double bmag(double r, double th) {
+  return MDIP * sqrt(1.0 + 3.0 * sq(cos(th))) / (r * r * r);
+}
+
+static void convection(orc *o) {
+  const kaos_tube_c *t = o->pending;
+  const double pN = t->pG, phN = t->phiG, ms = o->P.ms;
+  for (int64_t j = 0; j < o->np; ++j) {
+    if (o->ena[j])
+      continue;
+    double r1 = sqrt(o->x[j] * o->x[j] + o->y[j] * o->y[j] + o->z[j] * o->z[j]);
+    double th1 = acos(o->z[j] / r1);
+    double q = (RE * RE) * cos(th1) / (r1 * r1);
+    double ph1 = atan2(o->y[j], o->x[j]);
+    double el1 = 1.0 + 3.0 * sq(cos(th1));
+    double mu = ms * sq(o->Vp[j]) / (2.0 * bmag(r1, th1));
+    /* V|| sign along the old field direction */
+    double ct1 = cos(th1), st1 = sin(th1), cp1 = cos(ph1), sp1 = sin(ph1);
+    double vpar1 = 3.0 * ct1 * st1 * (o->Vx[j] * cp1 + o->Vy[j] * sp1) / sqrt(el1) +
+                   o->Vz[j] * (3.0 * (ct1 * ct1) - 1.0) / sqrt(el1);
+    double vmag = sqrt(sq(o->Vx[j]) + sq(o->Vy[j]) + sq(o->Vz[j]));
+    double vpar2 = (vpar1 < 0.0 ? -1.0 : 1.0) * fabs(vmag);
+    double r2, th2, x, y, z;
+    quartic(q, pN, phN, &r2, &th2, &x, &y, &z);
+    o->x[j] = x;
+    o->y[j] = y;
+    o->z[j] = z;
+    double V1 = o->V1[j], V2 = o->V2[j];
+    if (V1 > 0.0 && V2 > 0.0)
+      o->GAconv = atan(fabs(V2) / fabs(V1));
+    if (V1 < 0.0 && V2 > 0.0)
+      o->GAconv = PI - atan(fabs(V2) / fabs(V1));
+    if (V1 < 0.0 && V2 < 0.0)
+      o->GAconv = PI + atan(fabs(V2) / fabs(V1));
+    if (V1 > 0.0 && V2 < 0.0)
+      o->GAconv = 2.0 * PI - atan(fabs(V2) / fabs(V1));
+    double GA = o->GAconv;
+    double Vpn = sqrt(2.0 * bmag(r2, th2) * mu / ms);
+    o->Vp[j] = Vpn;
+    if (0.0 < GA && GA <= PI / 2.0) {
+      o->V1[j] = fabs(Vpn * cos(GA));
+      o->V2[j] = fabs(Vpn * sin(GA));
+    }
+    if (PI / 2.0 < GA && GA <= PI) {
+      o->V1[j] = -fabs(Vpn * cos(PI - GA));
+      o->V2[j] = fabs(Vpn * sin(PI - GA));
+    }
+    if (PI < GA && GA <= 3.0 * PI / 2.0) {
+      o->V1[j] = -fabs(Vpn * cos(GA - PI));
+      o->V2[j] = -fabs(Vpn * sin(GA - PI));
+    }
+    if (3.0 * PI / 2.0 < GA && GA <= 2.0 * PI) {
+      o->V1[j] = fabs(Vpn * cos(2.0 * PI - GA));
+      o->V2[j] = -fabs(Vpn * sin(2.0 * PI - GA));
+    }
+    double ct = cos(th2), st = sin(th2), el = 1.0 + 3.0 * ct * ct;
+    o->Vx[j] = cos(phN) * (3.0 * vpar2 * ct * st) / sqrt(el);
+    o->Vy[j] = sin(phN) * (3.0 * vpar2 * ct * st) / sqrt(el);
+    o->Vz[j] = vpar2 * (3.0 * (ct * ct) - 1.0) / sqrt(el);
+  }
+  o->pG = t->pG;
+  o->phiG = t->phiG;
+  o->nsnormfac = t->nsnormfac;
+  o->nsnormCLB = t->nsnormCLB;
+  o->nsnormCUB = t->nsnormCUB;
+  o->sumdsICR = t->sumdsICR;
+  int nq = o->nq;
+#define R(a)                                                                   \
+  if (t->a)                                                                    \
+    memcpy(o->a, t->a, sizeof(double) * (size_t)nq);
+  R(qGC) R(hqC) R(dqC) R(d3xC) R(rGC) R(thetaGC) R(ellGC) R(TeG) R(TsG)
+  R(nsnormCNeut) R(lambdaPerp) R(EtaLH) R(XiPerp1) R(XiPerp2) R(S0) R(OmegaG0)
+  R(ChiPerp1) R(ChiPerp2)
+#undef R
+}
+
 static int is_master(const orc *o, int64_t n) {
   if (n < 2)
     return 0;
@@ -1208,6 +1297,11 @@ static void step_once(orc *o) {
   }
   int master = is_master(o, n);
   uint32_t nn = (uint32_t)(n / P->ndatfac + 1);
+  if (master && o->pending) { /* ConvectionSub first, :62 */
+    convection(o);
+    free_tube(o->pending);
+    o->pending = NULL;
+  }
   if (master) /* Te update :69-89 */
     for (int Q = 0; Q < o->nq; ++Q)
       if (o->Te[Q] + P->dNTe <= P->dNTeEND)
@@ -1429,6 +1523,49 @@ int orc_set_fields(orc *o, const double *EA) {
 
 void orc_set_literal(orc *o, int on) { o->literal = on; }
 
+/* A deep copy of a tube's tables, held until the next master step. */
+static kaos_tube_c *copy_tube(const kaos_tube_c *t) {
+  kaos_tube_c *c = (kaos_tube_c *)malloc(sizeof(kaos_tube_c));
+  *c = *t;
+  const double **f[] = {&c->qGL, &c->qGH, &c->qGC, &c->hqC, &c->dqC, &c->d3xC,
+                        &c->rGC, &c->thetaGC, &c->ellGC, &c->TeG, &c->TsG,
+                        &c->nsnormCNeut, &c->lambdaPerp, &c->EtaLH, &c->XiPerp1,
+                        &c->XiPerp2, &c->S0, &c->OmegaG0, &c->ChiPerp1, &c->ChiPerp2};
+  for (size_t k = 0; k < sizeof(f) / sizeof(f[0]); ++k)
+    *f[k] = *f[k] ? dup(*f[k], t->nq) : NULL;
+  return c;
+}
+
+static void free_tube(kaos_tube_c *c) {
+  if (!c)
+    return;
+  const double *f[] = {c->qGL, c->qGH, c->qGC, c->hqC, c->dqC, c->d3xC, c->rGC,
+                       c->thetaGC, c->ellGC, c->TeG, c->TsG, c->nsnormCNeut,
+                       c->lambdaPerp, c->EtaLH, c->XiPerp1, c->XiPerp2, c->S0,
+                       c->OmegaG0, c->ChiPerp1, c->ChiPerp2};
+  for (size_t k = 0; k < sizeof(f) / sizeof(f[0]); ++k)
+    free((void *)f[k]);
+  free(c);
+}
+
+/* Test hook: apply a pending tube move now. */
+void orc_convect_now(orc *o) {
+  if (!o->pending)
+    return;
+  convection(o);
+  free_tube(o->pending);
+  o->pending = NULL;
+}
+
+/* ConvectionSub's tube move: applied at the next master step. */
+int orc_update_tube(orc *o, const kaos_tube_c *t) {
+  if (t->nq != o->nq)
+    return 1;
+  free_tube(o->pending);
+  o->pending = copy_tube(t);
+  return 0;
+}
+
 /* ENA velocity grid (Vp edges = e1/n1, Vphi = e2/n2, Vq = epar/npar). */
 void orc_set_ena_grid(orc *o, const kaos_vgrid_c *vg) {
   free(o->eep);
@@ -1576,6 +1713,7 @@ void orc_destroy(orc *o) {
   free(o->id);
   free(o->cnt);
   free(o->hist);
+  free_tube(o->pending);
   free(o);
 }
 

@@ -34,6 +34,8 @@ def lib():
         L.orc_set_fields.argtypes = [vp, vp]
         L.orc_set_literal.argtypes = [vp, C.c_int]
         L.orc_set_ena_grid.argtypes = [vp, vp]
+        L.orc_update_tube.argtypes = [vp, vp]
+        L.orc_convect_now.argtypes = [vp]
         L.orc_init.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, C.c_uint64]
         L.orc_step.argtypes = [vp, C.c_int64]
         L.orc_count.restype = C.c_int64
@@ -93,6 +95,16 @@ class Oracle:
 
     def set_literal(self, on):
         lib().orc_set_literal(self.h, int(on))
+
+    def update_tube(self, t):
+        """Move the tube to Tube `t`'s tables at the next master step."""
+        tc = t.to_c()
+        if lib().orc_update_tube(self.h, C.addressof(tc)):
+            raise ValueError("oracle: the moved tube must keep its cell count")
+
+    def convect_now(self):
+        """Test hook: apply a pending tube move immediately."""
+        lib().orc_convect_now(self.h)
 
     def set_ena_grid(self, vg):
         """ENA velocity grid: Vp edges = vg.e1, Vphi = vg.e2, Vq = vg.epar."""

@@ -294,3 +294,39 @@ def test_injection_variants(flux, static):
     for k in ("z", "vpar", "vperp1", "vperp2"):
         assert rel_norm(ps[k], po[k]) < TRAJ_TOL, k
     np.testing.assert_array_equal(s.counts(), o.counts())
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_convection_to_new_lshell(mixed):
+    """A tube moved to a new L-shell (ConvectionSub, applied first at the
+    next master step: q and V|| kept, magnetic moment kept) matches the
+    oracle: FP64 1e-12 / exact counts / moments 1e-10; mixed within its
+    precision."""
+    from kaos_b200.grids import moved_tube
+    mi, spec, tube, vg = grids.config_small(n_particles=3000, three_d=True,
+                                            steps_per_master=3, heating=True)
+    if mixed:
+        mi.precision = KAOS_PREC_MIXED
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=8)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    s = Solver(mi, [tube], vg)
+    s.load(0, q, vpar, v1, v2)
+    o.step(4)
+    s.step(4)
+    new = moved_tube(spec, mi, tube, 4.05)
+    o.update_tube(new)
+    s.update_tube(0, new)
+    o.step(7)  # the move at n = 6, another master step at n = 9
+    s.step(7)
+    assert o.count() == s.count()
+    po, ps = o.particles(), s.particles()
+    if mixed:
+        assert rel_norm(ps["vperp1"], po["vperp1"]) < 1e-4
+        assert rel_norm(ps["z"], po["z"]) < 1e-6
+        return
+    for k in ("z", "rho", "vpar", "vperp1", "vperp2"):
+        assert rel_norm(ps[k], po[k]) < TRAJ_TOL, k
+    np.testing.assert_array_equal(s.counts(), o.counts())
+    for m in (KAOS_M0, KAOS_M2, KAOS_M2PAR, KAOS_EAMAG):
+        assert rel_norm(s.moments(m), o.moments(m)) < MOM_TOL, m

@@ -298,3 +298,34 @@ def test_flux_weighted_injection():
             assert abs(np.mean(vin) / (sig * np.sqrt(np.pi / 2)) - 1) < 0.04
         else:
             assert np.mean(vin < 0) > 0.4
+
+
+def test_convection_keeps_q_mu_and_vpar():
+    """ConvectionSub (the tube moved to a new L-shell): every ion keeps its
+    q, |V||| and magnetic moment m Vperp^2 / (2B), and lies on the new
+    field line."""
+    from kaos_b200.grids import moved_tube
+    from kaos_b200.model_input import RE
+    mi, spec, tube, vg = grids.config_small(n_particles=3000, three_d=True,
+                                            steps_per_master=3)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=8)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    o.step(4)
+    p0 = o.particles()
+    o.update_tube(moved_tube(spec, mi, tube, 4.05))
+    o.convect_now()
+    p1 = o.particles()
+
+    def B(rho, z):
+        r = np.hypot(rho, z)
+        return np.sqrt(1 + 3 * (z / r) ** 2) / r ** 3
+
+    np.testing.assert_allclose(p1["q"], p0["q"], rtol=1e-12)
+    np.testing.assert_allclose(np.abs(p1["vpar"]), np.abs(p0["vpar"]), rtol=1e-12)
+    mu0 = (p0["vperp1"] ** 2 + p0["vperp2"] ** 2) / B(p0["rho"], p0["z"])
+    mu1 = (p1["vperp1"] ** 2 + p1["vperp2"] ** 2) / B(p1["rho"], p1["z"])
+    np.testing.assert_allclose(mu1, mu0, rtol=1e-10)
+    r = np.hypot(p1["rho"], p1["z"])
+    np.testing.assert_allclose(r / (p1["rho"] / r) ** 2 / RE, 4.05, rtol=1e-12)
+    assert np.all(np.sign(p1["vperp1"]) == np.sign(p0["vperp1"]))
