@@ -296,9 +296,10 @@ int kaos_set_graph(kaos_handle *h, int32_t on);
 /* Launch shape of the particle push: `chunk` ions per work item (1024,
  * 2048 or 4096; an item is a (tube, chunk of ions) pair) and `mode` bit 0:
  * 0 = one thread block per item, 1 = a persistent grid (resident blocks per
- * SM x SMs) striding over the items; bit 1 (mixed precision only): register
- * budget of the push, 0 = 64 registers (4 blocks of 256 threads per SM),
- * 1 = 80 registers (3 blocks).  chunk = 0 or mode < 0 re-arms the
+ * SM x SMs) striding over the items; bits 1-2 (mixed precision only):
+ * register budget of the push, 0 = 64 registers (4 blocks of 256 threads
+ * per SM), 1 = 80 registers (3 blocks of 256), 2 = 72 registers (7 blocks
+ * of 128).  chunk = 0 or mode < 0 re-arms the
  * autotuner, which is on by default: before the first step after step 1 it
  * times the push of every candidate on a copy of the ion state and keeps
  * the fastest.  Results do not depend on the shape.  No reference

@@ -157,9 +157,9 @@ struct kaos_handle {
   int wsel = 1;          // chosen map (CHUNKS[wsel] ions per item)
   int persistent = 0;    // persistent grid striding over the items
   int tune_pending = 1;  // autotune before the next step
-  int regsel = 0;        // mixed push register budget: 0 = 64, 1 = 80
+  int regsel = 0;        // mixed push register budget: 0 = 64, 1 = 80, 2 = 72
   int nsm = 0;
-  int occ[2] = {0, 0};   // resident push blocks per SM per budget (0: unknown)
+  int occ[3] = {0, 0, 0};  // resident push blocks per SM per budget (0: unknown)
   int64_t ion_len = 0;   // length of every ion array (all tubes' capacity)
   double last_ms = 0.0;
   int64_t launches = 0;
@@ -249,6 +249,10 @@ PushArgs push_args(kaos_handle *h) {
   a.cx_stride = max_nq(h);
   a.cx_chunk = CX_CHUNK;
   a.dstep = h->capturing ? h->d_step : nullptr;
+  for (int r = 0; r < 10; ++r) {  // Philox key schedule of the seed
+    a.rk[2 * r] = (uint32_t)h->P.seed + (uint32_t)r * KAOS_PHILOX_W0;
+    a.rk[2 * r + 1] = (uint32_t)(h->P.seed >> 32) + (uint32_t)r * KAOS_PHILOX_W1;
+  }
   return a;
 }
 
@@ -300,17 +304,23 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
   }
   if (timed) CK(cudaEventRecord(h->pev[2 * h->npev], h->s));
   size_t smem = (size_t)(2 * nq + 1) * sizeof(double) + (size_t)nq * sizeof(unsigned);
-  if (h->mixed) smem += (size_t)5 * nq * sizeof(double) + (size_t)6 * nq * sizeof(float);
+  if (h->mixed)  // + one double of padding before the 16-byte aligned floats
+    smem += (size_t)(5 * nq + 1) * sizeof(double) + (size_t)8 * nq * sizeof(float);
   smem += (size_t)BIN_WIN * (1 + h->vg.npar + h->vg.n1 + (h->three_d ? h->vg.n2 : 0)) *
           sizeof(unsigned);  // block-private binning window
   const int rs = h->mixed ? h->regsel : 0, ps = h->persistent;
-  // kernel variant: [mixed][three_d][register budget][persistent]
+  // kernel variant: [three_d][register budget][persistent]; the budgets:
+  // 64 registers (4 blocks of 256 threads per SM), 80 (3 blocks of 256),
+  // 72 (7 blocks of 128)
   using KFn = void (*)(PushArgs);
-  static const KFn k32[2][2][2] = {
-      {{k_push32<false, 4, false>, k_push32<false, 4, true>},
-       {k_push32<false, 3, false>, k_push32<false, 3, true>}},
-      {{k_push32<true, 4, false>, k_push32<true, 4, true>},
-       {k_push32<true, 3, false>, k_push32<true, 3, true>}}};
+  static const KFn k32[2][3][2] = {
+      {{k_push32<false, 256, 4, false>, k_push32<false, 256, 4, true>},
+       {k_push32<false, 256, 3, false>, k_push32<false, 256, 3, true>},
+       {k_push32<false, 128, 7, false>, k_push32<false, 128, 7, true>}},
+      {{k_push32<true, 256, 4, false>, k_push32<true, 256, 4, true>},
+       {k_push32<true, 256, 3, false>, k_push32<true, 256, 3, true>},
+       {k_push32<true, 128, 7, false>, k_push32<true, 128, 7, true>}}};
+  const int nt = rs == 2 ? 128 : PUSH_THREADS;
   static const KFn k64[2][2] = {{k_push64<false, false>, k_push64<false, true>},
                                 {k_push64<true, false>, k_push64<true, true>}};
   const KFn fn = h->mixed ? k32[h->three_d][rs][ps] : k64[h->three_d][ps];
@@ -320,11 +330,11 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ[rs], (const void *)fn, PUSH_THREADS, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ[rs], (const void *)fn, nt, smem));
     h->occ[rs] = std::max(h->occ[rs], 1);
   }
   const int grid = ps ? std::min(a.nitems, h->nsm * h->occ[rs]) : a.nitems;
-  if (grid > 0) fn<<<grid, PUSH_THREADS, smem, h->s>>>(a);
+  if (grid > 0) fn<<<grid, nt, smem, h->s>>>(a);
   if (timed) {
     CK(cudaEventRecord(h->pev[2 * h->npev + 1], h->s));
     h->npev++;
@@ -726,7 +736,7 @@ int autotune(kaos_handle *h) {
   int bw = h->wsel, bp = h->persistent, br = h->regsel;
   for (int m = 0; m < NCHUNKS; ++m)
     for (int pm = 0; pm < 2; ++pm)
-    for (int rs = 0; rs < (h->mixed ? 2 : 1); ++rs) {
+    for (int rs = 0; rs < (h->mixed ? 3 : 1); ++rs) {
       h->wsel = m;
       h->persistent = pm;
       h->regsel = rs;
@@ -1312,11 +1322,11 @@ int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode) {
   int m = -1;
   for (int k = 0; k < NCHUNKS; ++k)
     if (CHUNKS[k] == chunk) m = k;
-  if (m < 0 || mode > 3)
-    return fail(h, KAOS_ERR_PARAM, "launch: chunk must be 1024, 2048 or 4096 and mode 0..3");
+  if (m < 0 || mode > 5)
+    return fail(h, KAOS_ERR_PARAM, "launch: chunk must be 1024, 2048 or 4096 and mode 0..5");
   h->wsel = m;
   h->persistent = mode & 1;
-  h->regsel = (mode >> 1) & 1;
+  h->regsel = (mode >> 1) & 3;
   h->tune_pending = 0;
   for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
   h->graphs.clear();

@@ -46,6 +46,8 @@ struct PushArgs {
   int cx_stride, cx_chunk;
   // graph replay: the step number is read from device memory
   const uint32_t *dstep;
+  // Philox key schedule of the seed: key words of round r at rk[2r], rk[2r+1]
+  uint32_t rk[20];
 };
 
 // Flush a block's per-cell Qindk1 counts into its selection-chunk row.
@@ -334,6 +336,55 @@ __device__ __forceinline__ void heat(const PushArgs &a, uint32_t step,
   }
 }
 
+// Philox4x32-10 (include/kaos_philox.h) with the key schedule, the same for
+// every particle, read from the kernel arguments: the same output words.
+__device__ __forceinline__ kaos_u32x4 philox_rk(const PushArgs &a, uint32_t c0,
+                                                uint32_t c1, uint32_t c2,
+                                                uint32_t c3) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)KAOS_PHILOX_M0 * c0;
+    const uint64_t p1 = (uint64_t)KAOS_PHILOX_M1 * c2;
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ a.rk[2 * r];
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ a.rk[2 * r + 1];
+    c1 = (uint32_t)p1;
+    c3 = (uint32_t)p0;
+    c0 = n0;
+    c2 = n2;
+  }
+  kaos_u32x4 o;
+  o.v[0] = c0;
+  o.v[1] = c1;
+  o.v[2] = c2;
+  o.v[3] = c3;
+  return o;
+}
+
+// Uniform in (0, 1) from the high 23 bits of w, (2 (w >> 9) + 1) 2^-24, made
+// from the mantissa bits of a float in [1, 2) (exact; within 2^-25 of
+// kaos_u01f(w)).
+__device__ __forceinline__ float u01_bits(uint32_t w) {
+  return __uint_as_float(0x3f800000u | (w >> 9)) - 0x1.fffffep-1f;
+}
+
+// Single MUFU operations of the mixed push, denormals flushed: reciprocal,
+// sine and cosine (radians).
+__device__ __forceinline__ float rcpa(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float sina(float x) {
+  float r;
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float cosa(float x) {
+  float r;
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Hardware base-2 logarithm and exponential (MUFU, flush-to-zero).
 __device__ __forceinline__ float lg2f(float x) {
   float r;
@@ -350,41 +401,45 @@ __device__ __forceinline__ float ex2f(float x) {
 // product K_i x^(-c_i) (Om s)^(1/2) of heat() is one base-2 exponential,
 //   kick_i = K_i G_i 2^(-c_i log2(Om/Om0) + log2(Om |V||| / sum ds)/4 - pen),
 // the branch test h Om s <= 2 pi becomes Om |V||| / sum ds <= (2 pi/h)^2 and
-// Sigma^(-3/2) for lambda != 0 becomes pen = 1.5 log2 Sigma when Sigma >= 1.
+// Sigma^(-3/2) for lambda != 0 becomes pen = 1.5 log2 Sigma when Sigma >= 1,
+// log2 Sigma = log2(Vperp^2)/2 + log2(2 pi/lambda) - log2 Om.
 // The Gaussians are the same Box-Muller pair of one Philox draw as
-// gauss2_32.  hk: K1 K2 c1 c2 log2(1/Om0) lambda.
+// gauss2_32.  hk (8 per cell): K1 K2 c1 c2 log2(1/Om0) lambda
+// log2(2 pi/lambda) 0.
 __device__ __forceinline__ void heat32(const PushArgs &a, uint32_t step,
                                        const float *hk, uint64_t id,
                                        float invsumds, float ylim, float Om,
                                        float vabs, float &v1, float &v2) {
   const float y = Om * vabs * invsumds;  // (Om s)^2
   if (!(y <= ylim)) return;
+  const float4 h0 = *(const float4 *)hk, h1 = *(const float4 *)(hk + 4);
   const float LOm = lg2f(Om);
   float b = 0.25f * lg2f(y);
-  if (hk[5] != 0.0f) {  // Sigma = 2 pi |Vperp| / (Om lambda)
-    const float ls = lg2f(6.2831853f * sqrtf(v1 * v1 + v2 * v2) / hk[5]) - LOm;
+  if (h1.y != 0.0f) {  // lambda != 0
+    const float ls = fmaf(0.5f, lg2f(v1 * v1 + v2 * v2), h1.z) - LOm;
     if (ls >= 0.0f) b -= 1.5f * ls;
   }
-  const float lx = LOm + hk[4];
-  const float e1 = ex2f(fmaf(-hk[2], lx, b));
-  const float e2 = (hk[3] == hk[2]) ? e1 : ex2f(fmaf(-hk[3], lx, b));
-  kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), step,
-                             KAOS_RNG_HEAT << 24, a.seed);
-  const float u1 = kaos_u01f(w.v[0]), u2 = kaos_u01f(w.v[2]);
+  const float lx = LOm + h1.x;
+  const float e1 = ex2f(fmaf(-h0.z, lx, b));
+  const float e2 = (h0.w == h0.z) ? e1 : ex2f(fmaf(-h0.w, lx, b));
+  kaos_u32x4 w = philox_rk(a, (uint32_t)id, (uint32_t)(id >> 32), step,
+                           KAOS_RNG_HEAT << 24);
+  const float u1 = u01_bits(w.v[0]), u2 = u01_bits(w.v[2]);
   // -2 ln u1 > 0; the hardware logarithm's absolute error (~2^-22) can give
   // a tiny negative value for u1 just below 1
   const float t = fmaxf(-1.38629436f * lg2f(u1), 1e-30f);
-  const float R = t * rsqrtf(t);
-  float sn, cs;
-  __sincosf(6.2831853f * u2, &sn, &cs);
-  v1 = fmaf(hk[0] * e1 * R, cs, v1);
-  v2 = fmaf(hk[1] * e2 * R, sn, v2);
+  const float R = t * rsq(t);
+  const float ang = 6.2831853f * u2;
+  v1 = fmaf(h0.x * e1 * R, cosa(ang), v1);
+  v2 = fmaf(h0.y * e2 * R, sina(ang), v2);
 }
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0 by Newton from u0 (the
 // function is increasing and convex for u > 0: the root is unique).  The
-// derivative is inverted in FP32; each step still contracts the error by
-// ~1e-7 on top of the quadratic term.
+// derivative is inverted in FP32 (correctly rounded, or the one-instruction
+// approximation when FAST); each step still contracts the error by ~1e-7 on
+// top of the quadratic term.
+template <bool FAST = false>
 __device__ __forceinline__ double quartic_newton(double q, double ip, double u,
                                                  int iters) {
   const double q2 = q * q;
@@ -392,7 +447,8 @@ __device__ __forceinline__ double quartic_newton(double q, double ip, double u,
     const double u2 = u * u;
     const double f = fma(q2 * u2, u2, fma(u, ip, -1.0));
     const double fp = fma(4.0 * q2 * u2, u, ip);
-    u = fma(-f, (double)__frcp_rn((float)fp), u);
+    const float r = FAST ? rcpa((float)fp) : __frcp_rn((float)fp);
+    u = fma(-f, (double)r, u);
   }
   return u;
 }
@@ -594,15 +650,16 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
 // per-cell linear guess) and the renormalised q of the new position.
 // MINB = resident blocks per SM the register budget is sized for (4: 64
 // registers, 3: 80); the autotuner picks one.
-template <bool THREE_D, int MINB, bool PERSIST>
-__global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
-  extern __shared__ double sm[];
+template <bool THREE_D, int NT, int MINB, bool PERSIST>
+__global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
+  extern __shared__ __align__(16) double sm[];
   const int nqmax = a.nqs;
   double *E = sm, *Cc = sm + nqmax + 1;
   double *UL = Cc + nqmax, *UD = UL + nqmax, *QL = UD + nqmax, *IDQ = QL + nqmax,
          *DQ = IDQ + nqmax;
-  float *HK = (float *)(DQ + nqmax);  // 6 floats per cell: K1 K2 c1 c2 iom0 lam
-  unsigned *HC = (unsigned *)(HK + 6 * nqmax);
+  // 8 floats per cell (heat32), 16-byte aligned
+  float *HK = (float *)(sm + ((7 * nqmax + 2) & ~1));
+  unsigned *HC = (unsigned *)(HK + 8 * nqmax);
   const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
   const uint32_t step = a.dstep ? *a.dstep : a.step;
   const float fRE = (float)RE;
@@ -631,12 +688,15 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
       UL[k] = a.ct.uL[g];
       UD[k] = a.ct.uH[g] - a.ct.uL[g];
       if (a.icr) {
-        HK[6 * k + 0] = (float)a.ct.hK1[g];
-        HK[6 * k + 1] = (float)a.ct.hK2[g];
-        HK[6 * k + 2] = (float)a.ct.hc1[g];
-        HK[6 * k + 3] = (float)a.ct.hc2[g];
-        HK[6 * k + 4] = a.icrcoh ? (float)a.ct.hiom0[g] : lg2f((float)a.ct.hiom0[g]);
-        HK[6 * k + 5] = (float)a.ct.lambdaPerp[g];
+        const double lam = a.ct.lambdaPerp[g];
+        HK[8 * k + 0] = (float)a.ct.hK1[g];
+        HK[8 * k + 1] = (float)a.ct.hK2[g];
+        HK[8 * k + 2] = (float)a.ct.hc1[g];
+        HK[8 * k + 3] = (float)a.ct.hc2[g];
+        HK[8 * k + 4] = a.icrcoh ? (float)a.ct.hiom0[g] : lg2f((float)a.ct.hiom0[g]);
+        HK[8 * k + 5] = (float)lam;
+        HK[8 * k + 6] = lam != 0.0 ? (float)log2(2.0 * PI / lam) : 0.0f;
+        HK[8 * k + 7] = 0.0f;
       }
     }
     tcur = t;
@@ -685,9 +745,12 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
     }
     // ---- start-of-step position: q, then (r, theta) by FP64 Newton -------
     const double q0 = fma((double)o0, DQ[c0], QL[c0]);
-    const double u = quartic_newton(q0, ipG, fma((double)o0, UD[c0], UL[c0]), 2);
+    const double u = quartic_newton<true>(q0, ipG, fma((double)o0, UD[c0], UL[c0]), 2);
     const double s2 = u * ipG;  // sin^2(theta)
-    const double st = s2 * rsqrt(s2);
+    // sqrt(s2): FP32 seed and one FP64 Newton step (relative error ~1e-14)
+    double ys = (double)rsq((float)s2);
+    ys = ys * fma(-0.5 * s2 * ys, ys, 1.5);
+    const double st = s2 * ys;
     const double ct = q0 * u * u;
     const double r = u * RE;
     const double rho0 = r * st, z0 = r * ct;
@@ -696,10 +759,10 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
     Geo<float> g1;
     g1.ct = (float)ct;
     g1.st = (float)st;
-    g1.ir = __frcp_rn((float)u * fRE);
+    g1.ir = rcpa((float)u * fRE);
     g1.q = (float)q0;
     g1.ell = 1.0f + 3.0f * g1.ct * g1.ct;
-    g1.isl = rsqrtf(g1.ell);
+    g1.isl = rsq(g1.ell);
     g1.er = 3.0f * g1.ct * g1.st * g1.isl;
     g1.ez = (3.0f * g1.ct * g1.ct - 1.0f) * g1.isl;
     const float vp2 = v1 * v1 + v2 * v2;
@@ -732,7 +795,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
       const float ir3 = g1.ir * g1.ir * g1.ir;
       const float Om = qs_ms * (float)MDIP * sl * ir3;
       const float invOm = c_invOm * (rf * rf * rf) * g1.isl;
-      const float *hk = HK + 6 * qi;
+      const float *hk = HK + 8 * qi;
       if (!a.icrcoh) {
         heat32(a, step, hk, pid, invsumds, ylim, Om, fabsf(vpar), v1n, v2n);
       } else {
@@ -758,7 +821,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(PushArgs a) {
     // ---- renormalisation in FP64: q of the new point --------------------
     const double xr = rho0 + (double)dr, xz = z0 + (double)dz;
     const double r2 = xr * xr + xz * xz;
-    double y = (double)rsqrtf((float)r2);
+    double y = (double)rsq((float)r2);
     y = y * fma(-0.5 * r2 * y, y, 1.5);
     const double qN = (RE * RE) * xz * (y * y * y);
     const int cN = cell_search_from(E, T.nq, T.sgn * qN, qi >= 0 ? qi : c0);

@@ -247,8 +247,10 @@ class Solver:
         self._check(load().kaos_set_ena_grid(self.h, C.addressof(self._evg)))
 
     def set_launch(self, chunk, mode):
-        """chunk ions per work item (1024/2048/4096), mode 0 = block per
-        item, 1 = persistent grid; chunk 0 re-arms the autotuner."""
+        """chunk ions per work item (1024/2048/4096); mode bit 0: 0 = block
+        per item, 1 = persistent grid; bits 1-2 (mixed): register budget
+        0 = 64, 1 = 80, 2 = 72 (128-thread blocks); chunk 0 re-arms the
+        autotuner."""
         self._check(load().kaos_set_launch(self.h, int(chunk), int(mode)))
 
     def launch(self):

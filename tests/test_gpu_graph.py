@@ -90,12 +90,12 @@ def _run_shape(mixed, shape):
 @pytest.mark.parametrize("mixed", [False, True])
 def test_launch_shapes_bit_identical(mixed):
     """Every push launch shape (ions per work item, one block per item or a
-    persistent grid, register budget) and the autotuner's choice give the
-    same particles, ENAs and counts."""
+    persistent grid, register budget and block size) and the autotuner's
+    choice give the same particles, ENAs and counts."""
     ref = _run_shape(mixed, (2048, 0))
     shapes = [(1024, 1), (4096, 0), None]
     if mixed:
-        shapes += [(1024, 2), (4096, 3)]
+        shapes += [(1024, 2), (4096, 3), (2048, 4), (1024, 5)]
     for sh in shapes:
         o = _run_shape(mixed, sh)
         if sh is not None:
@@ -107,3 +107,16 @@ def test_launch_shapes_bit_identical(mixed):
         for k in ref["e"]:
             np.testing.assert_array_equal(ref["e"][k], o["e"][k], err_msg=f"{sh} {k}")
         np.testing.assert_array_equal(ref["cnt"], o["cnt"])
+
+
+def test_launch_mode_out_of_range_rejected():
+    from kaos_b200.lib import KaosError
+    mi, spec, tube, vg = grids.config_small(n_particles=500, three_d=True)
+    mi.precision = KAOS_PREC_MIXED
+    s = Solver(mi, [tube], vg)
+    for chunk, mode in ((4096, 6), (3000, 0)):
+        with pytest.raises(KaosError):
+            s.set_launch(chunk, mode)
+    s.set_launch(1024, 5)
+    assert s.launch() == (1024, 5)
+    s.close()
