@@ -185,28 +185,41 @@ def mixed_moment_error(s32, s64):
     return out
 
 
-def run_e2e(args, precision):
-    """Same metric through the public C-ABI with host buffers: the particle
-    arrays go host -> device once (amortised per step), every step reads the
-    per-cell moments back to the host, the final state comes back."""
+def run_e2e(args, precision, launch):
+    """Same metric through the public C-ABI with host buffers: the initial
+    particle arrays go from pinned host memory to the device once (amortised
+    per step), every step reads the eight per-cell moments back to the host,
+    and the final ion state comes back into pinned host memory.  The push
+    launch shape is the one the autotuner chose for the device-timed run."""
     from kaos_b200.lib import Solver
-    from kaos_b200.model_input import KAOS_M0, KAOS_M2PAR
+    import torch
     mi, spec, tube, vg, init = build_workload(precision, args.particles,
                                               heating=not args.no_heating,
                                               collisions=args.collisions)
     s = Solver(mi, [tube], vg)
+    s.set_launch(*launch)
     K = args.steps
-    import torch
+
+    def pinned(n, dtype):
+        return torch.empty(n, dtype=dtype, pin_memory=True).numpy()
+    src = []
+    for a in init:
+        b = pinned(len(a), torch.float64)
+        b[:] = a
+        src.append(b)
+    cap = tube.capacity
+    out = {k: pinned(cap, torch.float64) for k in ("q", "vpar", "vperp1", "vperp2")}
+    out["qind"] = pinned(cap, torch.int32)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s.load(0, *init)
-    h2d = sum(a.nbytes for a in init)
+    s.load(0, *src)
+    h2d = sum(a.nbytes for a in src)
     d2h = 0
     for _ in range(K):
         s.step(1)
         for m in range(8):
             d2h += s.moments(m).nbytes
-    p = s.state()
+    p = s.state(out=out)
     d2h += sum(v.nbytes for v in p.values())
     dt = time.perf_counter() - t0
     n = len(p["q"])
@@ -393,7 +406,7 @@ def main():
                  "mixed_over_fp64": l32["value"] / l64["value"],
                  "note": "mixed path replayed from CUDA graphs"}
     if not args.skip_e2e and full:
-        e2e = run_e2e(args, KAOS_PREC_MIXED)
+        e2e = run_e2e(args, KAOS_PREC_MIXED, r32["launch"])
     cpu = cpu_baseline(args) if (rank == 0 and world == 1 and full) else None
     tpi = profiled_traffic("k_push32_mixed_c2.md")
     traffic = None if tpi is None else tpi * r32["n"]
@@ -413,7 +426,8 @@ def main():
                        "l2": "inputs > L2 (particle arrays 0.5-1 GB); no flush",
                        "push_launch": {"ions_per_item": r32["launch"][0],
                                        "persistent": bool(r32["launch"][1] & 1),
-                                       "registers": 80 if r32["launch"][1] & 2 else 64,
+                                       "registers": (64, 80, 72)[(r32["launch"][1] >> 1) & 3],
+                                       "threads_per_block": 128 if r32["launch"][1] & 4 else 256,
                                        "chosen_by": "fixed" if args.launch else "autotuner"},
                        "parallelism": f"tube per GPU x{world}"},
             "fp64": None if not full else {

@@ -578,8 +578,9 @@ int launch_cx(kaos_handle *h) {
   CxArgs a = cx_args(h);
   const int nq = max_nq(h);
   // the per-chunk Qindk1 counts were accumulated by the previous push
-  k_cx_scan<<<(int)h->ncell, 256, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
-  k_cx_base<<<h->ntubes, 256, 0, h->s>>>(a);
+  // 1024 threads: one tile covers the chunks of a tube of up to 16.7 M ions
+  k_cx_scan<<<(int)h->ncell, 1024, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
+  k_cx_base<<<h->ntubes, 1024, 0, h->s>>>(a);
   k_cx_convert<<<h->ncx, 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
   h->launches += 3;
   CK(cudaGetLastError());
@@ -1531,54 +1532,56 @@ int kaos_get_particles(kaos_handle *h, int32_t tube, double *q, double *vpar,
   CK(cudaStreamSynchronize(h->s));
   int64_t nl = 0;
   CK(cudaMemcpy(&nl, h->d_nlive + tube, sizeof(int64_t), cudaMemcpyDeviceToHost));
-  const Ions &I = h->ion[h->cur];
-  const int64_t o = T.off;
-  std::vector<int32_t> qi(nl);
-  if (nl) CK(cudaMemcpy(qi.data(), I.qind + o, nl * 4, cudaMemcpyDeviceToHost));
-  int64_t live = 0;
-  for (auto v : qi) live += (v != DEAD);
-  if (n != live) return fail(h, KAOS_ERR_PARAM, "n (%lld) must equal the ion count (%lld)", (long long)n, (long long)live);
-  std::vector<double> a(nl), b(nl), c(nl), d(nl), e(nl);
-  if (h->mixed) {
-    std::vector<int32_t> cell(nl);
-    std::vector<float> fo(nl), f1(nl), f2(nl), f3(nl);
-    if (nl) {
-      CK(cudaMemcpy(cell.data(), I.cell + o, nl * 4, cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(fo.data(), I.off + o, nl * 4, cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(f1.data(), I.fvpar + o, nl * 4, cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(f2.data(), I.fv1 + o, nl * 4, cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(f3.data(), I.fv2 + o, nl * 4, cudaMemcpyDeviceToHost));
-    }
-    const double *qGL = h->host_cells[0].data() + T.coff;
-    const double *qGH = h->host_cells[1].data() + T.coff;
-    for (int64_t j = 0; j < nl; ++j) {
-      a[j] = qGL[cell[j]] + (double)fo[j] * (qGH[cell[j]] - qGL[cell[j]]);
-      b[j] = f1[j];
-      c[j] = f2[j];
-      d[j] = f3[j];
-    }
-  } else if (nl) {
-    CK(cudaMemcpy(a.data(), I.rho + o, nl * 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(e.data(), I.z + o, nl * 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(b.data(), I.vpar + o, nl * 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(c.data(), I.v1 + o, nl * 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(d.data(), I.v2 + o, nl * 8, cudaMemcpyDeviceToHost));
-    for (int64_t j = 0; j < nl; ++j) {
-      double r2 = a[j] * a[j] + e[j] * e[j];
-      double r = std::sqrt(r2);
-      a[j] = (RE * RE) * (e[j] / r) / r2;
-    }
+  if (nl == 0) {
+    if (n != 0) return fail(h, KAOS_ERR_PARAM, "n (%lld) must equal the ion count (0)", (long long)n);
+    return KAOS_OK;
   }
-  int64_t k = 0;
-  for (int64_t j = 0; j < nl; ++j) {
-    if (qi[j] == DEAD) continue;
-    if (q) q[k] = a[j];
-    if (vpar) vpar[k] = b[j];
-    if (vperp1) vperp1[k] = c[j];
-    if (vperp2) vperp2[k] = d[j];
-    if (qind) qind[k] = qi[j];
-    ++k;
+  // the export runs on the device into a staging area: q, V||, Vperp1,
+  // Vperp2 (FP64) and Qindk1 of the live ions in particle order
+  ExportArgs a{};
+  a.ion = h->ion[h->cur];
+  a.off = T.off;
+  a.nl = nl;
+  a.qGL = h->ct.qGL + T.coff;
+  a.qGH = h->ct.qGH + T.coff;
+  a.mixed = h->mixed;
+  a.nb = (int)ceil_div(nl, (int64_t)EXP_THREADS * EXP_ITEMS);
+  const size_t nd = (size_t)nl;
+  const size_t bytes = 4 * nd * sizeof(double) + nd * sizeof(int32_t) +
+                       (size_t)a.nb * (sizeof(unsigned) + sizeof(unsigned long long)) + 64;
+  char *st = nullptr;
+  if (cudaMalloc(&st, bytes) != cudaSuccess)
+    return fail(h, KAOS_ERR_CUDA, "cudaMalloc of the export staging area failed");
+  double *dq = (double *)st;
+  a.q = q ? dq : nullptr;
+  a.vpar = vpar ? dq + nd : nullptr;
+  a.v1 = vperp1 ? dq + 2 * nd : nullptr;
+  a.v2 = vperp2 ? dq + 3 * nd : nullptr;
+  int32_t *dqi = (int32_t *)(dq + 4 * nd);
+  a.qind = qind ? dqi : nullptr;
+  a.blkoff = (unsigned long long *)(((uintptr_t)(dqi + nd) + 15) & ~(uintptr_t)15);
+  a.total = a.blkoff + a.nb;
+  a.blkcnt = (unsigned *)(a.total + 1);
+  k_exp_count<<<a.nb, EXP_THREADS, 0, h->s>>>(a);
+  k_exp_scan<<<1, 1024, 0, h->s>>>(a);
+  k_exp_write<<<a.nb, EXP_THREADS, 0, h->s>>>(a);
+  unsigned long long live = 0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&live, a.total, sizeof(live), cudaMemcpyDeviceToHost, h->s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->s);
+  if (e == cudaSuccess && (int64_t)live != n) {
+    cudaFree(st);
+    return fail(h, KAOS_ERR_PARAM, "n (%lld) must equal the ion count (%lld)", (long long)n, (long long)live);
   }
+  double *dst[4] = {q, vpar, vperp1, vperp2};
+  for (int k = 0; k < 4 && e == cudaSuccess; ++k)
+    if (dst[k] && n) e = cudaMemcpyAsync(dst[k], dq + k * nd, n * sizeof(double), cudaMemcpyDeviceToHost, h->s);
+  if (e == cudaSuccess && qind && n)
+    e = cudaMemcpyAsync(qind, dqi, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->s);
+  cudaFree(st);
+  if (e != cudaSuccess) return fail(h, KAOS_ERR_CUDA, "get_particles: %s", cudaGetErrorString(e));
   return KAOS_OK;
 }
 

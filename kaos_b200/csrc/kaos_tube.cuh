@@ -864,3 +864,114 @@ __global__ void k_convect(ConvArgs a) {
 }
 
 }  // namespace kaos
+
+namespace kaos {
+
+// ---------------------------------------------------------------------------
+// kaos_get_particles on the device: field-line q in FP64 from the stored
+// position (mixed: cell + FP32 offset; FP64: the meridian-plane point), the
+// velocities widened to FP64 and Qindk1, for the live ions only (slots
+// converted to ENAs are skipped) in particle order.  Three passes: live
+// count per block, exclusive scan of the block counts, in-order write.
+constexpr int EXP_THREADS = 256, EXP_ITEMS = 8;  // 2048 ions per block
+
+struct ExportArgs {
+  Ions ion;
+  int64_t off, nl;           // the tube's segment and live slots
+  const double *qGL, *qGH;   // the tube's cell edges (mixed)
+  int mixed, nb;
+  unsigned *blkcnt;
+  unsigned long long *blkoff, *total;
+  double *q, *vpar, *v1, *v2;
+  int32_t *qind;
+};
+
+__global__ void __launch_bounds__(EXP_THREADS) k_exp_count(ExportArgs a) {
+  const int64_t beg = (int64_t)blockIdx.x * EXP_THREADS * EXP_ITEMS;
+  unsigned n = 0;
+  for (int k = 0; k < EXP_ITEMS; ++k) {
+    const int64_t i = beg + k * EXP_THREADS + threadIdx.x;
+    if (i < a.nl && a.ion.qind[a.off + i] != DEAD) ++n;
+  }
+  __shared__ unsigned ws[EXP_THREADS / 32];
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = n;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned t = 0;
+    for (int w = 0; w < EXP_THREADS / 32; ++w) t += ws[w];
+    a.blkcnt[blockIdx.x] = t;
+  }
+}
+
+// exclusive scan of the block counts (one block of 1024 threads)
+__global__ void __launch_bounds__(1024) k_exp_scan(ExportArgs a) {
+  __shared__ unsigned long long ws[32], base;
+  const int l = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  for (int r0 = 0; r0 < a.nb; r0 += blockDim.x) {
+    const int b = r0 + threadIdx.x;
+    const unsigned long long n = b < a.nb ? a.blkcnt[b] : 0ull;
+    unsigned long long x = n;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (l >= o) x += y;
+    }
+    if (l == 31) ws[w] = x;
+    __syncthreads();
+    unsigned long long woff = 0, tot = 0;
+    for (int v = 0; v < nw; ++v) { if (v < w) woff += ws[v]; tot += ws[v]; }
+    if (b < a.nb) a.blkoff[b] = base + woff + x - n;
+    __syncthreads();
+    if (threadIdx.x == 0) base += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *a.total = base;
+}
+
+__global__ void __launch_bounds__(EXP_THREADS) k_exp_write(ExportArgs a) {
+  const int64_t beg = (int64_t)blockIdx.x * EXP_THREADS * EXP_ITEMS;
+  __shared__ unsigned ws[EXP_THREADS / 32];
+  const int l = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned long long done = a.blkoff[blockIdx.x];
+  for (int k = 0; k < EXP_ITEMS; ++k) {
+    const int64_t i = beg + k * EXP_THREADS + threadIdx.x;
+    const int64_t j = a.off + i;
+    int qi = DEAD;
+    if (i < a.nl) qi = a.ion.qind[j];
+    const bool live = qi != DEAD;
+    const unsigned bal = __ballot_sync(0xffffffffu, live);
+    if (l == 0) ws[w] = __popc(bal);
+    __syncthreads();
+    unsigned woff = 0, tot = 0;
+    for (int v = 0; v < EXP_THREADS / 32; ++v) { if (v < w) woff += ws[v]; tot += ws[v]; }
+    __syncthreads();  // ws is rewritten by the next tile
+    if (live) {
+      const int64_t o = (int64_t)(done + woff + __popc(bal & ((1u << l) - 1u)));
+      double q, vp, v1, v2;
+      if (a.mixed) {
+        const int c = a.ion.cell[j];
+        q = fma((double)a.ion.off[j], a.qGH[c] - a.qGL[c], a.qGL[c]);
+        vp = a.ion.fvpar[j];
+        v1 = a.ion.fv1[j];
+        v2 = a.ion.fv2[j];
+      } else {
+        const double rho = a.ion.rho[j], z = a.ion.z[j];
+        const double r2 = rho * rho + z * z, r = sqrt(r2);
+        q = (RE * RE) * (z / r) / r2;
+        vp = a.ion.vpar[j];
+        v1 = a.ion.v1[j];
+        v2 = a.ion.v2[j];
+      }
+      if (a.q) a.q[o] = q;
+      if (a.vpar) a.vpar[o] = vp;
+      if (a.v1) a.v1[o] = v1;
+      if (a.v2) a.v2[o] = v2;
+      if (a.qind) a.qind[o] = qi;
+    }
+    done += tot;
+  }
+}
+
+}  // namespace kaos

@@ -161,11 +161,22 @@ class Solver:
         self._check(load().kaos_get_counts(self.h, tube, _p(out), n))
         return out
 
-    def state(self, tube=0):
-        """The ions' field-line state: q, V||, Vperp1, Vperp2, Qindk1."""
+    def state(self, tube=0, out=None):
+        """The ions' field-line state: q, V||, Vperp1, Vperp2, Qindk1.  With
+        `out` (arrays q, vpar, vperp1, vperp2 float64 and qind int32 of at
+        least the ion count, e.g. in pinned host memory) the state is
+        written into views of those arrays."""
         ni, _ = self.count(tube)
-        q, vp, v1, v2 = (np.zeros(ni) for _ in range(4))
-        qi = np.zeros(ni, dtype=np.int32)
+        if out is None:
+            q, vp, v1, v2 = (np.zeros(ni) for _ in range(4))
+            qi = np.zeros(ni, dtype=np.int32)
+        else:
+            q, vp, v1, v2 = (out[k][:ni] for k in ("q", "vpar", "vperp1", "vperp2"))
+            qi = out["qind"][:ni]
+            if not (all(a.dtype == np.float64 and a.flags.c_contiguous and len(a) == ni
+                        for a in (q, vp, v1, v2)) and qi.dtype == np.int32 and len(qi) == ni):
+                raise ValueError("out: float64 q/vpar/vperp1/vperp2 and int32 qind "
+                                 f"arrays of at least {ni} elements")
         self._check(load().kaos_get_particles(self.h, tube, _p(q), _p(vp), _p(v1),
                                               _p(v2), _p(qi), ni))
         return dict(q=q, vpar=vp, vperp1=v1, vperp2=v2, qind=qi)

@@ -114,3 +114,36 @@ def test_empty_and_single_ion_entries():
         o.step(10)
         _compare(s, k, o)
     assert s.count(0)[0] > 0
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_state_export_skips_converted_slots(mixed):
+    """kaos_get_particles (device export) between master steps, while slots
+    converted to ENAs are still in the ion arrays: the live ions in order,
+    the same into caller-provided arrays, and n must equal the live count."""
+    mi, spec, tube, vg = grids.config_small(n_particles=6000, three_d=True,
+                                            steps_per_master=5, collisions=True)
+    if mixed:
+        mi.precision = KAOS_PREC_MIXED
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=17)
+    s = Solver(mi, [tube], vg)
+    s.load(0, q, vpar, v1, v2)
+    s.step(8)  # master step at 5; conversions at 6..8 leave dead slots
+    ni, ne = s.count()
+    assert ne > 0
+    a = s.state()
+    assert len(a["q"]) == ni
+    assert np.all(a["qind"] >= -2)
+    out = {k: np.full(ni + 7, np.nan) for k in ("q", "vpar", "vperp1", "vperp2")}
+    out["qind"] = np.full(ni + 7, 99, dtype=np.int32)
+    b = s.state(out=out)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    assert np.isnan(out["q"][ni]) and out["qind"][ni] == 99  # nothing past n
+    from kaos_b200.lib import load
+    import ctypes as C
+    buf = np.zeros(ni + 1)
+    rc = load().kaos_get_particles(s.h, 0, buf.ctypes.data_as(C.c_void_p), None,
+                                   None, None, None, ni + 1)
+    assert rc != 0
+    s.close()
