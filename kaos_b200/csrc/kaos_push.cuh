@@ -754,7 +754,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     const double ct = q0 * u * u;
     const double r = u * RE;
     const double rho0 = r * st, z0 = r * ct;
-    const int qi = cell_search_from(E, T.nq, T.sgn * q0, c0);
+    // an offset strictly inside (0, 1) puts q0 inside cell c0 (its FP64
+    // rounding is far below the margin): no edge search
+    const int qi = (o0 > 1e-6f && o0 < 1.0f - 1e-6f)
+                       ? c0 : cell_search_from(E, T.nq, T.sgn * q0, c0);
     // ---- k1 geometry in FP32 ---------------------------------------------
     Geo<float> g1;
     g1.ct = (float)ct;
@@ -824,9 +827,18 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     double y = (double)rsq((float)r2);
     y = y * fma(-0.5 * r2 * y, y, 1.5);
     const double qN = (RE * RE) * xz * (y * y * y);
-    const int cN = cell_search_from(E, T.nq, T.sgn * qN, qi >= 0 ? qi : c0);
-    const int cpos = cN >= 0 ? cN : (cN == BELOW ? 0 : T.nq - 1);
-    const float oN = (float)((qN - QL[cpos]) * IDQ[cpos]);
+    // the new cell: most ions stay in the cell they started the step in,
+    // and an offset strictly inside (0, 1) there decides it without the
+    // edge search; escaped ions keep the end cell and an offset outside
+    const int cs = qi >= 0 ? qi : c0;
+    double od = (qN - QL[cs]) * IDQ[cs];
+    int cpos = cs;
+    if (!(od > 1e-6 && od < 1.0 - 1e-6)) {
+      const int cN = cell_search_from(E, T.nq, T.sgn * qN, cs);
+      cpos = cN >= 0 ? cN : (cN == BELOW ? 0 : T.nq - 1);
+      od = (qN - QL[cpos]) * IDQ[cpos];
+    }
+    const float oN = (float)od;
     // ---- V|| along the new field direction (FP32) -----------------------
     const Geo<float> gN = geo((float)xr, (float)xz);
     const float vparN = gN.er * VNr + gN.ez * VNz;
