@@ -160,14 +160,17 @@ def run_large(args, precision, steps):
     s = Solver(mi, [tube], vg)
     s.init_particles(0, tube._counts, seed=20261203, **grids.C3_TAIL)
     s.set_graph(precision == KAOS_PREC_MIXED)
+    if args.launch:
+        s.set_launch(*(int(x) for x in args.launch.split(",")))
     s.step(args.warmup)
     n0, _ = s.count()
     s.step(steps)
     ms, _ = s.timing()
     n1, _ = s.count()
+    launch = s.launch()
     s.close()
     n = 0.5 * (n0 + n1)
-    return dict(value=n * steps / (ms * 1e-3), ms=ms / steps, n=n)
+    return dict(value=n * steps / (ms * 1e-3), ms=ms / steps, n=n, launch=launch)
 
 
 def mixed_moment_error(s32, s64):
@@ -330,12 +333,14 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--large-particles", type=int, default=100_000_000,
                     help="ions of the large single-tube line (0: skip it)")
-    ap.add_argument("--only", default="all", choices=["all", "mixed"],
-                    help="mixed: time the mixed path alone (for profiling)")
+    ap.add_argument("--only", default="all", choices=["all", "mixed", "large"],
+                    help="mixed: time the mixed path alone; large: the large single "
+                         "tube's mixed path alone (both for profiling)")
     ap.add_argument("--launch", default=None,
                     help="fixed push launch shape CHUNK,MODE instead of the autotuner "
                          "(CHUNK ions per work item 1024/2048/4096; MODE bit 0 persistent "
-                         "grid, bit 1 80-register mixed push)")
+                         "grid, bits 1-2 mixed push register budget 0: 64, 1: 80, "
+                         "2: 72 with 128-thread blocks)")
     args = ap.parse_args()
     if args.impl == "reference":
         line = reference_arm(args)
@@ -343,6 +348,13 @@ def main():
             print(json.dumps(line), flush=True)
         return
     import torch
+    if args.only == "large":
+        from kaos_b200.model_input import KAOS_PREC_MIXED
+        l32 = run_large(args, KAOS_PREC_MIXED, args.steps)
+        print(json.dumps({"large_mixed": l32["value"], "ms_per_step": l32["ms"],
+                          "n": l32["n"], "steps": args.steps, "launch": l32["launch"]}),
+              flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

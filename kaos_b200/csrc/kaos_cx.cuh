@@ -51,13 +51,19 @@ __device__ __forceinline__ unsigned cx_need(const CxArgs &a, double nu) {
 // the per-chunk totals.
 // A cell with no conversion does nothing; the scan of a cell stops after the
 // tile of chunks in which its prefix reaches the conversion count, and
-// cxend records the first chunk without a written prefix.
+// cxend records the first chunk without a written prefix.  Only the chunks
+// holding live ions are scanned: the push writes no count beyond them.
+__device__ __forceinline__ int cx_live_end(const CxArgs &a, int t) {
+  const int c0 = a.tube_cx0[t], c1 = a.tube_cx0[t + 1];
+  return (int)min((int64_t)c1, c0 + ceil_div(a.nlive[t], (int64_t)CX_CHUNK));
+}
+
 __global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
   const int t = cell_tube[blockIdx.x], k = cell_q[blockIdx.x];
   const TubeD &T = a.tubes[t];
   const unsigned need = cx_need(a, a.ct.nuPoi[T.coff + k]);
   if (need == 0u) return;
-  const int c0 = a.tube_cx0[t], c1 = a.tube_cx0[t + 1];
+  const int c0 = a.tube_cx0[t], c1 = cx_live_end(a, t);
   __shared__ unsigned wsum[32];
   __shared__ unsigned base;
   if (threadIdx.x == 0) base = 0;
@@ -92,35 +98,34 @@ __global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
 }
 
 // ENA slots in ion-index order: exclusive scan of the per-chunk conversion
-// totals over the chunks of each tube (one block per tube); the ENA count
-// of the tube advances by the step's total.
+// totals over the live chunks of each tube (one block per tube, each thread
+// a run of consecutive chunks: run sums, one block scan, run prefixes); the
+// ENA count of the tube advances by the step's total.
 __global__ void k_cx_base(CxArgs a) {
   const int t = blockIdx.x;
-  const int c0 = a.tube_cx0[t], c1 = a.tube_cx0[t + 1];
+  const int c0 = a.tube_cx0[t], c1 = cx_live_end(a, t);
   __shared__ unsigned long long wsum[32];
-  __shared__ unsigned long long base;
   const int64_t n0 = a.nena[t];
-  if (threadIdx.x == 0) base = 0;
-  __syncthreads();
   const int l = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int r0 = c0; r0 < c1; r0 += blockDim.x) {
-    const int c = r0 + threadIdx.x;
-    const unsigned long long n = (c < c1) ? a.cxconv[c] : 0ull;
-    unsigned long long x = n;
-    for (int o = 1; o < 32; o <<= 1) {
-      unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-      if (l >= o) x += y;
-    }
-    if (l == 31) wsum[w] = x;
-    __syncthreads();
-    unsigned long long woff = 0, tot = 0;
-    for (int v = 0; v < nw; ++v) { if (v < w) woff += wsum[v]; tot += wsum[v]; }
-    if (c < c1) a.cxbase[c] = n0 + (int64_t)(base + woff + x - n);
-    __syncthreads();
-    if (threadIdx.x == 0) base += tot;
-    __syncthreads();
+  const int run = (int)ceil_div((int64_t)max(c1 - c0, 0), (int64_t)blockDim.x);
+  const int r0 = c0 + (int)threadIdx.x * run, r1 = min(r0 + run, c1);
+  unsigned long long n = 0;
+  for (int c = r0; c < r1; ++c) n += a.cxconv[c];
+  unsigned long long x = n;  // inclusive warp scan of the run sums
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (l >= o) x += y;
   }
-  if (threadIdx.x == 0) a.nena[t] = n0 + (int64_t)base;
+  if (l == 31) wsum[w] = x;
+  __syncthreads();
+  unsigned long long woff = 0, tot = 0;
+  for (int v = 0; v < nw; ++v) { if (v < w) woff += wsum[v]; tot += wsum[v]; }
+  unsigned long long s = woff + x - n;  // exclusive prefix of this run
+  for (int c = r0; c < r1; ++c) {
+    a.cxbase[c] = n0 + (int64_t)s;
+    s += a.cxconv[c];
+  }
+  if (threadIdx.x == 0) a.nena[t] = n0 + (int64_t)tot;
 }
 
 // Cartesian unit vectors along B (par), across the shell (p) and in
@@ -144,6 +149,9 @@ __global__ void k_cx_convert(CxArgs a) {
   const int t = a.cx_tube[c];
   const TubeD &T = a.tubes[t];
   unsigned *crow = a.cxc + (int64_t)c * a.nqmax;
+  // a chunk without live ions has no counts (the push wrote none since the
+  // last clear)
+  if (a.cx_start[c] >= a.nlive[t]) return;
   const unsigned nconv = a.cxconv[c];
   if (nconv == 0u) {
     for (int k = threadIdx.x; k < T.nq; k += blockDim.x) crow[k] = 0u;

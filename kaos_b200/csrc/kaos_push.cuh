@@ -644,12 +644,57 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   }  // work items
 }
 
+// The force switches of apar as 0/1 factors: the same a|| without branches
+// (s * (m - |AG| + |AEA|) + AEA with the switched-off terms multiplied by 0;
+// the sign s = -1 south of the equator).
+struct ForceC {
+  float cm, cg, ce1, ce2;  // mirror, gravity, signed / unsigned ambipolar
+};
+__device__ __forceinline__ ForceC force_c(const ForceFlags &f) {
+  return ForceC{f.mirror ? 1.0f : 0.0f, f.grav ? 1.0f : 0.0f,
+                (f.eamb && f.eambsign) ? 1.0f : 0.0f,
+                (f.eamb && !f.eambsign) ? 1.0f : 0.0f};
+}
+__device__ __forceinline__ float apar_bf(const Geo<float> &g, float vperp2,
+                                         float aea, float ag, const ForceC &f) {
+  const float m = 1.5f * vperp2 * fabsf(g.ct) * g.ir *
+                  (2.0f + g.st * g.st * g.isl * g.isl) * g.isl;
+  const float s = g.ct <= 0.0f ? -1.0f : 1.0f;
+  return s * (f.cm * m - f.cg * fabsf(ag) + f.ce2 * fabsf(aea)) + f.ce1 * aea;
+}
+
+// Start-of-step velocity bins of one ion: (V⊥1, V⊥2, V∥) on the 3D grid;
+// on the 2D grid (|V⊥|, V∥) with the previous bin kept for a value outside
+// the grid (the stale-index rule), stored back when it changed.
+template <bool THREE_D>
+__device__ __forceinline__ void start_bins(const PushArgs &a, const Ions &I,
+                                           int64_t j, const float *VE1,
+                                           const float *VE2, const float *VEP,
+                                           float vpar, float v1, float v2,
+                                           float vp2, int &b1, int &b2, int &bp) {
+  b2 = -1;
+  if (THREE_D) {
+    bp = vbin(VEP, c_vg.npar, vpar);
+    b1 = vbin(VE1, c_vg.n1, v1);
+    b2 = vbin(VE2, c_vg.n2, v2);
+  } else {
+    const int old = I.vb[j];
+    const int np_ = vbin(VEP, c_vg.npar, vpar);
+    const int n1_ = vbin(VE1, c_vg.n1, sqrtf(vp2));
+    bp = np_ >= 0 ? np_ : (old & 0xffff) - 1;
+    b1 = n1_ >= 0 ? n1_ : (old >> 16) - 1;
+    const int nw = ((b1 + 1) << 16) | (bp + 1);
+    if (nw != old && !a.bin_only) I.vb[j] = nw;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Mixed kernel: position = (cell, FP32 offset in q); FP32 velocities and RK
 // stages; FP64 for the q reconstruction, the quartic root (Newton from a
 // per-cell linear guess) and the renormalised q of the new position.
-// MINB = resident blocks per SM the register budget is sized for (4: 64
-// registers, 3: 80); the autotuner picks one.
+// NT threads per block and MINB resident blocks per SM set the register
+// budget (256 x 4: 64 registers, 256 x 3: 80, 128 x 7: 72); the autotuner
+// picks one.
 template <bool THREE_D, int NT, int MINB, bool PERSIST>
 __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   extern __shared__ __align__(16) double sm[];
@@ -663,6 +708,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
   const uint32_t step = a.dstep ? *a.dstep : a.step;
   const float fRE = (float)RE;
+  const ForceC fc = force_c(a.ff);
   Ions I = a.ion;
   TubeD T;
   int tcur = -1;
@@ -769,28 +815,14 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     g1.er = 3.0f * g1.ct * g1.st * g1.isl;
     g1.ez = (3.0f * g1.ct * g1.ct - 1.0f) * g1.isl;
     const float vp2 = v1 * v1 + v2 * v2;
-    int b1 = -1, b2 = -1, bp = -1;
-    if (THREE_D) {
-      if (a.bin) {
-        bp = vbin(VEP, c_vg.npar, vpar);
-        b1 = vbin(VE1, c_vg.n1, v1);
-        b2 = vbin(VE2, c_vg.n2, v2);
-      }
-    } else {
-      const int old = I.vb[j];
-      const int np_ = vbin(VEP, c_vg.npar, vpar);
-      const int n1_ = vbin(VE1, c_vg.n1, sqrtf(vp2));
-      bp = np_ >= 0 ? np_ : (old & 0xffff) - 1;
-      b1 = n1_ >= 0 ? n1_ : (old >> 16) - 1;
-      const int nw = ((b1 + 1) << 16) | (bp + 1);
-      if (nw != old && !a.bin_only) I.vb[j] = nw;
-    }
-    if (a.bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
     if (a.bin_only) {
+      int b1, b2, bp;
+      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, vpar, v1, v2, vp2, b1, b2, bp);
+      if (a.bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
       if (a.write_qind) I.qind[j] = qi;
       continue;
     }
-    const float a1 = apar(g1, vp2, aea, ag, a.ff);
+    const float a1 = apar_bf(g1, vp2, aea, ag, fc);
     float v1n = v1, v2n = v2;
     if (a.icr && qi >= 0) {
       const float rf = (float)r;
@@ -809,10 +841,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     const float rf = (float)rho0, zf = (float)z0;
     const float VRr = vpar * g1.er, VRz = vpar * g1.ez;
     const Geo<float> g2 = geo(fmaf(hh, VRr, rf), fmaf(hh, VRz, zf));
-    const float a2 = apar(g2, vp2, aea, ag, a.ff);
+    const float a2 = apar_bf(g2, vp2, aea, ag, fc);
     const float A1r = a1 * g1.er, A1z = a1 * g1.ez;
     const Geo<float> g4 = geo(rf + h * VRr + hsq2 * A1r, zf + h * VRz + hsq2 * A1z);
-    const float a4 = apar(g4, vp2, aea, ag, a.ff);
+    const float a4 = apar_bf(g4, vp2, aea, ag, fc);
     if (a.write_qk4) I.fqk4[j] = g4.q;
     const float A2r = a2 * g2.er, A2z = a2 * g2.ez;
     const float A4r = a4 * g4.er, A4z = a4 * g4.ez;
@@ -842,6 +874,11 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     // ---- V|| along the new field direction (FP32) -----------------------
     const Geo<float> gN = geo((float)xr, (float)xz);
     const float vparN = gN.er * VNr + gN.ez * VNz;
+    if (a.bin || !THREE_D) {
+      int b1, b2, bp;
+      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, vpar, v1, v2, vp2, b1, b2, bp);
+      if (a.bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
+    }
     if (!isfinite(vparN) || !isfinite(oN)) atomicOr(a.status, ST_NAN);
     I.cell[j] = cpos;
     I.off[j] = oN;
