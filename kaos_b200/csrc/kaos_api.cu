@@ -569,8 +569,20 @@ CxArgs cx_args(kaos_handle *h) {
   a.nranks = h->nranks;
   a.nqmax = max_nq(h);
   a.mixed = h->mixed;
+  a.ncx = h->ncx;
   a.status = h->d_status;
   return a;
+}
+
+// Blocks of a grid striding over n work items: a few per SM.
+static int strided_grid(kaos_handle *h, int n) {
+  if (!h->nsm) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      h->nsm = 148;
+  }
+  return std::max(1, std::min(n, 4 * h->nsm));
 }
 
 // charge exchange at the start of a step (_8_KineticSolver.f90:95-166)
@@ -581,7 +593,7 @@ int launch_cx(kaos_handle *h) {
   // 1024 threads: one tile covers the chunks of a tube of up to 16.7 M ions
   k_cx_scan<<<(int)h->ncell, 1024, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
   k_cx_base<<<h->ntubes, 1024, 0, h->s>>>(a);
-  k_cx_convert<<<h->ncx, 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
+  k_cx_convert<<<strided_grid(h, h->ncx), 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
   h->launches += 3;
   CK(cudaGetLastError());
   return KAOS_OK;
@@ -594,6 +606,8 @@ int launch_push_ena(kaos_handle *h, int bin) {
   a.tubes = h->d_tubes;
   a.blk_tube = h->d_eblk_tube;
   a.blk_start = h->d_eblk_start;
+  a.tube_blk0 = h->d_tube_eblk0;
+  a.nitems = h->neblk;
   a.chunk = PUSH_THREADS * PUSH_ITEMS;
   a.nena = h->d_nena;
   a.ct = h->ct;
@@ -601,7 +615,7 @@ int launch_push_ena(kaos_handle *h, int bin) {
   a.h = h->P.h;
   a.grav_GM = GG * ME;
   a.grav = h->P.GRAVflag == 1;
-  k_push_ena<<<h->neblk, PUSH_THREADS, (size_t)(max_nq(h) + 1) * sizeof(double), h->s>>>(a);
+  k_push_ena<<<strided_grid(h, h->neblk), PUSH_THREADS, (size_t)(max_nq(h) + 1) * sizeof(double), h->s>>>(a);
   h->launches++;
   CK(cudaGetLastError());
   return KAOS_OK;

@@ -35,6 +35,7 @@ struct CxArgs {
   int64_t *cxbase;           // per chunk: ENA slot of its first conversion
   int *cxend;                // per cell (all tubes): chunks >= cxend convert none
   int nqmax, mixed;
+  int ncx;                   // selection chunks (all tubes)
   int rank, nranks;          // this rank's share of a split tube's conversions
   uint32_t *status;
 };
@@ -141,17 +142,20 @@ __device__ __forceinline__ void dipole_frame(double ct, double st, double cp,
   e_phi[0] = -sp;    e_phi[1] = cp;     e_phi[2] = 0.0;
 }
 
+// The first item at or after `first` that belongs to this block of a grid
+// striding over work items (item = blockIdx.x mod gridDim.x).
+__device__ __forceinline__ int next_own_item(int first) {
+  const int G = (int)gridDim.x;
+  return first + (((int)blockIdx.x - first) % G + G) % G;
+}
+
 // in-order conversion of the first need[Q] eligible ions per cell; the
 // converted ions of a chunk take consecutive ENA slots from cxbase in index
-// order (every block also clears its chunk's count row for the next push)
-__global__ void k_cx_convert(CxArgs a) {
-  const int c = blockIdx.x;
-  const int t = a.cx_tube[c];
+// order (the chunk's count row is also cleared for the next push)
+__device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) {
   const TubeD &T = a.tubes[t];
   unsigned *crow = a.cxc + (int64_t)c * a.nqmax;
-  // a chunk without live ions has no counts (the push wrote none since the
-  // last clear)
-  if (a.cx_start[c] >= a.nlive[t]) return;
+  __syncthreads();  // the previous chunk of this block is done with smem
   const unsigned nconv = a.cxconv[c];
   if (nconv == 0u) {
     for (int k = threadIdx.x; k < T.nq; k += blockDim.x) crow[k] = 0u;
@@ -279,6 +283,22 @@ __global__ void k_cx_convert(CxArgs a) {
   }
 }
 
+// A grid striding over the selection chunks; a chunk without live ions has
+// no counts (the push wrote none since the last clear), and neither has any
+// later chunk of its tube: the block moves on to the next tube.
+__global__ void k_cx_convert(CxArgs a) {
+  int c = blockIdx.x;
+  while (c < a.ncx) {
+    const int t = a.cx_tube[c];
+    if (a.cx_start[c] >= a.nlive[t]) {
+      c = next_own_item(a.tube_cx0[t + 1]);
+      continue;
+    }
+    cx_convert_chunk(a, c, t);
+    c += gridDim.x;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Ballistic ENA step under gravity (FP64): the ENA branch of
 // KineticUpdateA/B/C and KineticRK4UpdateSub, including the reference's
@@ -288,6 +308,8 @@ struct EnaArgs {
   const TubeD *tubes;
   const int *blk_tube;
   const int64_t *blk_start;
+  const int *tube_blk0;  // first work item of each tube (ntubes + 1)
+  int nitems;            // work items (tube, chunk of ENA slots)
   int chunk;
   const int64_t *nena;
   CellTables ct;
@@ -332,19 +354,31 @@ __device__ __forceinline__ void ena_acc(const EnaArgs &a, const double x[3],
   A[0] = g * x[0]; A[1] = g * x[1]; A[2] = g * x[2];
 }
 
+// A grid striding over the (tube, chunk) items; the first idle item of a
+// tube (its ENAs end before it) sends the block on to the next tube.
 __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
   extern __shared__ double sm[];
-  const int t = a.blk_tube[blockIdx.x];
+  double *E = sm;
+  const double h = a.h, hh = 0.5 * h, h6 = h / 6.0, hsq2 = 0.5 * h * h;
+  int tcur = -1;
+  int item = blockIdx.x;
+  while (item < a.nitems) {
+  const int t = a.blk_tube[item];
   const TubeD &T = a.tubes[t];
   const int64_t nl = min(a.nena[t], T.ecap);
-  const int64_t beg = a.blk_start[blockIdx.x];
-  if (beg >= nl) return;  // whole block idle: before any barrier
+  const int64_t beg = a.blk_start[item];
+  if (beg >= nl) {  // uniform over the block
+    item = next_own_item(a.tube_blk0[t + 1]);
+    continue;
+  }
   const int64_t end = min(beg + (int64_t)a.chunk, nl);
-  double *E = sm;
-  for (int k = threadIdx.x; k <= T.nq; k += blockDim.x)
-    E[k] = (k < T.nq) ? T.sgn * a.ct.qGL[T.coff + k] : T.sgn * a.ct.qGH[T.coff + T.nq - 1];
-  __syncthreads();
-  const double h = a.h, hh = 0.5 * h, h6 = h / 6.0, hsq2 = 0.5 * h * h;
+  if (t != tcur) {
+    __syncthreads();  // the previous tube's edges are no longer read
+    for (int k = threadIdx.x; k <= T.nq; k += blockDim.x)
+      E[k] = (k < T.nq) ? T.sgn * a.ct.qGL[T.coff + k] : T.sgn * a.ct.qGH[T.coff + T.nq - 1];
+    __syncthreads();
+    tcur = t;
+  }
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t e = T.eoff + i;
     double x[3] = {a.ena.x[e], a.ena.y[e], a.ena.z[e]};
@@ -405,6 +439,8 @@ __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
     a.ena.vphs[e] = vphs;
     a.ena.qind[e] = qi;
   }
+  item += gridDim.x;
+  }  // work items
 }
 
 // ENA moments of one master step from the ENA counts and (Vp, Vq, Vphi)
