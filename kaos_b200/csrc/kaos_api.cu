@@ -593,7 +593,9 @@ int launch_cx(kaos_handle *h) {
   // 1024 threads: one tile covers the chunks of a tube of up to 16.7 M ions
   k_cx_scan<<<(int)h->ncell, 1024, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
   k_cx_base<<<h->ntubes, 1024, 0, h->s>>>(a);
-  k_cx_convert<<<strided_grid(h, h->ncx), 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
+  // one block per chunk (a chunk with conversions walks its ions in order;
+  // blocks of chunks without live ions leave at once)
+  k_cx_convert<<<std::max(h->ncx, 1), 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
   h->launches += 3;
   CK(cudaGetLastError());
   return KAOS_OK;
