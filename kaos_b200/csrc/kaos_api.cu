@@ -309,21 +309,22 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
   smem += (size_t)BIN_WIN * (1 + h->vg.npar + h->vg.n1 + (h->three_d ? h->vg.n2 : 0)) *
           sizeof(unsigned);  // block-private binning window
   const int rs = h->mixed ? h->regsel : 0, ps = h->persistent;
-  // kernel variant: [three_d][register budget][persistent]; the budgets:
-  // 64 registers (4 blocks of 256 threads per SM), 80 (3 blocks of 256),
-  // 72 (7 blocks of 128)
+  // kernel variant: [master-step work][three_d][register budget][persistent];
+  // the budgets: 64 registers (4 blocks of 256 threads per SM), 80 (3
+  // blocks of 256), 72 (7 blocks of 128)
   using KFn = void (*)(PushArgs);
-  static const KFn k32[2][3][2] = {
-      {{k_push32<false, 256, 4, false>, k_push32<false, 256, 4, true>},
-       {k_push32<false, 256, 3, false>, k_push32<false, 256, 3, true>},
-       {k_push32<false, 128, 7, false>, k_push32<false, 128, 7, true>}},
-      {{k_push32<true, 256, 4, false>, k_push32<true, 256, 4, true>},
-       {k_push32<true, 256, 3, false>, k_push32<true, 256, 3, true>},
-       {k_push32<true, 128, 7, false>, k_push32<true, 128, 7, true>}}};
+#define KAOS_K32(M, D)                                                        \
+  {{k_push32<D, 256, 4, false, M>, k_push32<D, 256, 4, true, M>},            \
+   {k_push32<D, 256, 3, false, M>, k_push32<D, 256, 3, true, M>},            \
+   {k_push32<D, 128, 7, false, M>, k_push32<D, 128, 7, true, M>}}
+  static const KFn k32[2][2][3][2] = {{KAOS_K32(false, false), KAOS_K32(false, true)},
+                                      {KAOS_K32(true, false), KAOS_K32(true, true)}};
+#undef KAOS_K32
+  const int ms = (a.bin || a.prologue || a.bin_only) ? 1 : 0;
   const int nt = rs == 2 ? 128 : PUSH_THREADS;
   static const KFn k64[2][2] = {{k_push64<false, false>, k_push64<false, true>},
                                 {k_push64<true, false>, k_push64<true, true>}};
-  const KFn fn = h->mixed ? k32[h->three_d][rs][ps] : k64[h->three_d][ps];
+  const KFn fn = h->mixed ? k32[ms][h->three_d][rs][ps] : k64[h->three_d][ps];
   if (smem > 48 * 1024)
     CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (!h->occ[rs]) {

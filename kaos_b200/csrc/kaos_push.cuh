@@ -695,8 +695,12 @@ __device__ __forceinline__ void start_bins(const PushArgs &a, const Ions &I,
 // NT threads per block and MINB resident blocks per SM set the register
 // budget (256 x 4: 64 registers, 256 x 3: 80, 128 x 7: 72); the autotuner
 // picks one.
-template <bool THREE_D, int NT, int MINB, bool PERSIST>
+template <bool THREE_D, int NT, int MINB, bool PERSIST, bool MASTER>
 __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
+  // master-step work (field re-interpolation, binning) only in the MASTER
+  // variant: the ordinary step carries none of its code or registers
+  const bool bin = MASTER && a.bin, prologue = MASTER && a.prologue,
+             bin_only = MASTER && a.bin_only;
   extern __shared__ __align__(16) double sm[];
   const int nqmax = a.nqs;
   double *E = sm, *Cc = sm + nqmax + 1;
@@ -714,7 +718,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   int tcur = -1;
   // velocity-cell edges for the bin searches in shared memory
   __shared__ float VE1[MAXV + 1], VE2[MAXV + 1], VEP[MAXV + 1];
-  if (a.bin || !THREE_D) load_vgrid_smem(c_vg.f1, c_vg.f2, c_vg.fpar, VE1, VE2, VEP);
+  if (bin || !THREE_D) load_vgrid_smem(c_vg.f1, c_vg.f2, c_vg.fpar, VE1, VE2, VEP);
   // one work item per block, or a persistent grid striding over the items
   for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
   const int t = a.blk_tube[item];
@@ -750,7 +754,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   if (a.cxc)
     for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
   BinWin W{};
-  if (a.bin) W = bin_win_init(HC + nqmax, max(a.ion.cell[T.off + beg], 0), T.nq);
+  if (bin) W = bin_win_init(HC + nqmax, max(a.ion.cell[T.off + beg], 0), T.nq);
   __syncthreads();
   const float invsumds = (float)(1.0 / T.sumdsICR);
   const double ipG = 1.0 / T.pG;
@@ -783,7 +787,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       if (a.icr) n_id = I.id[jn];
     }
     if (c0 == DEAD) continue;
-    if (a.prologue) {
+    if (prologue) {
       double da = aea, dg = ag;
       field_prologue(a, T, E, Cc, (double)I.fqk4[j], c0, da, dg);
       aea = (float)da;
@@ -815,10 +819,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     g1.er = 3.0f * g1.ct * g1.st * g1.isl;
     g1.ez = (3.0f * g1.ct * g1.ct - 1.0f) * g1.isl;
     const float vp2 = v1 * v1 + v2 * v2;
-    if (a.bin_only) {
+    if (bin_only) {
       int b1, b2, bp;
       start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, vpar, v1, v2, vp2, b1, b2, bp);
-      if (a.bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
+      if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
       if (a.write_qind) I.qind[j] = qi;
       continue;
     }
@@ -874,10 +878,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     // ---- V|| along the new field direction (FP32) -----------------------
     const Geo<float> gN = geo((float)xr, (float)xz);
     const float vparN = gN.er * VNr + gN.ez * VNz;
-    if (a.bin || !THREE_D) {
+    if (bin || !THREE_D) {
       int b1, b2, bp;
       start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, vpar, v1, v2, vp2, b1, b2, bp);
-      if (a.bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
+      if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
     }
     if (!isfinite(vparN) || !isfinite(oN)) atomicOr(a.status, ST_NAN);
     I.cell[j] = cpos;
@@ -887,14 +891,14 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       I.fv1[j] = v1n;
       I.fv2[j] = v2n;
     }
-    if (a.prologue) {
+    if (prologue) {
       I.faea[j] = aea;
       I.fag[j] = ag;
     }
     if (a.write_qind) I.qind[j] = qi;
     if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);
   }
-  if (a.bin) bin_win_flush(a.acc, T, W);
+  if (bin) bin_win_flush(a.acc, T, W);
   if (a.cxc) flush_cx_counts(a, t, beg, T.nq, HC);
   if (!PERSIST) break;  // one item per block: no loop-carried state
   }  // work items
