@@ -84,6 +84,10 @@ struct kaos_handle {
   VGridC evg{};  // ENA velocity grid (Vp = 1, Vq = par, Vphi = 2)
   cudaStream_t s = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // side stream of the ENA push, which runs beside the ion push (fork after
+  // the charge exchange, join before anything that follows the pushes)
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t efork = nullptr, ejoin = nullptr;
   // device
   TubeD *d_tubes = nullptr;
   int *d_blk_tube = nullptr;
@@ -602,7 +606,11 @@ int launch_cx(kaos_handle *h) {
   return KAOS_OK;
 }
 
+// The ENA push on the side stream, forked from the main stream here; the
+// caller joins it (join_push_ena) after the ion push.
 int launch_push_ena(kaos_handle *h, int bin) {
+  CK(cudaEventRecord(h->efork, h->s));
+  CK(cudaStreamWaitEvent(h->s2, h->efork, 0));
   EnaArgs a{};
   a.acc = h->acc;
   a.bin = bin;
@@ -618,9 +626,15 @@ int launch_push_ena(kaos_handle *h, int bin) {
   a.h = h->P.h;
   a.grav_GM = GG * ME;
   a.grav = h->P.GRAVflag == 1;
-  k_push_ena<<<strided_grid(h, h->neblk), PUSH_THREADS, (size_t)(max_nq(h) + 1) * sizeof(double), h->s>>>(a);
+  k_push_ena<<<strided_grid(h, h->neblk), PUSH_THREADS, (size_t)(max_nq(h) + 1) * sizeof(double), h->s2>>>(a);
   h->launches++;
   CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ejoin, h->s2));
+  return KAOS_OK;
+}
+
+int join_push_ena(kaos_handle *h) {
+  CK(cudaStreamWaitEvent(h->s, h->ejoin, 0));
   return KAOS_OK;
 }
 
@@ -725,8 +739,10 @@ int step_once(kaos_handle *h) {
   p.write_qind = (!h->mixed) || next_master || qx || h->export_on;
   p.write_qk4 = next_master || qx;
   if (qx) p.cxc = h->d_cxc;
-  if ((rc = launch_push(h, p))) return rc;
+  // the ENA push (independent of the ions) runs beside the ion push
   if (qx && (rc = launch_push_ena(h, master))) return rc;
+  if ((rc = launch_push(h, p))) return rc;
+  if (qx && (rc = join_push_ena(h))) return rc;
   if (master) {
     if (h->P.LBCONDITIONflag == 1 && (rc = launch_inject(h, 0))) return rc;
     if (h->P.UBCONDITIONflag == 1 && (rc = launch_inject(h, 1))) return rc;
@@ -989,8 +1005,11 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   *out = h;
   int rc;
   CK(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking));
   CK(cudaEventCreate(&h->e0));
   CK(cudaEventCreate(&h->e1));
+  CK(cudaEventCreateWithFlags(&h->efork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ejoin, cudaEventDisableTiming));
   CellTables &c = h->ct;
   c.ncell_total = coff;
   double *tmp;
@@ -1690,11 +1709,15 @@ int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches) {
 void kaos_destroy(kaos_handle *h) {
   if (!h) return;
   if (h->s) cudaStreamSynchronize(h->s);
+  if (h->s2) cudaStreamSynchronize(h->s2);
   for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
   for (auto e : h->pev) cudaEventDestroy(e);
   for (void *p : h->allocs) cudaFree(p);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
+  if (h->efork) cudaEventDestroy(h->efork);
+  if (h->ejoin) cudaEventDestroy(h->ejoin);
+  if (h->s2) cudaStreamDestroy(h->s2);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;
 }
