@@ -333,9 +333,10 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--large-particles", type=int, default=100_000_000,
                     help="ions of the large single-tube line (0: skip it)")
-    ap.add_argument("--only", default="all", choices=["all", "mixed", "large"],
+    ap.add_argument("--only", default="all", choices=["all", "mixed", "large", "cadence1"],
                     help="mixed: time the mixed path alone; large: the large single "
-                         "tube's mixed path alone (both for profiling)")
+                         "tube's mixed path alone; cadence1: the mixed path with every "
+                         "step a master step (all for profiling)")
     ap.add_argument("--launch", default=None,
                     help="fixed push launch shape CHUNK,MODE instead of the autotuner "
                          "(CHUNK ions per work item 1024/2048/4096; MODE bit 0 persistent "
@@ -348,6 +349,14 @@ def main():
             print(json.dumps(line), flush=True)
         return
     import torch
+    if args.only == "cadence1":
+        from kaos_b200.model_input import KAOS_PREC_MIXED
+        r = run_ours(args, KAOS_PREC_MIXED, graph=True, ndatfac=1)
+        r["solver"].close()
+        print(json.dumps({"cadence1_mixed": r["value"], "ms_per_step": r["ms"] / args.steps,
+                          "push_ms": r["push_ms"], "steps": args.steps,
+                          "launch": r["launch"]}), flush=True)
+        return
     if args.only == "large":
         from kaos_b200.model_input import KAOS_PREC_MIXED
         l32 = run_large(args, KAOS_PREC_MIXED, args.steps)

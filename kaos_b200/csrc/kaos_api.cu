@@ -26,6 +26,10 @@ namespace {
 constexpr int PUSH_THREADS = 256;
 constexpr int PUSH_ITEMS = 8;
 constexpr int BC_THREADS = 256;
+// Removal at a master step marks the escaped ions DEAD in place; the ion
+// arrays are compacted (order-preserving) every BC_COMPACT_EVERY master
+// steps, or earlier when an injection could overflow a tube's capacity.
+constexpr int BC_COMPACT_EVERY = 8;
 // cells per tube: the per-cell tables of a tube live in shared memory (the
 // mixed push holds 84 bytes per cell, the collision-count kernel 64)
 constexpr int MAX_CELLS = 2048;
@@ -170,6 +174,12 @@ struct kaos_handle {
   std::vector<cudaEvent_t> pev;  // event pairs around push launches
   int npev = 0;
   double push_ms = 0.0;
+  // deferred compaction: master steps since the last one, the decision of
+  // master step bc_for, and per tube an upper bound of the occupied slots
+  int bc_since = 0;
+  int64_t bc_for = -1;
+  int bc_compact = 1;
+  std::vector<int64_t> bc_bound;
   char err[512] = {0};
 };
 
@@ -486,7 +496,76 @@ Fields ion_fields(kaos_handle *h, int from, int to) {
   return F;
 }
 
-int launch_boundary(kaos_handle *h) {
+// Ions one master step's injection may add to tube t.
+int64_t inject_max(const kaos_handle *h, int t) {
+  const TubeD &T = h->th[t];
+  int64_t k = 0;
+  if (h->P.LBCONDITIONflag == 1) k += std::max<int64_t>(0, std::llround(T.nsnormCLB));
+  if (h->P.UBCONDITIONflag == 1) k += std::max<int64_t>(0, std::llround(T.nsnormCUB));
+  return k;
+}
+
+// Whether master step n compacts the ion arrays (decided once per step, before
+// any capture of it): every BC_COMPACT_EVERY master steps, or when the next
+// injection could exceed a tube's capacity after the occupied slots are read
+// back (outside a capture only; inside one the step compacts).
+int bc_decide(kaos_handle *h, int64_t n) {
+  if (h->bc_for == n) return h->bc_compact;
+  int c = h->bc_since + 1 >= BC_COMPACT_EVERY;
+  bool tight = false;
+  for (int t = 0; t < h->ntubes && !c; ++t)
+    tight = tight || h->bc_bound[t] + inject_max(h, t) > h->th[t].cap;
+  if (!c && tight) {
+    std::vector<int64_t> nl(h->ntubes);
+    if (h->capturing || cudaStreamSynchronize(h->s) != cudaSuccess ||
+        cudaMemcpy(nl.data(), h->d_nlive, h->ntubes * sizeof(int64_t),
+                   cudaMemcpyDeviceToHost) != cudaSuccess) {
+      c = 1;
+    } else {
+      for (int t = 0; t < h->ntubes; ++t) {
+        h->bc_bound[t] = nl[t];
+        c = c || nl[t] + inject_max(h, t) > h->th[t].cap;
+      }
+    }
+  }
+  h->bc_for = n;
+  h->bc_compact = c;
+  return c;
+}
+
+// Host bookkeeping of a master step's removal and injection (eager, capture
+// and replay alike).
+void bc_after(kaos_handle *h, int compact) {
+  if (compact) {
+    h->cur = 1 - h->cur;
+    h->bc_since = 0;
+  } else {
+    ++h->bc_since;
+  }
+  for (int t = 0; t < h->ntubes; ++t) h->bc_bound[t] += inject_max(h, t);
+}
+
+int launch_boundary(kaos_handle *h, int compact) {
+  if (!compact) {
+    BcArgs b{};
+    b.tubes = h->d_tubes;
+    b.blk_tube = h->d_blk_tube;
+    b.blk_start = h->d_blk_start;
+    b.chunk = PUSH_THREADS * PUSH_ITEMS;
+    b.nlive = h->d_nlive;
+    b.lb_out = h->d_lb_out;
+    b.ub_out = h->d_ub_out;
+    b.qind_w = h->ion[h->cur].qind;
+    b.cell_w = h->mixed ? h->ion[h->cur].cell : nullptr;
+    CK(cudaMemsetAsync(h->d_lb_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
+    CK(cudaMemsetAsync(h->d_ub_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
+    CK(cudaMemsetAsync(h->d_lb_in, 0, h->ntubes * sizeof(unsigned long long), h->s));
+    CK(cudaMemsetAsync(h->d_ub_in, 0, h->ntubes * sizeof(unsigned long long), h->s));
+    k_bc_mark<<<h->nblk, BC_THREADS, 0, h->s>>>(b);
+    h->launches++;
+    CK(cudaGetLastError());
+    return KAOS_OK;
+  }
   BcArgs b{};
   b.tubes = h->d_tubes;
   b.blk_tube = h->d_blk_tube;
@@ -513,8 +592,7 @@ int launch_boundary(kaos_handle *h) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h->d_nlive, h->d_nlive_new, h->ntubes * sizeof(int64_t),
                      cudaMemcpyDeviceToDevice, h->s));
-  h->cur = 1 - h->cur;
-  return KAOS_OK;
+  return KAOS_OK;  // the caller swaps the buffer sets (bc_after)
 }
 
 int launch_inject(kaos_handle *h, int ub) {
@@ -727,7 +805,9 @@ int step_once(kaos_handle *h) {
   }
   if (qx && (rc = launch_cx(h))) return rc;
   if (master) {
-    if ((rc = launch_boundary(h))) return rc;
+    const int compact = bc_decide(h, n);
+    if ((rc = launch_boundary(h, compact))) return rc;
+    bc_after(h, compact);
     if (qx && (rc = launch_boundary_ena(h))) return rc;
     if ((rc = launch_fields(h, 1))) return rc;
     if ((rc = zero_accum(h))) return rc;
@@ -815,7 +895,10 @@ int autotune(kaos_handle *h) {
 // does); a replay applies the same host-side transitions.
 int graph_steps(kaos_handle *h, int g) {
   const int64_t n = h->n + 1;
+  // a master step is replayed alone; whether it compacts is decided first
+  const int compact = is_master(h, n) ? bc_decide(h, n) : 0;
   const uint64_t key = (uint64_t)g | ((uint64_t)is_master(h, n) << 16) |
+                       ((uint64_t)compact << 21) |
                        ((uint64_t)is_master(h, n + 1) << 17) |
                        ((uint64_t)h->cur << 18) | ((uint64_t)h->ecur << 19) |
                        ((uint64_t)(h->export_on != 0) << 20);
@@ -832,7 +915,7 @@ int graph_steps(kaos_handle *h, int g) {
     for (int k = 0; k < g; ++k) {
       const int64_t m = h->n + 1;
       if (is_master(h, m)) {  // launch_boundary / launch_boundary_ena swaps
-        h->cur = 1 - h->cur;
+        bc_after(h, bc_decide(h, m));
         if (h->P.QEXCHANGEflag == 1) h->ecur = 1 - h->ecur;
       }
       h->n = m;
@@ -1002,6 +1085,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     hoff += (int64_t)T.nq * h->nv;
   }
   h->ncell = coff;
+  h->bc_bound.assign(ntubes, 0);
   *out = h;
   int rc;
   CK(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
@@ -1258,6 +1342,7 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
   }
   int64_t nl = n;
   uint64_t nid = h->id_base[tube] + (uint64_t)n;
+  h->bc_bound[tube] = n;
   CK(cudaMemcpy(h->d_nlive + tube, &nl, sizeof(int64_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_next_id + tube, &nid, sizeof(uint64_t), cudaMemcpyHostToDevice));
   if (h->d_cxc)  // the first push starts the selection counts from zero
@@ -1312,6 +1397,7 @@ int kaos_init_particles(kaos_handle *h, int32_t tube, const kaos_init_c *in) {
   if (e != cudaSuccess) return fail(h, KAOS_ERR_CUDA, "init: %s", cudaGetErrorString(e));
   int64_t nl = n;
   uint64_t nid = h->id_base[tube] + (uint64_t)n;
+  h->bc_bound[tube] = n;
   CK(cudaMemcpy(h->d_nlive + tube, &nl, sizeof(int64_t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_next_id + tube, &nid, sizeof(uint64_t), cudaMemcpyHostToDevice));
   if (h->d_cxc)  // the first push starts the selection counts from zero

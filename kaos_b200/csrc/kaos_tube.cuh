@@ -434,6 +434,8 @@ struct BcArgs {
   unsigned long long *lb_out, *ub_out;  // per tube escape counts
   Fields fields;
   int ena;  // 1: operate on the ENA segments (tube.eoff) instead of ions
+  // k_bc_mark: the slot arrays marked DEAD (cell: mixed precision only)
+  int32_t *qind_w, *cell_w;
 };
 
 __device__ __forceinline__ bool keep_slot(int q) {
@@ -467,6 +469,43 @@ __global__ void k_bc_count(BcArgs a) {
     int K = 0, L = 0, U = 0;
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { K += sk[k]; L += sl[k]; U += su[k]; }
     a.blkcnt[blockIdx.x] = K;
+    if (L) atomicAdd(a.lb_out + t, (unsigned long long)L);
+    if (U) atomicAdd(a.ub_out + t, (unsigned long long)U);
+  }
+}
+
+// Removal without moving the arrays: the escaped ions of a master step are
+// counted and marked DEAD in place, as slots converted to ENAs are; the
+// live ions keep their order, and a later compaction removes every DEAD
+// slot at once.
+__global__ void k_bc_mark(BcArgs a) {
+  const int t = a.blk_tube[blockIdx.x];
+  const TubeD &T = a.tubes[t];
+  const int64_t nl = a.nlive[t];
+  const int64_t beg = a.blk_start[blockIdx.x];
+  const int64_t end = min(beg + (int64_t)a.chunk, nl);
+  int lb = 0, ub = 0;
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const int64_t j = T.off + i;
+    const int q = a.qind_w[j];
+    if (q == BELOW || q == ABOVE) {
+      lb += (q == BELOW);
+      ub += (q == ABOVE);
+      a.qind_w[j] = DEAD;
+      if (a.cell_w) a.cell_w[j] = DEAD;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lb += __shfl_down_sync(0xffffffffu, lb, o);
+    ub += __shfl_down_sync(0xffffffffu, ub, o);
+  }
+  __shared__ int sl[32], su[32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sl[w] = lb; su[w] = ub; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int L = 0, U = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { L += sl[k]; U += su[k]; }
     if (L) atomicAdd(a.lb_out + t, (unsigned long long)L);
     if (U) atomicAdd(a.ub_out + t, (unsigned long long)U);
   }

@@ -262,3 +262,17 @@ def config_c3(n_particles=100_000_000, precision=KAOS_PREC_MIXED, ndatfac=50):
     tube = make_tube(spec, mi)
     vg = make_vgrid(True, 64, 64, 96, 40e3)
     return mi, spec, tube, vg
+
+
+def config_escaping():
+    """A short hot tube (L=3, 24 cells up to |q| = 0.5, 5 eV O+, dt 1 s,
+    master step every 2 steps) that loses ~40 ions per master step through
+    both boundaries, with 30 injected at the lower one: the removal and
+    injection test case."""
+    mi = ModelInput(h=1.0, ndatfac=2, ION2VPERPflag=1)
+    vg = make_vgrid(True, 16, 16, 24, 3e4)
+    spec = TubeSpec(L=3.0, nq=24, n_particles=2500, q_ub=0.5, H=400e3,
+                    Ti=5.0 * 1.602e-19 / KB)
+    tube = make_tube(spec, mi)
+    tube.nsnormCLB = 30.0
+    return mi, spec, tube, vg
