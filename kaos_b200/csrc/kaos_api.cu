@@ -319,7 +319,7 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
   if (timed) CK(cudaEventRecord(h->pev[2 * h->npev], h->s));
   size_t smem = (size_t)(2 * nq + 1) * sizeof(double) + (size_t)nq * sizeof(unsigned);
   if (h->mixed)  // + one double of padding before the 16-byte aligned floats
-    smem += (size_t)(5 * nq + 1) * sizeof(double) + (size_t)8 * nq * sizeof(float);
+    smem += (size_t)(5 * nq + 1) * sizeof(double) + (size_t)10 * nq * sizeof(float);
   smem += (size_t)BIN_WIN * (1 + h->vg.npar + h->vg.n1 + (h->three_d ? h->vg.n2 : 0)) *
           sizeof(unsigned);  // block-private binning window
   const int rs = h->mixed ? h->regsel : 0, ps = h->persistent;

@@ -385,6 +385,75 @@ __device__ __forceinline__ float cosa(float x) {
   return r;
 }
 
+// field_prologue for the mixed push, where q_k4 is held in FP32: the same
+// segment (walk over the oriented cell centres C = sgn qGC in shared
+// memory), the fraction with a one-instruction reciprocal, and the
+// interpolation and q/m scaling in FP32 from the cell fields FE (EAmag, EG
+// per cell, in shared memory).
+__device__ __forceinline__ void field_prologue32(const ForceFlags &ff,
+                                                 const TubeD &T, const double *E,
+                                                 const double *C, const float2 *FE,
+                                                 float qk, int guess, float qm,
+                                                 float &aea, float &ag) {
+  const int nq = T.nq;
+  const int k = centre_segment(E, C, nq, T.sgn * (double)qk, guess);
+  if (k < 0) return;
+  float2 f;
+  if (k == 0) {
+    f = FE[0];
+  } else if (k == nq) {
+    f = FE[nq - 1];
+  } else {
+    const double x1 = T.sgn * C[k - 1], x2 = T.sgn * C[k];
+    const float frac = (float)((double)qk - x1) * rcpa((float)(x2 - x1));
+    const float2 y1 = FE[k - 1], y2 = FE[k];
+    f.x = fmaf(frac, y2.x - y1.x, y1.x);
+    f.y = fmaf(frac, y2.y - y1.y, y1.y);
+  }
+  if (ff.eamb) {
+    const float e = ff.eambsign ? f.x : fabsf(f.x);
+    aea = (e == 0.0f) ? 0.0f : (ff.eambsign ? qm * e : fabsf(qm * e));
+  }
+  if (ff.grav) {
+    const float e = fabsf(f.y);
+    ag = (e == 0.0f) ? 0.0f : fabsf(qm * e);
+  }
+}
+
+// Velocity-bin search of the mixed push from a lookup table: VTAB uniform
+// slots over the axis hold the bin of each slot's left end, and a short
+// walk over the edges finishes the search.  The walk establishes both edge
+// conditions of vbin (v <= e[b+1], and v > e[b] unless b = 0), so the result
+// equals vbin's whatever the table holds.
+constexpr int VTAB = 256;
+struct VBinTab {
+  float e0, iw;              // first edge, VTAB / (last edge - first edge)
+  unsigned char t[VTAB];     // bin at each slot's left end (n <= 128)
+};
+
+// All threads of the block; edges e[0..n] in shared memory already visible,
+// and the caller synchronises before the table is used.
+__device__ __forceinline__ void build_vbin_tab(VBinTab &T, const float *e, int n) {
+  if (threadIdx.x == 0) {
+    T.e0 = e[0];
+    T.iw = (float)VTAB / (e[n] - e[0]);
+  }
+  for (int k = threadIdx.x; k < VTAB; k += blockDim.x) {
+    const float v = e[0] + (e[n] - e[0]) * ((float)k / (float)VTAB);
+    T.t[k] = (unsigned char)max(vbin(e, n, v), 0);
+  }
+}
+
+__device__ __forceinline__ int vbin_tab(const VBinTab &T, const float *e, int n,
+                                        float v) {
+  if (!(v >= e[0] && v <= e[n])) return -1;
+  const int s = min(max((int)((v - T.e0) * T.iw), 0), VTAB - 1);
+  int b = T.t[s];
+  while (b > 0 && v <= e[b]) --b;
+  while (b < n - 1 && v > e[b + 1]) ++b;
+  return b;
+}
+
 // Hardware base-2 logarithm and exponential (MUFU, flush-to-zero).
 __device__ __forceinline__ float lg2f(float x) {
   float r;
@@ -670,17 +739,19 @@ template <bool THREE_D>
 __device__ __forceinline__ void start_bins(const PushArgs &a, const Ions &I,
                                            int64_t j, const float *VE1,
                                            const float *VE2, const float *VEP,
+                                           const VBinTab &VT1, const VBinTab &VT2,
+                                           const VBinTab &VTP,
                                            float vpar, float v1, float v2,
                                            float vp2, int &b1, int &b2, int &bp) {
   b2 = -1;
   if (THREE_D) {
-    bp = vbin(VEP, c_vg.npar, vpar);
-    b1 = vbin(VE1, c_vg.n1, v1);
-    b2 = vbin(VE2, c_vg.n2, v2);
+    bp = vbin_tab(VTP, VEP, c_vg.npar, vpar);
+    b1 = vbin_tab(VT1, VE1, c_vg.n1, v1);
+    b2 = vbin_tab(VT2, VE2, c_vg.n2, v2);
   } else {
     const int old = I.vb[j];
-    const int np_ = vbin(VEP, c_vg.npar, vpar);
-    const int n1_ = vbin(VE1, c_vg.n1, sqrtf(vp2));
+    const int np_ = vbin_tab(VTP, VEP, c_vg.npar, vpar);
+    const int n1_ = vbin_tab(VT1, VE1, c_vg.n1, sqrtf(vp2));
     bp = np_ >= 0 ? np_ : (old & 0xffff) - 1;
     b1 = n1_ >= 0 ? n1_ : (old >> 16) - 1;
     const int nw = ((b1 + 1) << 16) | (bp + 1);
@@ -706,9 +777,11 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   double *E = sm, *Cc = sm + nqmax + 1;
   double *UL = Cc + nqmax, *UD = UL + nqmax, *QL = UD + nqmax, *IDQ = QL + nqmax,
          *DQ = IDQ + nqmax;
-  // 8 floats per cell (heat32), 16-byte aligned
+  // 8 floats per cell (heat32), 16-byte aligned; then the cell fields
+  // (EAmag, EG) of the field re-interpolation
   float *HK = (float *)(sm + ((7 * nqmax + 2) & ~1));
-  unsigned *HC = (unsigned *)(HK + 8 * nqmax);
+  float2 *FE = (float2 *)(HK + 8 * nqmax);
+  unsigned *HC = (unsigned *)(FE + nqmax);
   const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
   const uint32_t step = a.dstep ? *a.dstep : a.step;
   const float fRE = (float)RE;
@@ -718,7 +791,15 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   int tcur = -1;
   // velocity-cell edges for the bin searches in shared memory
   __shared__ float VE1[MAXV + 1], VE2[MAXV + 1], VEP[MAXV + 1];
-  if (bin || !THREE_D) load_vgrid_smem(c_vg.f1, c_vg.f2, c_vg.fpar, VE1, VE2, VEP);
+  __shared__ VBinTab VT1, VT2, VTP;
+  if (bin || !THREE_D) {
+    load_vgrid_smem(c_vg.f1, c_vg.f2, c_vg.fpar, VE1, VE2, VEP);
+    __syncthreads();
+    build_vbin_tab(VTP, VEP, c_vg.npar);
+    build_vbin_tab(VT1, VE1, c_vg.n1);
+    if (THREE_D) build_vbin_tab(VT2, VE2, c_vg.n2);
+    // the first barrier of the item loop orders the tables before any use
+  }
   // one work item per block, or a persistent grid striding over the items
   for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
   const int t = a.blk_tube[item];
@@ -748,6 +829,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
         HK[8 * k + 6] = lam != 0.0 ? (float)log2(2.0 * PI / lam) : 0.0f;
         HK[8 * k + 7] = 0.0f;
       }
+      if (prologue) FE[k] = make_float2((float)a.ct.EAmag[g], (float)a.ct.EG[g]);
     }
     tcur = t;
   }
@@ -787,12 +869,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       if (a.icr) n_id = I.id[jn];
     }
     if (c0 == DEAD) continue;
-    if (prologue) {
-      double da = aea, dg = ag;
-      field_prologue(a, T, E, Cc, (double)I.fqk4[j], c0, da, dg);
-      aea = (float)da;
-      ag = (float)dg;
-    }
+    if (prologue) field_prologue32(a.ff, T, E, Cc, FE, I.fqk4[j], c0, qs_ms, aea, ag);
     // ---- start-of-step position: q, then (r, theta) by FP64 Newton -------
     const double q0 = fma((double)o0, DQ[c0], QL[c0]);
     const double u = quartic_newton<true>(q0, ipG, fma((double)o0, UD[c0], UL[c0]), 2);
@@ -821,7 +898,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     const float vp2 = v1 * v1 + v2 * v2;
     if (bin_only) {
       int b1, b2, bp;
-      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, vpar, v1, v2, vp2, b1, b2, bp);
+      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, VT1, VT2, VTP, vpar, v1, v2, vp2, b1, b2, bp);
       if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
       if (a.write_qind) I.qind[j] = qi;
       continue;
@@ -880,7 +957,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     const float vparN = gN.er * VNr + gN.ez * VNz;
     if (bin || !THREE_D) {
       int b1, b2, bp;
-      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, vpar, v1, v2, vp2, b1, b2, bp);
+      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, VT1, VT2, VTP, vpar, v1, v2, vp2, b1, b2, bp);
       if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
     }
     if (!isfinite(vparN) || !isfinite(oN)) atomicOr(a.status, ST_NAN);

@@ -147,3 +147,43 @@ def test_state_export_skips_converted_slots(mixed):
                                    None, None, None, ni + 1)
     assert rc != 0
     s.close()
+
+
+def test_mixed_bins_equal_host_binning():
+    """The mixed push's start-of-step velocity bins (a lookup table plus a
+    walk over the FP32 edges) and cells equal a plain search on the host:
+    the full histogram of a master step against the host's count of the
+    same ions (the state after the step before it)."""
+    mi, spec, tube, vg = grids.config_small(n_particles=20000, three_d=True,
+                                            steps_per_master=4)
+    mi.precision = KAOS_PREC_MIXED
+    tube.nsnormCLB = 0.0  # no injected ions in the master step's counts
+    init = grids.initial_particles(tube, spec, mi, seed=41)
+    s = Solver(mi, [tube], vg)
+    s.load(0, *init)
+    s.set_export(True)
+    s.step(3)
+    P = s.particles()
+    s.step(1)  # master step 4 bins the state P
+    H = s.counts(full=True)
+    s.close()
+    qGL, qGH = np.asarray(tube.qGL), np.asarray(tube.qGH)
+    sgn = 1.0 if qGL[0] <= 0.0 else -1.0
+    E = sgn * np.append(qGL, qGH[-1])
+    sq = sgn * P["q"]
+    cell = np.searchsorted(E, sq, side="left") - 1
+    cell[sq == E[0]] = 0
+    cell[(sq < E[0]) | (sq > E[-1])] = -1
+
+    def vbin(e, v):
+        e32, v32 = np.asarray(e, np.float32), np.asarray(v, np.float32)
+        b = np.searchsorted(e32, v32, side="left") - 1
+        b[v32 == e32[0]] = 0
+        b[(v32 < e32[0]) | (v32 > e32[-1])] = -1
+        return b
+    b1, b2, bp = vbin(vg.e1, P["vperp1"]), vbin(vg.e2, P["vperp2"]), vbin(vg.epar, P["vpar"])
+    ok = (cell >= 0) & (b1 >= 0) & (b2 >= 0) & (bp >= 0)
+    idx = ((cell * vg.n1 + b1) * vg.n2 + b2) * vg.npar + bp
+    Hh = np.bincount(idx[ok], minlength=len(qGL) * vg.n1 * vg.n2 * vg.npar)
+    assert Hh.sum() > 10000
+    np.testing.assert_array_equal(H, Hh)
