@@ -124,6 +124,7 @@ struct kaos_handle {
   int64_t *d_cx_start = nullptr;
   unsigned *d_cxc = nullptr, *d_cxo = nullptr;
   int *d_cxend = nullptr;
+  int *d_tube_done = nullptr;  // per tube: charge-exchange cell scans done
   int *d_cell_tube = nullptr, *d_cell_q = nullptr;  // global cell -> (tube, cell)
   int ncx = 0;
   int64_t n = 0;      // computational steps taken
@@ -648,6 +649,7 @@ CxArgs cx_args(kaos_handle *h) {
   a.cxconv = h->d_cxconv;
   a.cxbase = h->d_cxbase;
   a.cxend = h->d_cxend;
+  a.tube_done = h->d_tube_done;
   a.rank = h->rank;
   a.nranks = h->nranks;
   a.nqmax = max_nq(h);
@@ -675,11 +677,10 @@ int launch_cx(kaos_handle *h) {
   // the per-chunk Qindk1 counts were accumulated by the previous push
   // 1024 threads: one tile covers the chunks of a tube of up to 16.7 M ions
   k_cx_scan<<<(int)h->ncell, 1024, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
-  k_cx_base<<<h->ntubes, 1024, 0, h->s>>>(a);
   // one block per chunk (a chunk with conversions walks its ions in order;
   // blocks of chunks without live ions leave at once)
   k_cx_convert<<<std::max(h->ncx, 1), 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
-  h->launches += 3;
+  h->launches += 2;
   CK(cudaGetLastError());
   return KAOS_OK;
 }
@@ -1278,6 +1279,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
         (rc = dalloc(h, &h->d_cxconv, cxt.size())) ||
         (rc = dalloc(h, &h->d_cxbase, cxt.size())) ||
         (rc = dalloc(h, &h->d_cxend, (size_t)h->ncell)) ||
+        (rc = dalloc(h, &h->d_tube_done, (size_t)ntubes)) ||
         (rc = dalloc(h, &h->d_cxc, cxt.size() * (size_t)max_nq(h))) ||
         (rc = dalloc(h, &h->d_cxo, cxt.size() * (size_t)max_nq(h))))
       return rc;

@@ -34,6 +34,7 @@ struct CxArgs {
   unsigned *cxconv;          // per chunk: ions converted in it this step
   int64_t *cxbase;           // per chunk: ENA slot of its first conversion
   int *cxend;                // per cell (all tubes): chunks >= cxend convert none
+  int *tube_done;            // per tube: cell scans finished this step
   int nqmax, mixed;
   int ncx;                   // selection chunks (all tubes)
   int rank, nranks;          // this rank's share of a split tube's conversions
@@ -59,8 +60,8 @@ __device__ __forceinline__ int cx_live_end(const CxArgs &a, int t) {
   return (int)min((int64_t)c1, c0 + ceil_div(a.nlive[t], (int64_t)CX_CHUNK));
 }
 
-__global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
-  const int t = cell_tube[blockIdx.x], k = cell_q[blockIdx.x];
+__device__ __forceinline__ void cx_scan_cell(const CxArgs &a, int t, int k,
+                                             int g) {
   const TubeD &T = a.tubes[t];
   const unsigned need = cx_need(a, a.ct.nuPoi[T.coff + k]);
   if (need == 0u) return;
@@ -91,27 +92,26 @@ __global__ void k_cx_scan(CxArgs a, const int *cell_tube, const int *cell_q) {
     if (threadIdx.x == 0) base += tot;
     __syncthreads();
     if (base >= need) {
-      if (threadIdx.x == 0) a.cxend[blockIdx.x] = min(r0 + (int)blockDim.x, c1);
+      if (threadIdx.x == 0) a.cxend[g] = min(r0 + (int)blockDim.x, c1);
       return;
     }
   }
-  if (threadIdx.x == 0) a.cxend[blockIdx.x] = c1;
+  if (threadIdx.x == 0) a.cxend[g] = c1;
 }
 
 // ENA slots in ion-index order: exclusive scan of the per-chunk conversion
 // totals over the live chunks of each tube (one block per tube, each thread
 // a run of consecutive chunks: run sums, one block scan, run prefixes); the
 // ENA count of the tube advances by the step's total.
-__global__ void k_cx_base(CxArgs a) {
-  const int t = blockIdx.x;
+__device__ __forceinline__ void cx_base_tube(const CxArgs &a, int t) {
   const int c0 = a.tube_cx0[t], c1 = cx_live_end(a, t);
   __shared__ unsigned long long wsum[32];
   const int64_t n0 = a.nena[t];
   const int l = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int run = (int)ceil_div((int64_t)max(c1 - c0, 0), (int64_t)blockDim.x);
   const int r0 = c0 + (int)threadIdx.x * run, r1 = min(r0 + run, c1);
-  unsigned long long n = 0;
-  for (int c = r0; c < r1; ++c) n += a.cxconv[c];
+  unsigned long long n = 0;  // (L2 reads: other blocks' atomics)
+  for (int c = r0; c < r1; ++c) n += __ldcg(a.cxconv + c);
   unsigned long long x = n;  // inclusive warp scan of the run sums
   for (int o = 1; o < 32; o <<= 1) {
     const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
@@ -124,9 +124,30 @@ __global__ void k_cx_base(CxArgs a) {
   unsigned long long s = woff + x - n;  // exclusive prefix of this run
   for (int c = r0; c < r1; ++c) {
     a.cxbase[c] = n0 + (int64_t)s;
-    s += a.cxconv[c];
+    s += __ldcg(a.cxconv + c);
   }
   if (threadIdx.x == 0) a.nena[t] = n0 + (int64_t)tot;
+}
+
+// One block (1024 threads) per (tube, cell): the cell's scan, then the last
+// block of a tube to finish (a per-tube arrival counter) gives the tube its
+// ENA slots; it also resets the counter for the next step.
+__global__ void __launch_bounds__(1024) k_cx_scan(CxArgs a, const int *cell_tube,
+                                                  const int *cell_q) {
+  const int t = cell_tube[blockIdx.x], k = cell_q[blockIdx.x];
+  cx_scan_cell(a, t, k, blockIdx.x);
+  __shared__ int last;
+  __syncthreads();  // every thread's counts and prefixes are written
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(a.tube_done + t, 1) == a.tubes[t].nq - 1;
+    if (last) a.tube_done[t] = 0;
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    cx_base_tube(a, t);
+  }
 }
 
 // Cartesian unit vectors along B (par), across the shell (p) and in
