@@ -485,14 +485,25 @@ __global__ void k_bc_mark(BcArgs a) {
   const int64_t beg = a.blk_start[blockIdx.x];
   const int64_t end = min(beg + (int64_t)a.chunk, nl);
   int lb = 0, ub = 0;
-  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
-    const int64_t j = T.off + i;
-    const int q = a.qind_w[j];
-    if (q == BELOW || q == ABOVE) {
-      lb += (q == BELOW);
-      ub += (q == ABOVE);
-      a.qind_w[j] = DEAD;
-      if (a.cell_w) a.cell_w[j] = DEAD;
+  // the indices of a tile of MARK_IT slots per thread are loaded before any
+  // is examined, so their HBM latencies overlap
+  constexpr int MARK_IT = 8;
+  for (int64_t i0 = beg; i0 < end; i0 += (int64_t)MARK_IT * blockDim.x) {
+    int q[MARK_IT];
+#pragma unroll
+    for (int k = 0; k < MARK_IT; ++k) {
+      const int64_t i = i0 + k * (int64_t)blockDim.x + threadIdx.x;
+      q[k] = i < end ? a.qind_w[T.off + i] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < MARK_IT; ++k) {
+      if (q[k] == BELOW || q[k] == ABOVE) {
+        const int64_t j = T.off + i0 + k * (int64_t)blockDim.x + threadIdx.x;
+        lb += (q[k] == BELOW);
+        ub += (q[k] == ABOVE);
+        a.qind_w[j] = DEAD;
+        if (a.cell_w) a.cell_w[j] = DEAD;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
