@@ -482,9 +482,8 @@ Fields ion_fields(kaos_handle *h, int from, int to) {
     if (s) F.f[F.n++] = Field{s, d, sz};
   };
   if (h->mixed) {
-    add(A.cell, B.cell, 4); add(A.off, B.off, 4); add(A.fvpar, B.fvpar, 4);
-    add(A.fv1, B.fv1, 4); add(A.fv2, B.fv2, 4); add(A.faea, B.faea, 4);
-    add(A.fag, B.fag, 4); add(A.fqk4, B.fqk4, 4);
+    add(A.co, B.co, 8); add(A.fvpar, B.fvpar, 4); add(A.fv, B.fv, 8);
+    add(A.ffl, B.ffl, 8); add(A.fqk4, B.fqk4, 4);
   } else {
     add(A.rho, B.rho, 8); add(A.z, B.z, 8); add(A.vpar, B.vpar, 8);
     add(A.v1, B.v1, 8); add(A.v2, B.v2, 8); add(A.aea, B.aea, 8);
@@ -557,7 +556,7 @@ int launch_boundary(kaos_handle *h, int compact) {
     b.lb_out = h->d_lb_out;
     b.ub_out = h->d_ub_out;
     b.qind_w = h->ion[h->cur].qind;
-    b.cell_w = h->mixed ? h->ion[h->cur].cell : nullptr;
+    b.co_w = h->mixed ? h->ion[h->cur].co : nullptr;
     CK(cudaMemsetAsync(h->d_lb_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
     CK(cudaMemsetAsync(h->d_ub_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
     CK(cudaMemsetAsync(h->d_lb_in, 0, h->ntubes * sizeof(unsigned long long), h->s));
@@ -1190,13 +1189,10 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   for (int b = 0; b < 2; ++b) {
     Ions &I = h->ion[b];
     if (h->mixed) {
-      if ((rc = dalloc(h, &I.cell, cap))) return rc;
-      if ((rc = dalloc(h, &I.off, cap))) return rc;
+      if ((rc = dalloc(h, &I.co, cap))) return rc;
       if ((rc = dalloc(h, &I.fvpar, cap))) return rc;
-      if ((rc = dalloc(h, &I.fv1, cap))) return rc;
-      if ((rc = dalloc(h, &I.fv2, cap))) return rc;
-      if ((rc = dalloc(h, &I.faea, cap))) return rc;
-      if ((rc = dalloc(h, &I.fag, cap))) return rc;
+      if ((rc = dalloc(h, &I.fv, cap))) return rc;
+      if ((rc = dalloc(h, &I.ffl, cap))) return rc;
       if ((rc = dalloc(h, &I.fqk4, cap))) return rc;
     } else {
       if ((rc = dalloc(h, &I.rho, cap))) return rc;

@@ -6,7 +6,9 @@
 //    FP64 mode stores the meridian-plane position (rho, z) -- the ion motion
 //    is confined to its flux-tube meridian (phi = phiG) -- plus V||, Vperp1,
 //    Vperp2 and the cached field accelerations.  Mixed mode stores the
-//    position as an integer cell + FP32 offset in q, and FP32 velocities.
+//    position as an integer cell + FP32 offset in q, and FP32 velocities,
+//    the pairs that are read together interleaved (cell|offset,
+//    Vperp1|Vperp2, AEA|AG).
 //  * per-cell tables: concatenated over tubes, tube t at [tube.coff, +nq).
 //  * velocity-grid edges: __constant__ memory (shared by all tubes).
 #pragma once
@@ -68,8 +70,12 @@ struct CellTables {
 struct Ions {
   double *rho, *z, *vpar, *v1, *v2, *aea, *ag, *qk4;  // FP64 mode
   double *rho4, *z4;   // FP64 + charge exchange: the k4 point of the step
-  int32_t *cell;                                      // mixed: position cell
-  float *off, *fvpar, *fv1, *fv2, *faea, *fag, *fqk4;  // mixed mode
+  // mixed mode: fields read together are stored together (one 8-byte
+  // access each): co = (position cell, FP32 offset bits), fv = (Vperp1,
+  // Vperp2), ffl = (AEA, AG)
+  int2 *co;
+  float2 *fv, *ffl;
+  float *fvpar, *fqk4;
   int32_t *qind;       // start-of-step cell Qindk1 (0-based, sentinels)
   int32_t *vb;         // 2D grid: stale (vperp,vpar) bins, packed
   uint64_t *id;        // persistent particle id (RNG key, order key)

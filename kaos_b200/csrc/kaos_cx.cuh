@@ -242,18 +242,21 @@ __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) 
       // ion position and velocity at the end of the previous step
       double rho, z, vpar, v1, v2, qk4;
       if (a.mixed) {
-        const int cc = a.ion.cell[j];
+        const int2 co = a.ion.co[j];
+        const int cc = co.x;
+        const double oo = (double)__int_as_float(co.y);
         const double qq = a.ct.qGL[T.coff + cc] +
-                          (double)a.ion.off[j] * (a.ct.qGH[T.coff + cc] - a.ct.qGL[T.coff + cc]);
+                          oo * (a.ct.qGH[T.coff + cc] - a.ct.qGL[T.coff + cc]);
         const double ug = a.ct.uL[T.coff + cc] +
-                          (double)a.ion.off[j] * (a.ct.uH[T.coff + cc] - a.ct.uL[T.coff + cc]);
+                          oo * (a.ct.uH[T.coff + cc] - a.ct.uL[T.coff + cc]);
         const double u = quartic_newton(qq, 1.0 / T.pG, ug, 3);
         const double s2 = u / T.pG;
         rho = u * RE * sqrt(s2);
         z = u * RE * qq * u * u;
         vpar = a.ion.fvpar[j];
-        v1 = a.ion.fv1[j];
-        v2 = a.ion.fv2[j];
+        const float2 v = a.ion.fv[j];
+        v1 = v.x;
+        v2 = v.y;
         qk4 = a.ion.fqk4[j];
       } else {
         rho = a.ion.rho[j];
@@ -298,7 +301,7 @@ __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) 
         atomicOr(a.status, ST_CAP);
       }
       a.ion.qind[j] = DEAD;
-      if (a.mixed) a.ion.cell[j] = DEAD;
+      if (a.mixed) a.ion.co[j].x = DEAD;
     }
     __syncthreads();
   }

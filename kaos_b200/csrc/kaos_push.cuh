@@ -836,7 +836,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   if (a.cxc)
     for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
   BinWin W{};
-  if (bin) W = bin_win_init(HC + nqmax, max(a.ion.cell[T.off + beg], 0), T.nq);
+  if (bin) W = bin_win_init(HC + nqmax, max(a.ion.co[T.off + beg].x, 0), T.nq);
   __syncthreads();
   const float invsumds = (float)(1.0 / T.sumdsICR);
   const double ipG = 1.0 / T.pG;
@@ -850,8 +850,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   uint64_t n_id = 0;
   if (beg + threadIdx.x < end) {
     const int64_t j = T.off + beg + threadIdx.x;
-    n_c = I.cell[j]; n_o = I.off[j]; n_vp = I.fvpar[j]; n_v1 = I.fv1[j];
-    n_v2 = I.fv2[j]; n_ea = I.faea[j]; n_ag = I.fag[j];
+    const int2 co = I.co[j];
+    const float2 v = I.fv[j], f = I.ffl[j];
+    n_c = co.x; n_o = __int_as_float(co.y); n_vp = I.fvpar[j];
+    n_v1 = v.x; n_v2 = v.y; n_ea = f.x; n_ag = f.y;
     if (a.icr) n_id = I.id[j];
   }
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
@@ -864,8 +866,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     const uint64_t pid = n_id;
     if (i + blockDim.x < end) {
       const int64_t jn = j + blockDim.x;
-      n_c = I.cell[jn]; n_o = I.off[jn]; n_vp = I.fvpar[jn]; n_v1 = I.fv1[jn];
-      n_v2 = I.fv2[jn]; n_ea = I.faea[jn]; n_ag = I.fag[jn];
+      const int2 co = I.co[jn];
+      const float2 v = I.fv[jn], f = I.ffl[jn];
+      n_c = co.x; n_o = __int_as_float(co.y); n_vp = I.fvpar[jn];
+      n_v1 = v.x; n_v2 = v.y; n_ea = f.x; n_ag = f.y;
       if (a.icr) n_id = I.id[jn];
     }
     if (c0 == DEAD) continue;
@@ -961,17 +965,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
     }
     if (!isfinite(vparN) || !isfinite(oN)) atomicOr(a.status, ST_NAN);
-    I.cell[j] = cpos;
-    I.off[j] = oN;
+    I.co[j] = make_int2(cpos, __float_as_int(oN));
     I.fvpar[j] = vparN;
-    if (a.icr) {
-      I.fv1[j] = v1n;
-      I.fv2[j] = v2n;
-    }
-    if (prologue) {
-      I.faea[j] = aea;
-      I.fag[j] = ag;
-    }
+    if (a.icr) I.fv[j] = make_float2(v1n, v2n);
+    if (prologue) I.ffl[j] = make_float2(aea, ag);
     if (a.write_qind) I.qind[j] = qi;
     if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);
   }

@@ -434,8 +434,9 @@ struct BcArgs {
   unsigned long long *lb_out, *ub_out;  // per tube escape counts
   Fields fields;
   int ena;  // 1: operate on the ENA segments (tube.eoff) instead of ions
-  // k_bc_mark: the slot arrays marked DEAD (cell: mixed precision only)
-  int32_t *qind_w, *cell_w;
+  // k_bc_mark: the slot arrays marked DEAD (co: mixed precision only)
+  int32_t *qind_w;
+  int2 *co_w;
 };
 
 __device__ __forceinline__ bool keep_slot(int q) {
@@ -502,7 +503,7 @@ __global__ void k_bc_mark(BcArgs a) {
         lb += (q[k] == BELOW);
         ub += (q[k] == ABOVE);
         a.qind_w[j] = DEAD;
-        if (a.cell_w) a.cell_w[j] = DEAD;
+        if (a.co_w) a.co_w[j].x = DEAD;
       }
     }
   }
@@ -663,13 +664,11 @@ __global__ void k_inject(InjArgs a) {
     int b2 = d3 ? vbin(c_vg.e2, c_vg.n2, v2) : 0;
     if (a.ion.vb) a.ion.vb[j] = ((b1 + 1) << 16) | (bp + 1);
     if (a.mixed) {
-      a.ion.cell[j] = Q;
-      a.ion.off[j] = (float)((qc - a.ct.qGL[g]) / (a.ct.qGH[g] - a.ct.qGL[g]));
+      a.ion.co[j] = make_int2(
+          Q, __float_as_int((float)((qc - a.ct.qGL[g]) / (a.ct.qGH[g] - a.ct.qGL[g]))));
       a.ion.fvpar[j] = (float)vpar;
-      a.ion.fv1[j] = (float)v1;
-      a.ion.fv2[j] = (float)v2;
-      a.ion.faea[j] = (float)aea;
-      a.ion.fag[j] = (float)ag;
+      a.ion.fv[j] = make_float2((float)v1, (float)v2);
+      a.ion.ffl[j] = make_float2((float)aea, (float)ag);
       a.ion.fqk4[j] = (float)qc;
     } else {
       a.ion.rho[j] = rho0;
@@ -741,11 +740,9 @@ __device__ __forceinline__ void store_ion(const Ions &I, const TubeD &T,
     I.vb[k] = ((b1 + 1) << 16) | (bp + 1);
   }
   if (mixed) {
-    I.cell[k] = c;
-    I.off[k] = (float)((q - qL) / (qH - qL));
+    I.co[k] = make_int2(c, __float_as_int((float)((q - qL) / (qH - qL))));
     I.fvpar[k] = (float)vpar;
-    I.fv1[k] = (float)v1;
-    I.fv2[k] = (float)v2;
+    I.fv[k] = make_float2((float)v1, (float)v2);
     I.fqk4[k] = (float)q;
   } else {
     const double fr = (q - qL) / (qH - qL);
@@ -883,10 +880,11 @@ __global__ void k_convect(ConvArgs a) {
     if (a.ion.qind[j] == DEAD) continue;
     double q, u_old;
     if (a.mixed) {
-      const int c = a.ion.cell[j];
+      const int2 co = a.ion.co[j];
+      const int c = co.x;
       if (c == DEAD) continue;
       const int64_t g = T.coff + c;
-      const double o = (double)a.ion.off[j];
+      const double o = (double)__int_as_float(co.y);
       q = a.ct.qGL[g] + o * (a.ct.qGH[g] - a.ct.qGL[g]);
       u_old = quartic_newton(q, ip_old, a.ct.uL[g] + o * (a.ct.uH[g] - a.ct.uL[g]), 4);
     } else {
@@ -898,8 +896,8 @@ __global__ void k_convect(ConvArgs a) {
     const double u_new = quartic_newton(q, ip_new, u_old, 6);
     const double f = sqrt(bnorm(q, u_new) / bnorm(q, u_old));
     if (a.mixed) {
-      a.ion.fv1[j] = (float)(f * (double)a.ion.fv1[j]);
-      a.ion.fv2[j] = (float)(f * (double)a.ion.fv2[j]);
+      const float2 v = a.ion.fv[j];
+      a.ion.fv[j] = make_float2((float)(f * (double)v.x), (float)(f * (double)v.y));
     } else {
       const double rr = u_new * RE, st = sqrt(u_new * ip_new), ctv = q * u_new * u_new;
       double rho = rr * st, z = rr * ctv;
@@ -1001,11 +999,13 @@ __global__ void __launch_bounds__(EXP_THREADS) k_exp_write(ExportArgs a) {
       const int64_t o = (int64_t)(done + woff + __popc(bal & ((1u << l) - 1u)));
       double q, vp, v1, v2;
       if (a.mixed) {
-        const int c = a.ion.cell[j];
-        q = fma((double)a.ion.off[j], a.qGH[c] - a.qGL[c], a.qGL[c]);
+        const int2 co = a.ion.co[j];
+        const int c = co.x;
+        q = fma((double)__int_as_float(co.y), a.qGH[c] - a.qGL[c], a.qGL[c]);
         vp = a.ion.fvpar[j];
-        v1 = a.ion.fv1[j];
-        v2 = a.ion.fv2[j];
+        const float2 v = a.ion.fv[j];
+        v1 = v.x;
+        v2 = v.y;
       } else {
         const double rho = a.ion.rho[j], z = a.ion.z[j];
         const double r2 = rho * rho + z * z, r = sqrt(r2);
