@@ -216,18 +216,23 @@ def run_e2e(args, precision, launch):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s.load(0, *src)
+    t1 = time.perf_counter()
     h2d = sum(a.nbytes for a in src)
     d2h = 0
     for _ in range(K):
         s.step(1)
         for m in range(8):
             d2h += s.moments(m).nbytes
+    t2 = time.perf_counter()
     p = s.state(out=out)
     d2h += sum(v.nbytes for v in p.values())
-    dt = time.perf_counter() - t0
+    t3 = time.perf_counter()
+    dt = t3 - t0
     n = len(p["q"])
     s.close()
-    return dict(value=n * K / dt, h2d=h2d / K, d2h=d2h / K)
+    return dict(value=n * K / dt, h2d=h2d / K, d2h=d2h / K,
+                phases_ms={"load": 1e3 * (t1 - t0), "steps": 1e3 * (t2 - t1),
+                           "state": 1e3 * (t3 - t2)})
 
 
 def cpu_baseline(args, sample_particles=20000, sample_steps=5):
@@ -477,7 +482,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": None if e2e is None else {
                 "value": e2e["value"] * world, "unit": "particle-steps/s",
-                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                "phases_ms": e2e["phases_ms"]},
             "gpu_launches": r32["launches"],
             "clocks": summarize_clocks(samples),
         }
