@@ -496,6 +496,26 @@ Fields ion_fields(kaos_handle *h, int from, int to) {
   return F;
 }
 
+// Staging for the host transfers of kaos_load_particles and
+// kaos_get_particles: four 8-byte-per-slot arrays and the Qindk1 array of
+// the spare buffer set at tube t's segment (the spare set holds nothing
+// between steps; the packing and the autotuner use it only inside a step).
+void spare_slots(kaos_handle *h, int t, double *d[4], int32_t **qi) {
+  Ions &S = h->ion[1 - h->cur];
+  const int64_t o = h->th[t].off;
+  if (h->mixed) {
+    d[0] = (double *)(S.co + o);
+    d[1] = (double *)(S.fv + o);
+    d[2] = (double *)(S.ffl + o);
+  } else {
+    d[0] = S.rho + o;
+    d[1] = S.z + o;
+    d[2] = S.vpar + o;
+  }
+  d[3] = (double *)(S.id + o);
+  if (qi) *qi = S.qind + o;
+}
+
 // Ions one master step's injection may add to tube t.
 int64_t inject_max(const kaos_handle *h, int t) {
   const TubeD &T = h->th[t];
@@ -1307,24 +1327,24 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
   const TubeD &T = h->th[tube];
   if (n > T.cap) return fail(h, KAOS_ERR_CAPACITY, "tube %d: %lld particles exceed capacity %lld", tube, (long long)n, (long long)T.cap);
   if (n > 0) {
-    // the caller's arrays go to a device staging area; k_load derives the
-    // per-ion state there (clamp, cell search, bins, positions)
+    // the caller's arrays go to the spare buffer set (no allocation); k_load
+    // derives the per-ion state from there (clamp, cell search, bins,
+    // positions)
     const int na = vperp2 ? 4 : 3;
-    double *stage = nullptr;
-    if (cudaMalloc(&stage, (size_t)na * n * sizeof(double)) != cudaSuccess)
-      return fail(h, KAOS_ERR_CUDA, "cudaMalloc of the load staging area failed");
+    double *stage[4];
+    spare_slots(h, tube, stage, nullptr);
     const double *src[4] = {q, vpar, vperp1, vperp2};
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < na && e == cudaSuccess; ++k)
-      e = cudaMemcpy(stage + (size_t)k * n, src[k], n * sizeof(double), cudaMemcpyHostToDevice);
+      e = cudaMemcpy(stage[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_vg, &h->vg, sizeof(VGridC));
     if (e == cudaSuccess) {
       LoadArgs a{};
       a.T = T;
-      a.q = stage;
-      a.vpar = stage + n;
-      a.v1 = stage + 2 * n;
-      a.v2 = vperp2 ? stage + 3 * n : nullptr;
+      a.q = stage[0];
+      a.vpar = stage[1];
+      a.v1 = stage[2];
+      a.v2 = vperp2 ? stage[3] : nullptr;
       a.n = n;
       a.id0 = h->id_base[tube];
       a.ion = h->ion[h->cur];
@@ -1335,7 +1355,6 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    cudaFree(stage);
     if (e != cudaSuccess) return fail(h, KAOS_ERR_CUDA, "load: %s", cudaGetErrorString(e));
   }
   int64_t nl = n;
@@ -1656,8 +1675,10 @@ int kaos_get_particles(kaos_handle *h, int32_t tube, double *q, double *vpar,
     if (n != 0) return fail(h, KAOS_ERR_PARAM, "n (%lld) must equal the ion count (0)", (long long)n);
     return KAOS_OK;
   }
-  // the export runs on the device into a staging area: q, V||, Vperp1,
-  // Vperp2 (FP64) and Qindk1 of the live ions in particle order
+  // the export runs on the device into the spare buffer set (no
+  // allocation): q, V||, Vperp1, Vperp2 (FP64) and Qindk1 of the live ions
+  // in particle order; the block counts and offsets use the packing's
+  // per-block arrays, the total the packing's new-count slot of the tube
   ExportArgs a{};
   a.ion = h->ion[h->cur];
   a.off = T.off;
@@ -1666,22 +1687,17 @@ int kaos_get_particles(kaos_handle *h, int32_t tube, double *q, double *vpar,
   a.qGH = h->ct.qGH + T.coff;
   a.mixed = h->mixed;
   a.nb = (int)ceil_div(nl, (int64_t)EXP_THREADS * EXP_ITEMS);
-  const size_t nd = (size_t)nl;
-  const size_t bytes = 4 * nd * sizeof(double) + nd * sizeof(int32_t) +
-                       (size_t)a.nb * (sizeof(unsigned) + sizeof(unsigned long long)) + 64;
-  char *st = nullptr;
-  if (cudaMalloc(&st, bytes) != cudaSuccess)
-    return fail(h, KAOS_ERR_CUDA, "cudaMalloc of the export staging area failed");
-  double *dq = (double *)st;
-  a.q = q ? dq : nullptr;
-  a.vpar = vpar ? dq + nd : nullptr;
-  a.v1 = vperp1 ? dq + 2 * nd : nullptr;
-  a.v2 = vperp2 ? dq + 3 * nd : nullptr;
-  int32_t *dqi = (int32_t *)(dq + 4 * nd);
+  double *dq[4];
+  int32_t *dqi = nullptr;
+  spare_slots(h, tube, dq, &dqi);
+  a.q = q ? dq[0] : nullptr;
+  a.vpar = vpar ? dq[1] : nullptr;
+  a.v1 = vperp1 ? dq[2] : nullptr;
+  a.v2 = vperp2 ? dq[3] : nullptr;
   a.qind = qind ? dqi : nullptr;
-  a.blkoff = (unsigned long long *)(((uintptr_t)(dqi + nd) + 15) & ~(uintptr_t)15);
-  a.total = a.blkoff + a.nb;
-  a.blkcnt = (unsigned *)(a.total + 1);
+  a.blkoff = (unsigned long long *)h->d_blkoff;
+  a.blkcnt = (unsigned *)h->d_blkcnt;
+  a.total = (unsigned long long *)(h->d_nlive_new + tube);
   k_exp_count<<<a.nb, EXP_THREADS, 0, h->s>>>(a);
   k_exp_scan<<<1, 1024, 0, h->s>>>(a);
   k_exp_write<<<a.nb, EXP_THREADS, 0, h->s>>>(a);
@@ -1690,17 +1706,14 @@ int kaos_get_particles(kaos_handle *h, int32_t tube, double *q, double *vpar,
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&live, a.total, sizeof(live), cudaMemcpyDeviceToHost, h->s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->s);
-  if (e == cudaSuccess && (int64_t)live != n) {
-    cudaFree(st);
+  if (e == cudaSuccess && (int64_t)live != n)
     return fail(h, KAOS_ERR_PARAM, "n (%lld) must equal the ion count (%lld)", (long long)n, (long long)live);
-  }
   double *dst[4] = {q, vpar, vperp1, vperp2};
   for (int k = 0; k < 4 && e == cudaSuccess; ++k)
-    if (dst[k] && n) e = cudaMemcpyAsync(dst[k], dq + k * nd, n * sizeof(double), cudaMemcpyDeviceToHost, h->s);
+    if (dst[k] && n) e = cudaMemcpyAsync(dst[k], dq[k], n * sizeof(double), cudaMemcpyDeviceToHost, h->s);
   if (e == cudaSuccess && qind && n)
     e = cudaMemcpyAsync(qind, dqi, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->s);
-  cudaFree(st);
   if (e != cudaSuccess) return fail(h, KAOS_ERR_CUDA, "get_particles: %s", cudaGetErrorString(e));
   return KAOS_OK;
 }
