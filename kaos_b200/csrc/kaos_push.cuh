@@ -848,6 +848,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   int n_c = DEAD;
   float n_o = 0.f, n_vp = 0.f, n_v1 = 0.f, n_v2 = 0.f, n_ea = 0.f, n_ag = 0.f;
   uint64_t n_id = 0;
+  float n_qk = 0.f;  // q_k4 of the master-step field re-interpolation
   if (beg + threadIdx.x < end) {
     const int64_t j = T.off + beg + threadIdx.x;
     const int2 co = I.co[j];
@@ -855,6 +856,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     n_c = co.x; n_o = __int_as_float(co.y); n_vp = I.fvpar[j];
     n_v1 = v.x; n_v2 = v.y; n_ea = f.x; n_ag = f.y;
     if (a.icr) n_id = I.id[j];
+    if (prologue) n_qk = I.fqk4[j];
   }
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t j = T.off + i;
@@ -864,6 +866,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     float v1 = n_v1, v2 = n_v2;
     float aea = n_ea, ag = n_ag;
     const uint64_t pid = n_id;
+    const float qk0 = n_qk;
     if (i + blockDim.x < end) {
       const int64_t jn = j + blockDim.x;
       const int2 co = I.co[jn];
@@ -871,9 +874,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       n_c = co.x; n_o = __int_as_float(co.y); n_vp = I.fvpar[jn];
       n_v1 = v.x; n_v2 = v.y; n_ea = f.x; n_ag = f.y;
       if (a.icr) n_id = I.id[jn];
+      if (prologue) n_qk = I.fqk4[jn];
     }
     if (c0 == DEAD) continue;
-    if (prologue) field_prologue32(a.ff, T, E, Cc, FE, I.fqk4[j], c0, qs_ms, aea, ag);
+    if (prologue) field_prologue32(a.ff, T, E, Cc, FE, qk0, c0, qs_ms, aea, ag);
     // ---- start-of-step position: q, then (r, theta) by FP64 Newton -------
     const double q0 = fma((double)o0, DQ[c0], QL[c0]);
     const double u = quartic_newton<true>(q0, ipG, fma((double)o0, UD[c0], UL[c0]), 2);
