@@ -151,3 +151,30 @@ def test_graph_replay_with_escapes_and_deferred_packing(tight):
     np.testing.assert_array_equal(a["cnt"], b["cnt"])
     np.testing.assert_array_equal(np.array(a["b"]), np.array(b["b"]))
     assert sum(x[0] + x[1] for x in a["b"]) > 50
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_state_reads_between_steps_change_nothing(mixed):
+    """kaos_get_particles stages through the spare particle buffers, which
+    the packing and the autotuner also use inside a step: reading the state
+    between steps (across a master step with packing and the autotuner's
+    first step) leaves the run bit-identical to one that never reads it."""
+    def run(read):
+        mi, spec, tube, vg = grids.config_escaping()
+        if mixed:
+            mi.precision = KAOS_PREC_MIXED
+        init = grids.initial_particles(tube, spec, mi, seed=37)
+        s = Solver(mi, [tube], vg)
+        s.load(0, *init)
+        for c in (1, 1, 3, 5, 6, 4):  # 20 steps, master every 2
+            s.step(c)
+            if read:
+                s.particles()
+        out = {"p": s.particles(), "cnt": s.counts(), "b": s.boundary()}
+        s.close()
+        return out
+    a, b = run(False), run(True)
+    for k in a["p"]:
+        np.testing.assert_array_equal(a["p"][k], b["p"][k], err_msg=k)
+    np.testing.assert_array_equal(a["cnt"], b["cnt"])
+    np.testing.assert_array_equal(a["b"], b["b"])
