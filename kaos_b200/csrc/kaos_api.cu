@@ -1618,12 +1618,27 @@ int kaos_get_count(kaos_handle *h, int32_t tube, int64_t *nion, int64_t *nena) {
   CK(cudaStreamSynchronize(h->s));
   int64_t nl = 0;
   CK(cudaMemcpy(&nl, h->d_nlive + tube, sizeof(int64_t), cudaMemcpyDeviceToHost));
-  // converted slots (DEAD) are not ions
-  std::vector<int32_t> q(nl);
-  if (nl) CK(cudaMemcpy(q.data(), h->ion[h->cur].qind + h->th[tube].off, nl * 4, cudaMemcpyDeviceToHost));
-  int64_t dead = 0;
-  for (auto v : q) dead += (v == DEAD);
-  if (nion) *nion = nl - dead;
+  // slots converted to ENAs or marked at a removal (DEAD) are not ions:
+  // the live slots are counted on the device (the export's count and scan)
+  int64_t live = 0;
+  if (nl) {
+    ExportArgs a{};
+    a.ion = h->ion[h->cur];
+    a.off = h->th[tube].off;
+    a.nl = nl;
+    a.nb = (int)ceil_div(nl, (int64_t)EXP_THREADS * EXP_ITEMS);
+    a.blkoff = (unsigned long long *)h->d_blkoff;
+    a.blkcnt = (unsigned *)h->d_blkcnt;
+    a.total = (unsigned long long *)(h->d_nlive_new + tube);
+    k_exp_count<<<a.nb, EXP_THREADS, 0, h->s>>>(a);
+    k_exp_scan<<<1, 1024, 0, h->s>>>(a);
+    CK(cudaGetLastError());
+    unsigned long long t = 0;
+    CK(cudaMemcpyAsync(&t, a.total, sizeof(t), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    live = (int64_t)t;
+  }
+  if (nion) *nion = live;
   int64_t ne = 0;
   if (h->d_nena) {
     CK(cudaMemcpy(&ne, h->d_nena + tube, sizeof(int64_t), cudaMemcpyDeviceToHost));
