@@ -191,7 +191,8 @@ def mixed_moment_error(s32, s64):
 def run_e2e(args, precision, launch):
     """Same metric through the public C-ABI with host buffers: the initial
     particle arrays go from pinned host memory to the device once (amortised
-    per step), every step reads the eight per-cell moments back to the host,
+    per step), every step reads all the per-cell moments back to the host
+    (kaos_get_moments_all, into pinned memory),
     and the final ion state comes back into pinned host memory.  The push
     launch shape is the one the autotuner chose for the device-timed run."""
     from kaos_b200.lib import Solver
@@ -213,6 +214,9 @@ def run_e2e(args, precision, launch):
     cap = tube.capacity
     out = {k: pinned(cap, torch.float64) for k in ("q", "vpar", "vperp1", "vperp2")}
     out["qind"] = pinned(cap, torch.int32)
+    from kaos_b200.model_input import KAOS_NMOMENTS
+    mom = torch.empty((KAOS_NMOMENTS, tube.nq), dtype=torch.float64,
+                      pin_memory=True).numpy()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s.load(0, *src)
@@ -221,8 +225,7 @@ def run_e2e(args, precision, launch):
     d2h = 0
     for _ in range(K):
         s.step(1)
-        for m in range(8):
-            d2h += s.moments(m).nbytes
+        d2h += s.moments_all(out=mom).nbytes
     t2 = time.perf_counter()
     p = s.state(out=out)
     d2h += sum(v.nbytes for v in p.values())

@@ -238,6 +238,13 @@ int kaos_get_count(kaos_handle *h, int32_t tube, int64_t *nion,
 int kaos_get_moments(kaos_handle *h, int32_t tube, int32_t which,
                      double *out, int32_t nq);
 
+/* Every selector of kaos_get_moments at once, in one device-to-host copy:
+ * out[m * nq + k] = selector m (KAOS_M0 ... KAOS_ENA_M2PHI), cell k;
+ * out has KAOS_NMOMENTS * nq doubles.  The set DataExport2Sub writes per
+ * master step (_8_0_2_DataExport2.f90:29-150) without one call and one
+ * synchronisation per moment. */
+int kaos_get_moments_all(kaos_handle *h, int32_t tube, double *out, int32_t nq);
+
 /* Integer counts of the latest master step: per-cell ion counts
  * (NqReNormT, nq entries) when nbins == nq, or the full phase-space
  * histogram N2PerpphReNormRT / NphReNormRT laid out

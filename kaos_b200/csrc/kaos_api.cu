@@ -1660,6 +1660,18 @@ int kaos_get_moments(kaos_handle *h, int32_t tube, int32_t which, double *out,
   return KAOS_OK;
 }
 
+int kaos_get_moments_all(kaos_handle *h, int32_t tube, double *out, int32_t nq) {
+  if (!h || !out || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  if (nq != h->th[tube].nq) return fail(h, KAOS_ERR_PARAM, "nq mismatch");
+  // rows of the [KAOS_NMOMENTS][ncell] block, the tube's nq cells of each
+  CK(cudaMemcpy2DAsync(out, (size_t)nq * sizeof(double),
+                       h->ct.mom + h->th[tube].coff, (size_t)h->ncell * sizeof(double),
+                       (size_t)nq * sizeof(double), KAOS_NMOMENTS,
+                       cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return KAOS_OK;
+}
+
 int kaos_get_counts(kaos_handle *h, int32_t tube, int64_t *out, int64_t nbins) {
   if (!h || !out || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
   const TubeD &T = h->th[tube];

@@ -128,6 +128,14 @@ module kaos_gpu_iface
       real(c_double), intent(out) :: out(*)
     end function kaos_get_moments
 
+    integer(c_int) function kaos_get_moments_all(h, tube, out, nq) &
+        bind(C, name="kaos_get_moments_all")
+      import :: c_int, c_int32_t, c_double, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: tube, nq
+      real(c_double), intent(out) :: out(*)
+    end function kaos_get_moments_all
+
     integer(c_int) function kaos_get_counts(h, tube, out, nbins) &
         bind(C, name="kaos_get_counts")
       import :: c_int, c_int32_t, c_int64_t, c_ptr

@@ -14,7 +14,7 @@ from typing import Sequence
 import numpy as np
 
 from .model_input import (KaosParams, KaosTube, KaosVGrid, ModelInput, Tube,
-                          VGrid)
+                          VGrid, KAOS_NMOMENTS)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libkaos_gpu.so")
@@ -29,6 +29,7 @@ EXPORTS = [
     "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
     "kaos_get_launch", "kaos_set_ena_grid", "kaos_init_particles",
     "kaos_set_reduce", "kaos_set_rank", "kaos_set_id_base", "kaos_update_tube",
+    "kaos_get_moments_all",
 ]
 
 # int fn(void *ctx, uint32_t *buf, int64_t count, void *stream)
@@ -57,6 +58,7 @@ def load(path: str = LIBPATH):
     L.kaos_get_step.argtypes = [vp, C.POINTER(i64)]
     L.kaos_get_count.argtypes = [vp, i32, C.POINTER(i64), C.POINTER(i64)]
     L.kaos_get_moments.argtypes = [vp, i32, i32, vp, i32]
+    L.kaos_get_moments_all.argtypes = [vp, i32, vp, i32]
     L.kaos_get_counts.argtypes = [vp, i32, vp, i64]
     L.kaos_set_export.argtypes = [vp, i32]
     L.kaos_get_particles.argtypes = [vp, i32, vp, vp, vp, vp, vp, i64]
@@ -152,6 +154,18 @@ class Solver:
     def moments(self, which, tube=0):
         out = np.zeros(self._tubes[tube].nq)
         self._check(load().kaos_get_moments(self.h, tube, which, _p(out), len(out)))
+        return out
+
+    def moments_all(self, tube=0, out=None):
+        """All KAOS_NMOMENTS selectors at once: array [KAOS_NMOMENTS, nq]
+        (into `out` when given, e.g. pinned host memory)."""
+        nq = self._tubes[tube].nq
+        if out is None:
+            out = np.zeros((KAOS_NMOMENTS, nq))
+        elif out.shape != (KAOS_NMOMENTS, nq) or out.dtype != np.float64 or \
+                not out.flags.c_contiguous:
+            raise ValueError(f"out: C-contiguous float64 array of shape ({KAOS_NMOMENTS}, {nq})")
+        self._check(load().kaos_get_moments_all(self.h, tube, _p(out), nq))
         return out
 
     def counts(self, tube=0, full=False):

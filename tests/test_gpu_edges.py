@@ -187,3 +187,22 @@ def test_mixed_bins_equal_host_binning():
     Hh = np.bincount(idx[ok], minlength=len(qGL) * vg.n1 * vg.n2 * vg.npar)
     assert Hh.sum() > 10000
     np.testing.assert_array_equal(H, Hh)
+
+
+def test_moments_all_equals_each_selector():
+    """kaos_get_moments_all (every selector in one copy) equals
+    kaos_get_moments selector by selector, ion and ENA moments alike."""
+    from kaos_b200.model_input import KAOS_NMOMENTS
+    mi, spec, tube, vg = grids.config_small(n_particles=3000, three_d=True,
+                                            steps_per_master=3, collisions=True)
+    s = Solver(mi, [tube], vg)
+    s.load(0, *grids.initial_particles(tube, spec, mi, seed=19))
+    s.step(7)
+    A = s.moments_all()
+    assert A.shape == (KAOS_NMOMENTS, tube.nq)
+    assert np.max(A[KAOS_M0]) > 0
+    for m in range(KAOS_NMOMENTS):
+        np.testing.assert_array_equal(A[m], s.moments(m), err_msg=str(m))
+    with pytest.raises(ValueError):
+        s.moments_all(out=np.zeros((3, tube.nq)))
+    s.close()
