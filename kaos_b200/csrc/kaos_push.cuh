@@ -449,8 +449,13 @@ __device__ __forceinline__ int vbin_tab(const VBinTab &T, const float *e, int n,
   if (!(v >= e[0] && v <= e[n])) return -1;
   const int s = min(max((int)((v - T.e0) * T.iw), 0), VTAB - 1);
   int b = T.t[s];
-  while (b > 0 && v <= e[b]) --b;
-  while (b < n - 1 && v > e[b + 1]) ++b;
+  // one predicated step up settles almost every value (the table gives the
+  // bin of the slot's left end); the loops finish the rare rest exactly
+  b += (b < n - 1 && v > e[b + 1]) ? 1 : 0;
+  if (__builtin_expect((b > 0 && v <= e[b]) || (b < n - 1 && v > e[b + 1]), 0)) {
+    while (b > 0 && v <= e[b]) --b;
+    while (b < n - 1 && v > e[b + 1]) ++b;
+  }
   return b;
 }
 
