@@ -173,6 +173,32 @@ def run_large(args, precision, steps):
     return dict(value=n * steps / (ms * 1e-3), ms=ms / steps, n=n, launch=launch)
 
 
+def run_batched(args, precision, steps):
+    """Batched uneven tubes (256 tubes, L in [2, 8], 64-512 cells, 1e4-1e6
+    ions each, ~5.7e7 in all, heating on) advancing together: one launch
+    per kernel over the (tube, chunk) work items, steps replayed from CUDA
+    graphs, the autotuner's launch shape."""
+    from kaos_b200 import grids
+    from kaos_b200.lib import Solver
+    mi, specs, tubes, vg = grids.config_c4(args.batched_tubes, precision=precision)
+    s = Solver(mi, tubes, vg)
+    for k, t in enumerate(tubes):
+        s.init_particles(k, t._counts, seed=20261203 + k)
+    s.set_graph(True)
+    if args.launch:
+        s.set_launch(*(int(x) for x in args.launch.split(",")))
+    s.step(args.warmup)
+    n0 = sum(s.count(k)[0] for k in range(len(tubes)))
+    s.step(steps)
+    ms, _ = s.timing()
+    n1 = sum(s.count(k)[0] for k in range(len(tubes)))
+    launch = s.launch()
+    s.close()
+    n = 0.5 * (n0 + n1)
+    return dict(value=n * steps / (ms * 1e-3), ms=ms / steps, n=n, launch=launch,
+                ntubes=len(tubes))
+
+
 def mixed_moment_error(s32, s64):
     """Norm-wise relative difference max|m32 - m64| / max|m64| per moment."""
     from kaos_b200 import model_input as M
@@ -341,7 +367,9 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--large-particles", type=int, default=100_000_000,
                     help="ions of the large single-tube line (0: skip it)")
-    ap.add_argument("--only", default="all", choices=["all", "mixed", "large", "cadence1"],
+    ap.add_argument("--batched-tubes", type=int, default=256,
+                    help="tubes of the batched uneven-tube line (0: skip it)")
+    ap.add_argument("--only", default="all", choices=["all", "mixed", "large", "cadence1", "batched"],
                     help="mixed: time the mixed path alone; large: the large single "
                          "tube's mixed path alone; cadence1: the mixed path with every "
                          "step a master step (all for profiling)")
@@ -364,6 +392,13 @@ def main():
         print(json.dumps({"cadence1_mixed": r["value"], "ms_per_step": r["ms"] / args.steps,
                           "push_ms": r["push_ms"], "steps": args.steps,
                           "launch": r["launch"]}), flush=True)
+        return
+    if args.only == "batched":
+        from kaos_b200.model_input import KAOS_PREC_MIXED
+        b32 = run_batched(args, KAOS_PREC_MIXED, args.steps)
+        print(json.dumps({"batched_mixed": b32["value"], "ms_per_step": b32["ms"],
+                          "n": b32["n"], "tubes": b32["ntubes"], "steps": args.steps,
+                          "launch": b32["launch"]}), flush=True)
         return
     if args.only == "large":
         from kaos_b200.model_input import KAOS_PREC_MIXED
@@ -436,6 +471,22 @@ def main():
                  "fp64_ms_per_step": l64["ms"],
                  "mixed_over_fp64": l32["value"] / l64["value"],
                  "note": "both paths replayed from CUDA graphs"}
+    batched = None
+    if full and args.batched_tubes > 0:
+        bsteps = min(args.steps, 100)
+        b32 = run_batched(args, KAOS_PREC_MIXED, bsteps)
+        b64 = run_batched(args, KAOS_PREC_FP64, bsteps)
+        batched = {"workload": f"{b32['ntubes']} batched uneven tubes: L uniform in [2, 8], "
+                               "64-512 cells, 1e4-1e6 O+ each (log-uniform), "
+                               f"{int(b32['n'])} in all, n0 1e9-1e11 m^-3, T 0.1-1 eV, "
+                               "shared 3D grid 48x48x64, heating 1e-4-1e-2 eV/s, dt 5 ms",
+                   "steps": bsteps, "mixed": b32["value"] * world,
+                   "mixed_ms_per_step": b32["ms"], "fp64": b64["value"] * world,
+                   "fp64_ms_per_step": b64["ms"],
+                   "mixed_over_fp64": b32["value"] / b64["value"],
+                   "push_launch": b32["launch"],
+                   "note": "one launch per kernel over (tube, chunk) work items; "
+                           "both paths replayed from CUDA graphs"}
     cpu = cpu_baseline(args) if (rank == 0 and world == 1 and full) else None
     tpi = profiled_traffic("k_push32_mixed_c2.md")
     traffic = None if tpi is None else tpi * r32["n"]
@@ -465,6 +516,7 @@ def main():
             "mixed_over_fp64": value / (r64["value"] * world) if full else None,
             "mixed_push_ms": r32["push_ms"],
             "large": large,
+            "batched": batched,
             "moment_error_vs_fp64": moment_error,
             "graph": None if not full else {
                 "value": rg["value"] * world, "ms_per_step": rg["ms"] / args.steps,

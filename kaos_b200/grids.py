@@ -264,6 +264,33 @@ def config_c3(n_particles=100_000_000, precision=KAOS_PREC_MIXED, ndatfac=50):
     return mi, spec, tube, vg
 
 
+def config_c4(ntubes=256, precision=KAOS_PREC_MIXED, ndatfac=50, seed=4):
+    """Batched uneven tubes in one launch: ntubes flux tubes with L uniform
+    in [2, 8], cells per tube uniform in {64..512}, ions per tube
+    log-uniform in [1e4, 1e6] (about 5e7 for 256 tubes), base density
+    log-uniform in [1e9, 1e11] m^-3, T uniform in [0.1, 1] eV, a shared
+    3D grid 48x48x64, heating on with a per-tube base rate log-uniform in
+    [1e-4, 1e-2] eV/s; dt 0.005 s.  The tube parameters are drawn from a
+    seeded generator; initial ions come from kaos_init_particles with each
+    tube's per-cell counts (tube._counts)."""
+    rng = np.random.default_rng(seed)
+    mi = ModelInput(h=0.005, ndatfac=ndatfac, ION2VPERPflag=1, ICRflag=1,
+                    precision=precision)
+    specs, tubes = [], []
+    for _ in range(ntubes):
+        sp = TubeSpec(L=float(rng.uniform(2.0, 8.0)),
+                      nq=int(rng.integers(64, 513)),
+                      n_particles=int(round(10 ** rng.uniform(4.0, 6.0))),
+                      q_ub=1e-3, n0=float(10 ** rng.uniform(9.0, 11.0)),
+                      Ti=float(rng.uniform(0.1, 1.0)) * 1.602e-19 / KB,
+                      heat_rate_eV_s=float(10 ** rng.uniform(-4.0, -2.0)),
+                      chi=1.7)
+        specs.append(sp)
+        tubes.append(make_tube(sp, mi))
+    vg = make_vgrid(True, 48, 48, 64, 30e3)
+    return mi, specs, tubes, vg
+
+
 def config_escaping():
     """A short hot tube (L=3, 24 cells up to |q| = 0.5, 5 eV O+, dt 1 s,
     master step every 2 steps) that loses ~40 ions per master step through
