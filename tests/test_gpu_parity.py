@@ -352,3 +352,22 @@ def test_convection_to_new_lshell(mixed):
     np.testing.assert_array_equal(s.counts(), o.counts())
     for m in (KAOS_M0, KAOS_M2, KAOS_M2PAR, KAOS_EAMAG):
         assert rel_norm(s.moments(m), o.moments(m)) < MOM_TOL, m
+
+
+def test_fp64_charge_exchange_across_packing():
+    """Charge exchange every step over ten master steps (slots converted to
+    ENAs and escaped ions both marked dead, the arrays packed at the eighth
+    master step): ions, ENA count, counts and moments equal the oracle's."""
+    mi, spec, tube, vg = grids.config_small(n_particles=4000, three_d=True,
+                                            steps_per_master=2, collisions=True)
+    tube.nsnormCLB = 12.0
+    o, s = run_pair(mi, spec, tube, vg, 21)
+    assert s.count() == o.count()
+    assert o.count()[1] > 10
+    po, ps = o.particles(), s.particles()
+    for k in ("z", "vpar", "vperp1", "vperp2"):
+        assert rel_norm(ps[k], po[k]) < TRAJ_TOL, k
+    np.testing.assert_array_equal(ps["qind"], po["qind"])
+    np.testing.assert_array_equal(s.counts(), o.counts())
+    for m in (KAOS_M0, KAOS_M2PAR):
+        assert rel_norm(s.moments(m), o.moments(m)) < MOM_TOL, m
