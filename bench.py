@@ -207,6 +207,49 @@ def run_batched(args, precision, steps):
                 ntubes=len(tubes))
 
 
+def run_c5(args, precision, steps):
+    """Two species plus neutral products, batched: 64 tubes (L 3-7, 256
+    cells) with O+ and H+ as two entries each (2e7 ions), charge exchange
+    with an H exosphere producing ENAs, ENA moments, and the 0.5 km/s E x B
+    drift: after every master interval each entry's tables are regenerated
+    on its new L-shell on the host and queued with kaos_update_tube (applied
+    at the next master step).  Device time of the steps only; steps replayed
+    from CUDA graphs except the master steps that apply a move."""
+    from kaos_b200 import grids
+    from kaos_b200.lib import Solver
+    mi, specs, tubes, vg, evg = grids.config_c5(precision=precision)
+    s = Solver(mi, tubes, vg)
+    s.set_ena_grid(evg)
+    for k, t in enumerate(tubes):
+        s.init_particles(k, t._counts, seed=20261203 + k)
+    s.set_graph(True)
+    if args.launch:
+        s.set_launch(*(int(x) for x in args.launch.split(",")))
+    Ls = [sp.L for sp in specs]
+    nd = mi.ndatfac
+
+    def intervals(n):
+        ms = 0.0
+        for _ in range(n):
+            s.step(nd)
+            ms += s.timing()[0]
+            for k in range(len(tubes)):  # E x B drift to the next L-shell
+                Ls[k] += grids.CONV_C5_DL
+                s.update_tube(k, grids.moved_tube(specs[k], mi, s._tubes[k], Ls[k]))
+        return ms
+    intervals(2)  # warm-up: two master intervals (every step graph captured)
+    cnt = lambda i: sum(s.count(k)[i] for k in range(len(tubes)))
+    n0 = cnt(0)
+    nint = max(1, steps // nd)
+    ms = intervals(nint)
+    n1, ne = cnt(0), cnt(1)
+    launch = s.launch()
+    s.close()
+    n = 0.5 * (n0 + n1)
+    return dict(value=n * nint * nd / (ms * 1e-3), ms=ms / (nint * nd), n=n, enas=ne,
+                steps=nint * nd, launch=launch, entries=len(tubes))
+
+
 def mixed_moment_error(s32, s64):
     """Norm-wise relative difference max|m32 - m64| / max|m64| per moment."""
     from kaos_b200 import model_input as M
@@ -377,7 +420,10 @@ def main():
                     help="ions of the large single-tube line (0: skip it)")
     ap.add_argument("--batched-tubes", type=int, default=256,
                     help="tubes of the batched uneven-tube line (0: skip it)")
-    ap.add_argument("--only", default="all", choices=["all", "mixed", "large", "cadence1", "batched"],
+    ap.add_argument("--c5", type=int, default=1,
+                    help="1: time the two-species/ENA/convection batch (0: skip it)")
+    ap.add_argument("--only", default="all",
+                    choices=["all", "mixed", "large", "cadence1", "batched", "c5"],
                     help="mixed: time the mixed path alone; large: the large single "
                          "tube's mixed path alone; cadence1: the mixed path with every "
                          "step a master step (all for profiling)")
@@ -400,6 +446,13 @@ def main():
         print(json.dumps({"cadence1_mixed": r["value"], "ms_per_step": r["ms"] / args.steps,
                           "push_ms": r["push_ms"], "steps": args.steps,
                           "launch": r["launch"]}), flush=True)
+        return
+    if args.only == "c5":
+        from kaos_b200.model_input import KAOS_PREC_MIXED
+        c = run_c5(args, KAOS_PREC_MIXED, args.steps)
+        print(json.dumps({"c5_mixed": c["value"], "ms_per_step": c["ms"], "n": c["n"],
+                          "enas": c["enas"], "steps": c["steps"], "launch": c["launch"]}),
+              flush=True)
         return
     if args.only == "batched":
         from kaos_b200.model_input import KAOS_PREC_MIXED
@@ -495,6 +548,28 @@ def main():
                    "push_launch": b32["launch"],
                    "note": "one launch per kernel over (tube, chunk) work items; "
                            "both paths replayed from CUDA graphs"}
+    species = None
+    if full and args.c5:
+        try:
+            c32 = run_c5(args, KAOS_PREC_MIXED, min(args.steps, 100))
+            c64 = run_c5(args, KAOS_PREC_FP64, min(args.steps, 100))
+            species = {"workload": "64 tubes (L 3-7, 256 cells), O+ and H+ at 4:1 density as "
+                                   f"{c32['entries']} entries, {int(c32['n'])} ions, charge "
+                                   "exchange with an H exosphere (1e16 m^-3 at the base: "
+                                   "the per-cell Poisson mean at 1e11 forms no ENA; "
+                                   "scale height 1000 km) to "
+                                   f"{c32['enas']} ENAs, ENA moments on 48x48x64, E x B "
+                                   "drift 0.5 km/s (tables regenerated each master interval), "
+                                   "dt 5 ms",
+                       "steps": c32["steps"], "mixed": c32["value"] * world,
+                       "mixed_ms_per_step": c32["ms"], "fp64": c64["value"] * world,
+                       "fp64_ms_per_step": c64["ms"],
+                       "mixed_over_fp64": c32["value"] / c64["value"],
+                       "note": "ion-steps per second of device time (host table "
+                               "regeneration excluded); CUDA graphs except the master "
+                               "steps that apply a move"}
+        except Exception as e:  # reported, never fatal to the bench line
+            species = {"error": f"{type(e).__name__}: {e}"}
     cpu = cpu_baseline(args) if (rank == 0 and world == 1 and full) else None
     tpi = profiled_traffic("k_push32_mixed_c2.md")
     traffic = None if tpi is None else tpi * r32["n"]
@@ -525,6 +600,7 @@ def main():
             "mixed_push_ms": r32["push_ms"],
             "large": large,
             "batched": batched,
+            "species_ena_convection": species,
             "moment_error_vs_fp64": moment_error,
             "graph": None if not full else {
                 "value": rg["value"] * world, "ms_per_step": rg["ms"] / args.steps,

@@ -15,7 +15,7 @@ import dataclasses
 
 import numpy as np
 
-from .model_input import (KB, MO, PI, RE, GG, ME, ModelInput, Tube, VGrid,
+from .model_input import (KB, MH, MO, PI, RE, GG, ME, ModelInput, Tube, VGrid,
                           KAOS_PREC_FP64, KAOS_PREC_MIXED)
 
 
@@ -289,6 +289,43 @@ def config_c4(ntubes=256, precision=KAOS_PREC_MIXED, ndatfac=50, seed=4):
         tubes.append(make_tube(sp, mi))
     vg = make_vgrid(True, 48, 48, 64, 30e3)
     return mi, specs, tubes, vg
+
+
+def config_c5(ntubes=64, n_ions=20_000_000, precision=KAOS_PREC_MIXED,
+              ndatfac=50, seed=5, neut_n0=1e16):
+    """Two species plus neutral products, batched: ntubes flux tubes with L
+    uniform in [3, 7], 256 cells each, H+ and O+ at a 1:4 density ratio as
+    two entries per tube (2e7 ions in all), charge exchange with a neutral
+    H exosphere (scale height 1000 km) producing ENAs, ENA moments on a
+    48x48x64 grid (the returned evg), dt 0.005 s.  The collision model's
+    Poisson mean is per cell and step (n_n sigma v h, not times the cell's
+    ions), so at the configuration's 1e11 m^-3 base density it is ~1e-7 and
+    no ENA would form within a run; neut_n0 (default 1e16 m^-3) sets it.
+    Entries alternate O+, H+ per tube.  The E x B drift of 0.5 km/s moves
+    each tube by CONV_C5_DL in L per master step (grids.moved_tube and
+    kaos_update_tube)."""
+    rng = np.random.default_rng(seed)
+    mi = ModelInput(h=0.005, ndatfac=ndatfac, ION2VPERPflag=1, QEXCHANGEflag=1,
+                    precision=precision)
+    mi.mNeut = MH
+    per_tube = n_ions / ntubes
+    specs, tubes = [], []
+    for _ in range(ntubes):
+        L = float(rng.uniform(3.0, 7.0))
+        for ms, frac, n0 in ((MO, 0.8, 1e10), (MH, 0.2, 2.5e9)):
+            sp = TubeSpec(L=L, nq=256, n_particles=int(round(per_tube * frac)),
+                          q_ub=1e-3, n0=n0, neut_n0=neut_n0, neut_H=1000e3,
+                          ms=ms, qs=1.602e-19)
+            specs.append(sp)
+            tubes.append(make_tube(sp, mi))
+    vg = make_vgrid(True, 48, 48, 64, 30e3)
+    evg = make_vgrid(True, 48, 48, 64, 30e3)
+    return mi, specs, tubes, vg, evg
+
+
+# L-shell change of a tube per master step under a 0.5 km/s E x B drift at
+# the equator (dL = v dt / RE, dt = 50 steps of 5 ms)
+CONV_C5_DL = 500.0 * 50 * 0.005 / RE
 
 
 def config_escaping():
