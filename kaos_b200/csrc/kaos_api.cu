@@ -125,6 +125,16 @@ struct kaos_handle {
   unsigned *d_cxc = nullptr, *d_cxo = nullptr;
   int *d_cxend = nullptr;
   int *d_tube_done = nullptr;  // per tube: charge-exchange cell scans done
+  // convection: device staging of the moves of one master step (allocated
+  // at the first move) and its host side
+  double *d_conv_stage = nullptr, *d_conv_pnew = nullptr;
+  TubeD *d_conv_td = nullptr;
+  int *d_conv_tube = nullptr;
+  struct ConvHost {
+    std::vector<double> stage, pnew;
+    std::vector<TubeD> td;
+    std::vector<int> tube;
+  } conv_host;
   int *d_cell_tube = nullptr, *d_cell_q = nullptr;  // global cell -> (tube, cell)
   int ncx = 0;
   int64_t n = 0;      // computational steps taken
@@ -406,31 +416,64 @@ const double *conv_table_ptr(const CellTables &c, int k) {
   return p[k];
 }
 
-// Move the tubes given to kaos_update_tube: re-project their ions with the
-// old tables (k_convect), then copy the new tables and descriptor in.  The
-// host copies are asynchronous from the handle's pending vectors, which stay
-// alive until the end of the kaos_step call.
+// Move the tubes given to kaos_update_tube, all in two launches: re-project
+// their ions with the old tables and descriptors (k_convect_many), then put
+// the new tables and descriptors in place (k_apply_tables) from one staging
+// copy.
 int apply_pending_tubes(kaos_handle *h) {
-  for (auto &pt : h->pending) {
-    TubeD &old = h->th[pt.tube];
-    ConvArgs ca{};
-    ca.T = old;
-    ca.p_new = pt.d.pG;
-    ca.nlive = h->d_nlive;
-    ca.tube = pt.tube;
-    ca.ion = h->ion[h->cur];
-    ca.ct = h->ct;
-    ca.mixed = h->mixed;
-    const int grid = (int)std::min<int64_t>((old.cap + 255) / 256, 148 * 16);
-    k_convect<<<grid, 256, 0, h->s>>>(ca);
-    h->launches++;
-    CK(cudaGetLastError());
+  static_assert(CONV_TABLES == CONV_NTAB, "table count");
+  const int np = (int)h->pending.size();
+  if (!np) return KAOS_OK;
+  const int nqm = max_nq(h);
+  int rc;
+  if (!h->d_conv_stage &&  // staging for every entry moving at once
+      ((rc = dalloc(h, &h->d_conv_stage, (size_t)h->ntubes * CONV_TABLES * nqm)) ||
+       (rc = dalloc(h, &h->d_conv_td, (size_t)h->ntubes)) ||
+       (rc = dalloc(h, &h->d_conv_tube, (size_t)h->ntubes)) ||
+       (rc = dalloc(h, &h->d_conv_pnew, (size_t)h->ntubes))))
+    return rc;
+  // the moves, their new descriptors and tables in host staging (kept in
+  // the handle until the next move), one copy each
+  auto &S = h->conv_host;
+  S.stage.assign((size_t)np * CONV_TABLES * nqm, 0.0);
+  S.td.resize(np);
+  S.tube.resize(np);
+  S.pnew.resize(np);
+  for (int p = 0; p < np; ++p) {
+    const auto &pt = h->pending[p];
+    S.td[p] = pt.d;
+    S.tube[p] = pt.tube;
+    S.pnew[p] = pt.d.pG;
     for (int k = 0; k < CONV_TABLES; ++k)
-      CK(cudaMemcpyAsync((void *)(conv_table_ptr(h->ct, k) + old.coff), pt.tables[k].data(),
-                         old.nq * sizeof(double), cudaMemcpyHostToDevice, h->s));
-    old = pt.d;
-    CK(cudaMemcpyAsync(h->d_tubes + pt.tube, &old, sizeof(TubeD), cudaMemcpyHostToDevice, h->s));
+      std::copy(pt.tables[k].begin(), pt.tables[k].end(),
+                S.stage.begin() + ((size_t)p * CONV_TABLES + k) * nqm);
   }
+  CK(cudaMemcpyAsync(h->d_conv_stage, S.stage.data(), S.stage.size() * sizeof(double),
+                     cudaMemcpyHostToDevice, h->s));
+  CK(cudaMemcpyAsync(h->d_conv_td, S.td.data(), np * sizeof(TubeD), cudaMemcpyHostToDevice, h->s));
+  CK(cudaMemcpyAsync(h->d_conv_tube, S.tube.data(), np * sizeof(int), cudaMemcpyHostToDevice, h->s));
+  CK(cudaMemcpyAsync(h->d_conv_pnew, S.pnew.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->s));
+  // re-project the ions with the old tables and descriptors, then swap them
+  ConvManyArgs ca{};
+  ca.tubes = h->d_tubes;
+  ca.tube = h->d_conv_tube;
+  ca.p_new = h->d_conv_pnew;
+  ca.nlive = h->d_nlive;
+  ca.ion = h->ion[h->cur];
+  ca.ct = h->ct;
+  ca.mixed = h->mixed;
+  k_convect_many<<<dim3(std::max(1, 148 * 16 / np), np), 256, 0, h->s>>>(ca);
+  TableApplyArgs ta{};
+  for (int k = 0; k < CONV_TABLES; ++k) ta.dst[k] = (double *)conv_table_ptr(h->ct, k);
+  ta.stage = h->d_conv_stage;
+  ta.td = h->d_conv_td;
+  ta.tube = h->d_conv_tube;
+  ta.tubes = h->d_tubes;
+  ta.nqmax = nqm;
+  k_apply_tables<<<dim3(CONV_TABLES, np), 256, 0, h->s>>>(ta);
+  h->launches += 2;
+  CK(cudaGetLastError());
+  for (const auto &pt : h->pending) h->th[pt.tube] = pt.d;
   return KAOS_OK;
 }
 

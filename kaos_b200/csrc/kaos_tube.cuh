@@ -870,7 +870,19 @@ __device__ __forceinline__ double bnorm(double q, double u) {
   return sqrt(1.0 + 3.0 * ct * ct) / (u * u * u);
 }
 
-__global__ void k_convect(ConvArgs a) {
+// The queued moves of one master step in one launch: blockIdx.y = the move
+// (its entry and new L-shell), blockIdx.x strides over the entry's ions.
+struct ConvManyArgs {
+  const TubeD *tubes;   // the descriptors before the moves
+  const int *tube;      // per move: the entry
+  const double *p_new;  // per move: the new L-shell
+  const int64_t *nlive;
+  Ions ion;
+  CellTables ct;
+  int mixed;
+};
+
+__device__ __forceinline__ void convect_ions(const ConvArgs &a) {
   const TubeD &T = a.T;
   const int64_t nl = a.nlive[a.tube];
   const double ip_old = 1.0 / T.pG, ip_new = 1.0 / a.p_new;
@@ -909,6 +921,38 @@ __global__ void k_convect(ConvArgs a) {
       a.ion.v2[j] = f * a.ion.v2[j];
     }
   }
+}
+
+__global__ void k_convect_many(ConvManyArgs m) {
+  ConvArgs a;
+  a.tube = m.tube[blockIdx.y];
+  a.T = m.tubes[a.tube];
+  a.p_new = m.p_new[blockIdx.y];
+  a.nlive = m.nlive;
+  a.ion = m.ion;
+  a.ct = m.ct;
+  a.mixed = m.mixed;
+  convect_ions(a);
+}
+
+// The new per-cell tables and descriptors of the moved entries, from one
+// staging copy: blockIdx.y = the move, blockIdx.x = the table.
+constexpr int CONV_NTAB = 27;
+struct TableApplyArgs {
+  double *dst[CONV_NTAB];  // the per-cell tables (concatenated over entries)
+  const double *stage;     // [move][table][nqmax]
+  const TubeD *td;         // per move: the new descriptor
+  const int *tube;         // per move: the entry
+  TubeD *tubes;
+  int nqmax;
+};
+
+__global__ void k_apply_tables(TableApplyArgs a) {
+  const int p = blockIdx.y, k = blockIdx.x;
+  const TubeD &T = a.td[p];
+  const double *src = a.stage + ((int64_t)p * CONV_NTAB + k) * a.nqmax;
+  for (int i = threadIdx.x; i < T.nq; i += blockDim.x) a.dst[k][T.coff + i] = src[i];
+  if (k == 0 && threadIdx.x == 0) a.tubes[a.tube[p]] = T;
 }
 
 }  // namespace kaos
