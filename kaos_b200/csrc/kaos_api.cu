@@ -125,6 +125,7 @@ struct kaos_handle {
   unsigned *d_cxc = nullptr, *d_cxo = nullptr;
   int *d_cxend = nullptr;
   int *d_tube_done = nullptr;  // per tube: charge-exchange cell scans done
+  int *d_cx_list = nullptr, *d_cx_nlist = nullptr, *d_tube_active = nullptr;
   // convection: device staging of the moves of one master step (allocated
   // at the first move) and its host side
   double *d_conv_stage = nullptr, *d_conv_pnew = nullptr;
@@ -487,6 +488,8 @@ int reduce_accum(kaos_handle *h) {
   return KAOS_OK;
 }
 
+CxArgs cx_args(kaos_handle *h);
+
 int launch_moments(kaos_handle *h, uint32_t nn) {
   TubeArgs ta = tube_args(h, nn);
   const int cells_per_block = 256 / 32;
@@ -496,7 +499,12 @@ int launch_moments(kaos_handle *h, uint32_t nn) {
   if (ta.qexchange) {
     size_t smem = (size_t)8 * max_nq(h) * sizeof(double);
     k_collision_counts<<<h->ntubes, 256, smem, h->s>>>(ta);
-    h->launches++;
+    // the cells that will convert ions until the next master step
+    CK(cudaMemsetAsync(h->d_cx_nlist, 0, sizeof(int), h->s));
+    CK(cudaMemsetAsync(h->d_tube_active, 0, h->ntubes * sizeof(int), h->s));
+    k_cx_list<<<(int)((h->ncell + 255) / 256), 256, 0, h->s>>>(cx_args(h), h->d_cell_tube,
+                                                             h->ncell);
+    h->launches += 2;
     if (nn > 1) {  // ENA statistics from the second master step on
       k_ena_moments<<<(int)((h->ncell + cells_per_block - 1) / cells_per_block), 256, 0, h->s>>>(
           h->d_tubes, h->d_cell_tube, h->ct, h->acc);
@@ -712,6 +720,9 @@ CxArgs cx_args(kaos_handle *h) {
   a.cxbase = h->d_cxbase;
   a.cxend = h->d_cxend;
   a.tube_done = h->d_tube_done;
+  a.list = h->d_cx_list;
+  a.nlist = h->d_cx_nlist;
+  a.tube_active = h->d_tube_active;
   a.rank = h->rank;
   a.nranks = h->nranks;
   a.nqmax = max_nq(h);
@@ -738,7 +749,8 @@ int launch_cx(kaos_handle *h) {
   const int nq = max_nq(h);
   // the per-chunk Qindk1 counts were accumulated by the previous push
   // 1024 threads: one tile covers the chunks of a tube of up to 16.7 M ions
-  k_cx_scan<<<(int)h->ncell, 1024, 0, h->s>>>(a, h->d_cell_tube, h->d_cell_q);
+  k_cx_scan<<<std::max(1, strided_grid(h, (int)h->ncell) / 2), 1024, 0, h->s>>>(
+      a, h->d_cell_tube, h->d_cell_q);
   // one block per chunk (a chunk with conversions walks its ions in order;
   // blocks of chunks without live ions leave at once)
   k_cx_convert<<<std::max(h->ncx, 1), 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
@@ -1339,6 +1351,9 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
         (rc = dalloc(h, &h->d_cxbase, cxt.size())) ||
         (rc = dalloc(h, &h->d_cxend, (size_t)h->ncell)) ||
         (rc = dalloc(h, &h->d_tube_done, (size_t)ntubes)) ||
+        (rc = dalloc(h, &h->d_cx_list, (size_t)h->ncell)) ||
+        (rc = dalloc(h, &h->d_cx_nlist, 1)) ||
+        (rc = dalloc(h, &h->d_tube_active, (size_t)ntubes)) ||
         (rc = dalloc(h, &h->d_cxc, cxt.size() * (size_t)max_nq(h))) ||
         (rc = dalloc(h, &h->d_cxo, cxt.size() * (size_t)max_nq(h))))
       return rc;

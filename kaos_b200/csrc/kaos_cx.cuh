@@ -35,6 +35,8 @@ struct CxArgs {
   int64_t *cxbase;           // per chunk: ENA slot of its first conversion
   int *cxend;                // per cell (all tubes): chunks >= cxend convert none
   int *tube_done;            // per tube: cell scans finished this step
+  int *list, *nlist;         // cells with conversions (need > 0), their count
+  int *tube_active;          // per tube: listed cells
   int nqmax, mixed;
   int ncx;                   // selection chunks (all tubes)
   int rank, nranks;          // this rank's share of a split tube's conversions
@@ -129,24 +131,40 @@ __device__ __forceinline__ void cx_base_tube(const CxArgs &a, int t) {
   if (threadIdx.x == 0) a.nena[t] = n0 + (int64_t)tot;
 }
 
-// One block (1024 threads) per (tube, cell): the cell's scan, then the last
-// block of a tube to finish (a per-tube arrival counter) gives the tube its
-// ENA slots; it also resets the counter for the next step.
+// The cells that convert ions (need > 0) are listed once per master step,
+// when the collision counts change, with each tube's number of them.
+__global__ void k_cx_list(CxArgs a, const int *cell_tube, int64_t ncell) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ncell) return;
+  if (cx_need(a, a.ct.nuPoi[g]) == 0u) return;
+  a.list[atomicAdd(a.nlist, 1)] = (int)g;
+  atomicAdd(a.tube_active + cell_tube[g], 1);
+}
+
+// A block (1024 threads) per listed cell, striding over the list: the
+// cell's scan, then the last listed cell of a tube to finish (a per-tube
+// arrival counter) gives the tube its ENA slots and resets the counter.
+// Tubes without a listed cell convert nothing this step.
 __global__ void __launch_bounds__(1024) k_cx_scan(CxArgs a, const int *cell_tube,
                                                   const int *cell_q) {
-  const int t = cell_tube[blockIdx.x], k = cell_q[blockIdx.x];
-  cx_scan_cell(a, t, k, blockIdx.x);
+  const int nl = *a.nlist;
   __shared__ int last;
-  __syncthreads();  // every thread's counts and prefixes are written
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(a.tube_done + t, 1) == a.tubes[t].nq - 1;
-    if (last) a.tube_done[t] = 0;
-  }
-  __syncthreads();
-  if (last) {
-    __threadfence();
-    cx_base_tube(a, t);
+  for (int i = blockIdx.x; i < nl; i += gridDim.x) {
+    const int g = a.list[i];
+    const int t = cell_tube[g], k = cell_q[g];
+    __syncthreads();  // the previous cell of this block is done with smem
+    cx_scan_cell(a, t, k, g);
+    __syncthreads();  // every thread's counts and prefixes are written
+    if (threadIdx.x == 0) {
+      __threadfence();
+      last = atomicAdd(a.tube_done + t, 1) == a.tube_active[t] - 1;
+      if (last) a.tube_done[t] = 0;
+    }
+    __syncthreads();
+    if (last) {
+      __threadfence();
+      cx_base_tube(a, t);
+    }
   }
 }
 
