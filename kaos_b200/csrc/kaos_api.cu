@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -196,6 +197,10 @@ struct kaos_handle {
 };
 
 namespace {
+
+// The handle whose velocity grids were copied last into c_vg / c_evg; a
+// step of another handle, or after a grid change, copies its own.
+std::atomic<const kaos_handle *> g_grid_owner{nullptr};
 
 int fail(kaos_handle *h, int code, const char *fmt, ...) {
   if (h) {
@@ -1396,6 +1401,7 @@ int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
     for (int k = 0; k < na && e == cudaSuccess; ++k)
       e = cudaMemcpy(stage[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_vg, &h->vg, sizeof(VGridC));
+    g_grid_owner = nullptr;  // c_evg may belong to another handle
     if (e == cudaSuccess) {
       LoadArgs a{};
       a.T = T;
@@ -1462,6 +1468,7 @@ int kaos_init_particles(kaos_handle *h, int32_t tube, const kaos_init_c *in) {
   a.mixed = h->mixed;
   cudaError_t e = cudaMemcpy(d_pre, pre.data(), pre.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_vg, &h->vg, sizeof(VGridC));
+    g_grid_owner = nullptr;  // c_evg may belong to another handle
   if (e == cudaSuccess && n > 0) {
     const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 32);
     k_init<<<grid, 256>>>(a);
@@ -1533,6 +1540,7 @@ int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode) {
 
 int kaos_set_ena_grid(kaos_handle *h, const kaos_vgrid_c *vg) {
   if (!h || !vg) return KAOS_ERR_PARAM;
+  g_grid_owner = nullptr;  // the next step uploads the new grid
   if (h->n != 0) return fail(h, KAOS_ERR_STATE, "the ENA grid is set before the first step");
   if (vg->n1 < 1 || vg->n2 < 1 || vg->npar < 1 || vg->n1 > MAXV || vg->n2 > MAXV ||
       vg->npar > MAXV || !vg->e1 || !vg->e2 || !vg->epar)
@@ -1616,8 +1624,11 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
   if (!h) return KAOS_ERR_PARAM;
   if (!h->loaded) return fail(h, KAOS_ERR_STATE, "kaos_step before kaos_load_particles");
   if (nsteps < 0) return fail(h, KAOS_ERR_PARAM, "nsteps < 0");
-  CK(cudaMemcpyToSymbolAsync(c_vg, &h->vg, sizeof(VGridC), 0, cudaMemcpyHostToDevice, h->s));
-  CK(cudaMemcpyToSymbolAsync(c_evg, &h->evg, sizeof(VGridC), 0, cudaMemcpyHostToDevice, h->s));
+  if (g_grid_owner != h) {  // the velocity grids in constant memory
+    CK(cudaMemcpyToSymbolAsync(c_vg, &h->vg, sizeof(VGridC), 0, cudaMemcpyHostToDevice, h->s));
+    CK(cudaMemcpyToSymbolAsync(c_evg, &h->evg, sizeof(VGridC), 0, cudaMemcpyHostToDevice, h->s));
+    g_grid_owner = h;
+  }
   h->launches = 0;
   h->npev = 0;
   CK(cudaEventRecord(h->e0, h->s));
@@ -1890,6 +1901,7 @@ int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches) {
 
 void kaos_destroy(kaos_handle *h) {
   if (!h) return;
+  if (g_grid_owner == h) g_grid_owner = nullptr;
   if (h->s) cudaStreamSynchronize(h->s);
   if (h->s2) cudaStreamSynchronize(h->s2);
   for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
