@@ -226,6 +226,7 @@ def run_c5(args, precision, steps):
     if args.launch:
         s.set_launch(*(int(x) for x in args.launch.split(",")))
     Ls = [sp.L for sp in specs]
+    cur = list(tubes)  # each entry's tables on its current L-shell
     nd = mi.ndatfac
 
     def intervals(n):
@@ -235,7 +236,8 @@ def run_c5(args, precision, steps):
             ms += s.timing()[0]
             for k in range(len(tubes)):  # E x B drift to the next L-shell
                 Ls[k] += grids.CONV_C5_DL
-                s.update_tube(k, grids.moved_tube(specs[k], mi, s._tubes[k], Ls[k]))
+                cur[k] = grids.moved_tube(specs[k], mi, cur[k], Ls[k])
+                s.update_tube(k, cur[k])
         return ms
     intervals(2)  # warm-up: two master intervals (every step graph captured)
     cnt = lambda i: sum(s.count(k)[i] for k in range(len(tubes)))
