@@ -133,7 +133,8 @@ struct kaos_handle {
   TubeD *d_conv_td = nullptr;
   int *d_conv_tube = nullptr;
   struct ConvHost {
-    std::vector<double> stage, pnew;
+    double *stage = nullptr;  // pinned: [move][table][nqmax]
+    std::vector<double> pnew;
     std::vector<TubeD> td;
     std::vector<int> tube;
   } conv_host;
@@ -432,16 +433,19 @@ int apply_pending_tubes(kaos_handle *h) {
   if (!np) return KAOS_OK;
   const int nqm = max_nq(h);
   int rc;
-  if (!h->d_conv_stage &&  // staging for every entry moving at once
-      ((rc = dalloc(h, &h->d_conv_stage, (size_t)h->ntubes * CONV_TABLES * nqm)) ||
-       (rc = dalloc(h, &h->d_conv_td, (size_t)h->ntubes)) ||
-       (rc = dalloc(h, &h->d_conv_tube, (size_t)h->ntubes)) ||
-       (rc = dalloc(h, &h->d_conv_pnew, (size_t)h->ntubes))))
-    return rc;
-  // the moves, their new descriptors and tables in host staging (kept in
-  // the handle until the next move), one copy each
+  const size_t stage_len = (size_t)h->ntubes * CONV_TABLES * nqm;
+  if (!h->d_conv_stage) {  // staging for every entry moving at once
+    if ((rc = dalloc(h, &h->d_conv_stage, stage_len)) ||
+        (rc = dalloc(h, &h->d_conv_td, (size_t)h->ntubes)) ||
+        (rc = dalloc(h, &h->d_conv_tube, (size_t)h->ntubes)) ||
+        (rc = dalloc(h, &h->d_conv_pnew, (size_t)h->ntubes)))
+      return rc;
+    CK(cudaMallocHost((void **)&h->conv_host.stage, stage_len * sizeof(double)));
+  }
+  // the moves, their new descriptors and tables in host staging (the tables
+  // in pinned memory, copied asynchronously; the staging is next written at
+  // the next move, after the step that applied this one has finished)
   auto &S = h->conv_host;
-  S.stage.assign((size_t)np * CONV_TABLES * nqm, 0.0);
   S.td.resize(np);
   S.tube.resize(np);
   S.pnew.resize(np);
@@ -452,9 +456,9 @@ int apply_pending_tubes(kaos_handle *h) {
     S.pnew[p] = pt.d.pG;
     for (int k = 0; k < CONV_TABLES; ++k)
       std::copy(pt.tables[k].begin(), pt.tables[k].end(),
-                S.stage.begin() + ((size_t)p * CONV_TABLES + k) * nqm);
+                S.stage + ((size_t)p * CONV_TABLES + k) * nqm);
   }
-  CK(cudaMemcpyAsync(h->d_conv_stage, S.stage.data(), S.stage.size() * sizeof(double),
+  CK(cudaMemcpyAsync(h->d_conv_stage, S.stage, (size_t)np * CONV_TABLES * nqm * sizeof(double),
                      cudaMemcpyHostToDevice, h->s));
   CK(cudaMemcpyAsync(h->d_conv_td, S.td.data(), np * sizeof(TubeD), cudaMemcpyHostToDevice, h->s));
   CK(cudaMemcpyAsync(h->d_conv_tube, S.tube.data(), np * sizeof(int), cudaMemcpyHostToDevice, h->s));
@@ -1909,6 +1913,7 @@ void kaos_destroy(kaos_handle *h) {
   for (void *p : h->allocs) cudaFree(p);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
+  if (h->conv_host.stage) cudaFreeHost(h->conv_host.stage);
   if (h->efork) cudaEventDestroy(h->efork);
   if (h->ejoin) cudaEventDestroy(h->ejoin);
   if (h->s2) cudaStreamDestroy(h->s2);
