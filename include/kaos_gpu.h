@@ -182,7 +182,9 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
 /* Load the initial particles of one tube: the initial-condition arrays
  * x0T..Vz0T, Vperp10T, Vperp20T of FluxTubeT (_7_InitialConditions.f90:
  * 51-98).  Positions are field-line q values (p = pG is implied);
- * velocities are field-aligned components. */
+ * velocities are field-aligned components.  The arrays are staged through
+ * the library's spare particle buffers (no device allocation); pinned host
+ * arrays copy fastest. */
 int kaos_load_particles(kaos_handle *h, int32_t tube, const double *q,
                         const double *vpar, const double *vperp1,
                         const double *vperp2, int64_t n);
@@ -261,7 +263,9 @@ int kaos_set_export(kaos_handle *h, int32_t on);
 /* Copy the ion state of a tube to host arrays of length n (n must equal the
  * live ion count): field-line q, parallel velocity, Vperp1, Vperp2 and the
  * start-of-step cell index Qindk1 (0-based, -1/-2 escape sentinels).  Any
- * pointer may be NULL.  Order is the reference particle order. */
+ * pointer may be NULL.  Order is the reference particle order.  The state
+ * is gathered on the device into the spare particle buffers (no device
+ * allocation) and copied once per array. */
 int kaos_get_particles(kaos_handle *h, int32_t tube, double *q, double *vpar,
                        double *vperp1, double *vperp2, int32_t *qind,
                        int64_t n);
