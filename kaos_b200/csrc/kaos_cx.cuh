@@ -226,6 +226,8 @@ __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) 
       q = a.ion.qind[T.off + i];
       if (q < 0 || need[q] == 0) q = -1;
     }
+    // most tiles hold no candidate: one barrier and on to the next tile
+    if (!__syncthreads_or(q >= 0)) continue;
     // rank among same-cell candidates of this tile, in index order
     const unsigned peers = __match_any_sync(0xffffffffu, q);
     const int wr = __popc(peers & ((1u << l) - 1u));
