@@ -37,6 +37,22 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s, mixed-prec vs FP64 on 1 B200, at stated moment error"
 N_PART = 10_000_000
 
+# F_alg: FP64 flop-equivalents of one ion push-step of the reference
+# formulation on this tube, counted by the op-counting build of the oracle
+# (add 176, mul 554, div 158, sqrt 22, transcendental calls 41; weights
+# add/mul 1, div/sqrt 4, transcendental 20).
+F_ALG = 2270
+FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64, nominal; no FP64 figure is measured
+
+
+def fp64_pipe_roofline(rate_per_gpu):
+    """The FP64 path against the FP64 pipe: ion-steps/s x F_alg."""
+    achieved = rate_per_gpu * F_ALG / 1e12
+    return {"bound": "fp64", "achieved": achieved, "peak": FP64_NOMINAL_TFLOPS,
+            "unit": "TFLOP/s (flop-equivalents)", "frac": achieved / FP64_NOMINAL_TFLOPS,
+            "peak_kind": "nominal", "f_alg": F_ALG,
+            "weights": "add/mul 1, div/sqrt 4, transcendental call 20"}
+
 
 def clocks_sampler(stop, out):
     """nvidia-smi clocks during the timed region (one sample per 200 ms)."""
@@ -599,6 +615,7 @@ def main():
                 "value": r64["value"] * world, "ms_per_step": r64["ms"] / args.steps,
                 "push_ms": r64["push_ms"]},
             "mixed_over_fp64": value / (r64["value"] * world) if full else None,
+            "fp64_roofline": fp64_pipe_roofline(r64["value"]) if full else None,
             "mixed_push_ms": r32["push_ms"],
             "large": large,
             "batched": batched,

@@ -21,7 +21,9 @@
  *
  * Build: oracle/Makefile (gcc -O2 -ffp-contract=off -fno-fast-math).
  */
+#ifndef ORC_OPS_COUNTED
 #include <complex.h>
+#endif
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -31,8 +33,27 @@
 #include "../include/kaos_gpu.h"
 #include "../include/kaos_philox.h"
 
+/* Hooks of the op-counting build (oracle/op_count.cpp, which includes this
+ * file with `double` replaced by a counting type).  In this plain C build
+ * they do nothing and the complex arithmetic is C99's. */
+#ifndef ORC_OPS_COUNTED
+typedef double complex orc_cplx;
+#define ORC_I I
+#define orc_cacos cacos
+#define orc_ccos ccos
+#define orc_creal creal
+#define ORC_PHASE(ph) ((void)0)
+#define ORC_SEARCH_BEGIN() ((void)0)
+#define ORC_SEARCH_END() ((void)0)
+#endif
+/* op-counting phases of one step */
+#define ORC_PH_PUSH_ION 0
+#define ORC_PH_PUSH_ENA 1
+#define ORC_PH_CX 2
+#define ORC_PH_MASTER 3
+
 /* ---- _ModelInput.f90:35-43 physical constants ---------------------------- */
-static const double PI = 3.14159265358979323846;
+#define PI 3.14159265358979323846 /* a parameter: folded into constants */
 #define KB 138e-25
 #define EPS0 8.854e-12
 #define MDIP 8.06e15
@@ -103,6 +124,7 @@ static double orient(const orc *o) { return o->qGL[0] <= 0.0 ? 1.0 : -1.0; }
 /* Cell search, KineticUpdateA _8_1_1_KineticUpdateA.f90:221-273: first cell
  * is [lo,hi], later cells (lo,hi]; 0 below LB, -1 above UB (1-based).  */
 static int64_t cell_search(const orc *o, double q) {
+  ORC_SEARCH_BEGIN(); /* the orientation products stand for branches */
   double s = orient(o);
   double sq_ = s * q;
   int64_t idx = -9; /* "unset": the reference leaves Qindk1 unchanged */
@@ -122,6 +144,7 @@ static int64_t cell_search(const orc *o, double q) {
     idx = 0;
   else if (s * o->qGH[o->nq - 1] < sq_)
     idx = -1;
+  ORC_SEARCH_END();
   return idx;
 }
 
@@ -158,11 +181,11 @@ static void quartic(double qN, double pN, double phiN, double *r, double *th,
   double Bbb = 2.0 * (Ab * Ab * Ab) / 27.0 - Ab * Bb / 3.0 + Cb;
   double Delta = -Bbb / 2.0;
   double Eps = Abb / 3.0;
-  double complex I1 = I;
-  double complex Thetap = cacos(Delta / (I1 * sqrt(Eps * Eps * Eps)));
-  double complex s23 =
-      2.0 * I1 * sqrt(Eps) * ccos((Thetap + 4.0 * PI) / 3.0) - Ab / 3.0;
-  double sigma = fabs(creal(s23));
+  orc_cplx I1 = ORC_I;
+  orc_cplx Thetap = orc_cacos(Delta / (I1 * sqrt(Eps * Eps * Eps)));
+  orc_cplx s23 =
+      2.0 * I1 * sqrt(Eps) * orc_ccos((Thetap + 4.0 * PI) / 3.0) - Ab / 3.0;
+  double sigma = fabs(orc_creal(s23));
   double mu = sqrt((Ap * Ap) / 4.0 - Bp + sigma);
   double pii;
   if (mu != 0.0)
@@ -618,31 +641,34 @@ static void gravfield(orc *o) {
  * (_8_7_AmbipolarEfield.f90:1453-2722, _8_7_2_Gravfield.f90:132-...).
  * Returns 0 if q lies outside the grid (value unchanged). */
 static int interp_field(const orc *o, const double *E, double q, double *out) {
+  ORC_SEARCH_BEGIN(); /* the orientation products stand for branches */
   double s = orient(o);
   double sq_ = s * q;
   int nq = o->nq;
-  for (int Q = 0; Q < nq; ++Q) {
+  int found = 0, lerp = 0, at = 0;
+  for (int Q = 0; Q < nq && !found; ++Q) {
     double cQ = s * o->qGC[Q];
     if (Q == 0 && s * o->qGL[0] <= sq_ && sq_ <= cQ) {
-      *out = E[0];
-      return 1;
-    }
-    if (Q != 0 && Q != nq - 1 && s * o->qGC[Q - 1] < sq_ && sq_ <= cQ) {
-      *out = lin_interp(q, E[Q - 1], E[Q], o->qGC[Q - 1], o->qGC[Q]);
-      return 1;
-    }
-    if (Q == nq - 1) {
+      found = 1;
+      at = 0;
+    } else if (Q != 0 && Q != nq - 1 && s * o->qGC[Q - 1] < sq_ && sq_ <= cQ) {
+      found = lerp = 1;
+      at = Q;
+    } else if (Q == nq - 1) {
       if (s * o->qGC[Q - 1] < sq_ && sq_ < cQ) {
-        *out = lin_interp(q, E[Q - 1], E[Q], o->qGC[Q - 1], o->qGC[Q]);
-        return 1;
-      }
-      if (cQ <= sq_ && sq_ <= s * o->qGH[Q]) {
-        *out = E[Q];
-        return 1;
+        found = lerp = 1;
+        at = Q;
+      } else if (cQ <= sq_ && sq_ <= s * o->qGH[Q]) {
+        found = 1;
+        at = Q;
       }
     }
   }
-  return 0;
+  ORC_SEARCH_END();
+  if (found)
+    *out = lerp ? lin_interp(q, E[at - 1], E[at], o->qGC[at - 1], o->qGC[at])
+                : E[at];
+  return found;
 }
 
 static void interpolate_particles(orc *o, int use_q0, const double *q0) {
@@ -1267,6 +1293,7 @@ static void step_once(orc *o) {
   const kaos_params_c *P = &o->P;
   int64_t n = o->n + 1;
   o->n = n; /* RNG step key = n */
+  ORC_PHASE(ORC_PH_MASTER);
   if (n == 1) {
     /* KineticSolverASub _8_0_0_1_KineticSolverA.f90:43-404: counts and
      * moments from the initial indices, fields, then push from x0. */
@@ -1289,10 +1316,12 @@ static void step_once(orc *o) {
     memcpy(o->mom[KAOS_EAMAG], o->EAmag, sizeof(double) * (size_t)o->nq);
     memcpy(o->mom[KAOS_EGMAG], o->EG, sizeof(double) * (size_t)o->nq);
     for (int64_t j = 0; j < o->np; ++j) {
+      ORC_PHASE(ORC_PH_PUSH_ION);
       o->AEA[j] = o->AEAN[j];
       o->AG[j] = o->AGN[j];
       push_particle(o, j);
     }
+    ORC_PHASE(ORC_PH_MASTER);
     return;
   }
   int master = is_master(o, n);
@@ -1306,8 +1335,10 @@ static void step_once(orc *o) {
     for (int Q = 0; Q < o->nq; ++Q)
       if (o->Te[Q] + P->dNTe <= P->dNTeEND)
         o->Te[Q] = o->Te[Q] + P->dNTe;
+  ORC_PHASE(ORC_PH_CX);
   if (P->QEXCHANGEflag == 1)
     charge_exchange(o);
+  ORC_PHASE(ORC_PH_MASTER);
   int64_t nexist = o->np;
   if (master) {
     o->lb_out = o->ub_out = o->lb_in = o->ub_in = 0;
@@ -1319,12 +1350,14 @@ static void step_once(orc *o) {
     interpolate_particles(o, 0, NULL);
   }
   for (int64_t j = 0; j < nexist; ++j) {
+    ORC_PHASE(o->ena[j] ? ORC_PH_PUSH_ENA : ORC_PH_PUSH_ION);
     if (!o->ena[j]) {
       o->AEA[j] = o->AEAN[j];
       o->AG[j] = o->AGN[j];
     }
     push_particle(o, j);
   }
+  ORC_PHASE(ORC_PH_MASTER);
   if (master) {
     if (P->LBCONDITIONflag == 1)
       inject(o, 0);
