@@ -272,6 +272,24 @@ module kaos_gpu_iface
       type(c_ptr), value :: h
     end subroutine kaos_destroy
 
+    ! statistics without device allocation: every array but p and vg is a
+    ! device pointer (c_ptr from the host's own device allocator);
+    ! d_moments holds [11][nq] doubles, d_counts nq int64 or c_null_ptr
+    integer(c_int) function kaos_moments_noalloc(p, vg, nq, d_qedges, d_d3x, &
+        nsnormfac, d_q, d_vpar, d_vperp1, d_vperp2, n, d_moments, d_counts, &
+        stream) bind(C, name="kaos_moments_noalloc")
+      import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr, kaos_params_t, &
+                kaos_vgrid_t
+      type(kaos_params_t), intent(in) :: p
+      type(kaos_vgrid_t), intent(in) :: vg
+      integer(c_int32_t), value :: nq
+      type(c_ptr), value :: d_qedges, d_d3x
+      real(c_double), value :: nsnormfac
+      type(c_ptr), value :: d_q, d_vpar, d_vperp1, d_vperp2
+      integer(c_int64_t), value :: n
+      type(c_ptr), value :: d_moments, d_counts, stream
+    end function kaos_moments_noalloc
+
     type(c_ptr) function kaos_version() bind(C, name="kaos_version")
       import :: c_ptr
     end function kaos_version

@@ -34,6 +34,13 @@ def test_python_export_list_matches_header():
     assert sorted(klib.EXPORTS) == declared_symbols()
 
 
+def test_fortran_module_binds_every_symbol():
+    """The bind(C) module a Fortran host uses names every entry point."""
+    src = open(os.path.join(ROOT, "kaos_b200", "fortran", "kaos_gpu_iface.f90")).read()
+    bound = sorted(set(re.findall(r'bind\(C,\s*name\s*=\s*"(kaos_[a-z_0-9]+)"', src)))
+    assert bound == declared_symbols()
+
+
 def test_version_and_null_handle(lib):
     assert b"sm_100a" in lib.kaos_version()
     assert lib.kaos_last_error(None) == b"null handle"
