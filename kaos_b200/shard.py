@@ -96,3 +96,21 @@ def nccl_reduce_hook(group=None):
         return 0
 
     return hook
+
+
+def host_reduce_hook(group=None):
+    """The same hook contract over HOST memory (a CPU process group such as
+    gloo): in-place sum of `count` 32-bit counters at host address `buf`
+    over the group.  For ranks that hold their accumulators on the host."""
+    import ctypes
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    def hook(buf: int, count: int, stream: int) -> int:
+        a = np.ctypeslib.as_array((ctypes.c_int32 * int(count)).from_address(int(buf)))
+        dist.all_reduce(torch.from_numpy(a), op=dist.ReduceOp.SUM, group=group)
+        return 0
+
+    return hook

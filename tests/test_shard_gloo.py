@@ -58,6 +58,51 @@ def _worker(rank, world, port, counts, q):
         dist.destroy_process_group()
 
 
+def _hook_worker(rank, world, port, q):
+    """One rank of a split tube: its accumulator block (uint32 counters in
+    host memory) is summed over the ranks in place through the hook
+    contract the library calls (fn(buf_ptr, count, stream_ptr) -> 0)."""
+    import ctypes
+
+    import torch.distributed as dist
+    from kaos_b200.lib import REDUCE_FN
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        n = 1 + 3 * 4099                     # ncell x (1 + n|| + n1 + n2) counters
+        buf = (ctypes.c_uint32 * n)()
+        for i in range(n):
+            buf[i] = (i * 7 + rank * 1000003) % 65536
+        hook = shard.host_reduce_hook()
+        cb = REDUCE_FN(lambda ctx, p, count, stream: int(hook(p, count, stream)))
+        rc = cb(None, ctypes.addressof(buf), n, None)
+        q.put((rank, rc, list(buf)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_split_tube_hook_sums_accumulators_in_place():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_hook_worker, args=(r, world, port, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=240) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    n = len(res[0][2])
+    want = [sum((i * 7 + r * 1000003) % 65536 for r in range(world)) for i in range(n)]
+    for rank, rc, got in res:
+        assert rc == 0
+        assert got == want
+
+
 def test_assign_tubes_balances_and_covers():
     counts = [10, 200, 30, 150, 90, 5]
     a = shard.assign_tubes(counts, 3)
