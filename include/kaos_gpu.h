@@ -284,6 +284,12 @@ int kaos_get_enas(kaos_handle *h, int32_t tube, double *x, double *y,
 int kaos_get_boundary(kaos_handle *h, int32_t tube, int64_t *lb_out,
                       int64_t *ub_out, int64_t *lb_in, int64_t *ub_in);
 
+/* ENAs that left the tube at the latest master step through the lower and
+ * the upper boundary (Qindk1 = 0 / -1; NqReNormLB/UBoutfluxENAT,
+ * _8_0_7_BoundaryConditions.f90:305-416).  Zero without charge exchange. */
+int kaos_get_boundary_ena(kaos_handle *h, int32_t tube, int64_t *lb_out,
+                          int64_t *ub_out);
+
 /* Device time (ms) of the last kaos_step call, measured with CUDA events on
  * the handle's stream, and the number of kernels it launched. */
 int kaos_get_timing(kaos_handle *h, double *ms, int64_t *launches);

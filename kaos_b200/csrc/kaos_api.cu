@@ -1889,6 +1889,20 @@ int kaos_get_boundary(kaos_handle *h, int32_t tube, int64_t *lb_out,
   return KAOS_OK;
 }
 
+int kaos_get_boundary_ena(kaos_handle *h, int32_t tube, int64_t *lb_out,
+                          int64_t *ub_out) {
+  if (!h || tube < 0 || tube >= h->ntubes) return KAOS_ERR_PARAM;
+  unsigned long long v[2] = {0, 0};
+  if (h->d_lbe_out) {
+    CK(cudaStreamSynchronize(h->s));
+    CK(cudaMemcpy(&v[0], h->d_lbe_out + tube, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&v[1], h->d_ube_out + tube, 8, cudaMemcpyDeviceToHost));
+  }
+  if (lb_out) *lb_out = (int64_t)v[0];
+  if (ub_out) *ub_out = (int64_t)v[1];
+  return KAOS_OK;
+}
+
 int kaos_get_timing(kaos_handle *h, double *ms, int64_t *launches) {
   if (!h) return KAOS_ERR_PARAM;
   if (ms) *ms = h->last_ms;

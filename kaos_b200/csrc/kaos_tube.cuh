@@ -679,6 +679,10 @@ __global__ void k_inject(InjArgs a) {
       a.ion.aea[j] = aea;
       a.ion.ag[j] = ag;
       a.ion.qk4[j] = qc;
+      if (a.ion.rho4) {  // k4 point before the first push: where it stands
+        a.ion.rho4[j] = rho0;
+        a.ion.z4[j] = z0;
+      }
     }
     a.ion.qind[j] = Q;
     a.ion.id[j] = id;
@@ -758,6 +762,12 @@ __device__ __forceinline__ void store_ion(const Ions &I, const TubeD &T,
     I.v1[k] = v1;
     I.v2[k] = v2;
     I.qk4[k] = q;
+    // the k4 point of an ion not yet pushed is where it stands (charge
+    // exchange may convert an injected ion before its first push)
+    if (I.rho4) {
+      I.rho4[k] = rho;
+      I.z4[k] = z;
+    }
   }
 }
 

@@ -187,6 +187,14 @@ module kaos_gpu_iface
       integer(c_int64_t), intent(out) :: lb_out, ub_out, lb_in, ub_in
     end function kaos_get_boundary
 
+    integer(c_int) function kaos_get_boundary_ena(h, tube, lb_out, ub_out) &
+        bind(C, name="kaos_get_boundary_ena")
+      import :: c_int, c_int32_t, c_int64_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: tube
+      integer(c_int64_t), intent(out) :: lb_out, ub_out
+    end function kaos_get_boundary_ena
+
     integer(c_int) function kaos_get_timing(h, ms, launches) &
         bind(C, name="kaos_get_timing")
       import :: c_int, c_int64_t, c_double, c_ptr

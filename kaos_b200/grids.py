@@ -328,15 +328,18 @@ def config_c5(ntubes=64, n_ions=20_000_000, precision=KAOS_PREC_MIXED,
 CONV_C5_DL = 500.0 * 50 * 0.005 / RE
 
 
-def config_escaping():
+def config_escaping(neut_n0=0.0):
     """A short hot tube (L=3, 24 cells up to |q| = 0.5, 5 eV O+, dt 1 s,
     master step every 2 steps) that loses ~40 ions per master step through
     both boundaries, with 30 injected at the lower one: the removal and
-    injection test case."""
-    mi = ModelInput(h=1.0, ndatfac=2, ION2VPERPflag=1)
+    injection test case.  neut_n0 > 0 adds charge exchange with neutrals of
+    that base density (scale height 300 km), whose ENAs leave through both
+    boundaries too."""
+    mi = ModelInput(h=1.0, ndatfac=2, ION2VPERPflag=1,
+                    QEXCHANGEflag=1 if neut_n0 > 0 else 0)
     vg = make_vgrid(True, 16, 16, 24, 3e4)
     spec = TubeSpec(L=3.0, nq=24, n_particles=2500, q_ub=0.5, H=400e3,
-                    Ti=5.0 * 1.602e-19 / KB)
+                    Ti=5.0 * 1.602e-19 / KB, neut_n0=neut_n0, neut_H=300e3)
     tube = make_tube(spec, mi)
     tube.nsnormCLB = 30.0
     return mi, spec, tube, vg

@@ -24,7 +24,8 @@ EXPORTS = [
     "kaos_create", "kaos_load_particles", "kaos_set_fields", "kaos_step",
     "kaos_get_step", "kaos_get_count", "kaos_get_moments", "kaos_get_counts",
     "kaos_set_export", "kaos_get_particles", "kaos_get_positions",
-    "kaos_get_enas", "kaos_get_boundary", "kaos_get_timing", "kaos_set_graph",
+    "kaos_get_enas", "kaos_get_boundary", "kaos_get_boundary_ena", "kaos_get_timing",
+    "kaos_set_graph",
     "kaos_set_launch", "kaos_last_error", "kaos_get_status", "kaos_destroy",
     "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
     "kaos_get_launch", "kaos_set_ena_grid", "kaos_init_particles",
@@ -65,6 +66,7 @@ def load(path: str = LIBPATH):
     L.kaos_get_positions.argtypes = [vp, i32, vp, vp, i64]
     L.kaos_get_enas.argtypes = [vp, i32] + [vp] * 6 + [i64]
     L.kaos_get_boundary.argtypes = [vp, i32] + [C.POINTER(i64)] * 4
+    L.kaos_get_boundary_ena.argtypes = [vp, i32] + [C.POINTER(i64)] * 2
     L.kaos_get_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
     L.kaos_get_push_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
     L.kaos_moments_noalloc.argtypes = [vp, vp, i32, vp, vp, C.c_double, vp, vp,
@@ -214,6 +216,12 @@ class Solver:
     def boundary(self, tube=0):
         v = [C.c_int64() for _ in range(4)]
         self._check(load().kaos_get_boundary(self.h, tube, *[C.byref(x) for x in v]))
+        return np.array([x.value for x in v])
+
+    def boundary_ena(self, tube=0):
+        """Escaped LB/UB ENA counts of the latest master step."""
+        v = [C.c_int64() for _ in range(2)]
+        self._check(load().kaos_get_boundary_ena(self.h, tube, *[C.byref(x) for x in v]))
         return np.array([x.value for x in v])
 
     def timing(self):

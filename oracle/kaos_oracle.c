@@ -92,6 +92,7 @@ typedef struct orc {
   double *EAimport;
   int64_t n; /* computational steps taken */
   int64_t lb_out, ub_out, lb_in, ub_in;
+  int64_t lbe_out, ube_out; /* escaped ENAs of the latest master step */
   kaos_tube_c *pending; /* orc_update_tube: applied at the next master step */
   double GAconv;        /* gyro-angle carried between ions as in the reference */
   char err[256];
@@ -1027,7 +1028,14 @@ static void place_ion(orc *o, int64_t j, double q, double vpar, double v1,
   o->V2[j] = v2;
   o->Vp[j] = fabs(sqrt(v1 * v1 + v2 * v2));
   o->ena[j] = 0;
+  /* the k4 point of an ion not yet pushed is where it stands: charge
+   * exchange may convert an injected ion before its first push (the
+   * reference leaves the k4 arrays of reallocated slots unset) */
   o->qk4[j] = q;
+  o->rk4[j] = r;
+  o->thk4[j] = th;
+  o->phk4[j] = o->phiG;
+  o->ellk4[j] = ell;
   o->Qind[j] = cell_search(o, q);
   int d3 = o->P.ION2VPERPflag == 1;
   o->ipar[j] = vbin(o->epar, o->npar, vpar, d3, 0);
@@ -1088,7 +1096,7 @@ static void inject(orc *o, int ub) {
 /* BoundaryConditionsSub escape masks + BCReIndexSub order-preserving pack
  * (_8_0_7_BoundaryConditions.f90:158-503, _8_0_7_1_BCReIndex.f90:33-241). */
 static void boundary(orc *o) {
-  int64_t w = 0, lb = 0, ub = 0;
+  int64_t w = 0, lb = 0, ub = 0, lbe = 0, ube = 0;
   for (int64_t j = 0; j < o->np; ++j) {
     int esc = (o->Qind[j] == 0 || o->Qind[j] == -1);
     if (esc && !o->ena[j]) {
@@ -1096,6 +1104,12 @@ static void boundary(orc *o) {
         lb++;
       else
         ub++;
+    }
+    if (esc && o->ena[j]) { /* ENA escape counts :305-416 */
+      if (o->Qind[j] == 0)
+        lbe++;
+      else
+        ube++;
     }
     if (!esc) {
       if (w != j)
@@ -1106,6 +1120,8 @@ static void boundary(orc *o) {
   o->np = w;
   o->lb_out = lb;
   o->ub_out = ub;
+  o->lbe_out = lbe;
+  o->ube_out = ube;
 }
 
 /* charge exchange on step n (_8_KineticSolver.f90:95-166,
@@ -1700,6 +1716,11 @@ void orc_get_boundary(orc *o, int64_t *v) {
   v[1] = o->ub_out;
   v[2] = o->lb_in;
   v[3] = o->ub_in;
+}
+
+void orc_get_boundary_ena(orc *o, int64_t *v) {
+  v[0] = o->lbe_out;
+  v[1] = o->ube_out;
 }
 
 /* single quartic evaluation for known-answer tests */

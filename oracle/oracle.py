@@ -64,6 +64,7 @@ def _open(path):
     L.orc_get_particles.argtypes = [vp] + [vp] * 7
     L.orc_get_enas.argtypes = [vp] + [vp] * 6
     L.orc_get_boundary.argtypes = [vp, vp]
+    L.orc_get_boundary_ena.argtypes = [vp, vp]
     L.orc_quartic.argtypes = [C.c_double, C.c_double, C.c_double, vp]
     L.orc_filter.argtypes = [vp, vp, C.c_int, C.c_int]
     L.orc_destroy.argtypes = [vp]
@@ -179,6 +180,12 @@ class Oracle:
     def boundary(self):
         v = np.zeros(4, dtype=np.int64)
         self._L.orc_get_boundary(self.h, _p(v))
+        return v
+
+    def boundary_ena(self):
+        """Escaped LB/UB ENA counts of the latest master step."""
+        v = np.zeros(2, dtype=np.int64)
+        self._L.orc_get_boundary_ena(self.h, _p(v))
         return v
 
 

@@ -354,6 +354,33 @@ def test_convection_to_new_lshell(mixed):
         assert rel_norm(s.moments(m), o.moments(m)) < MOM_TOL, m
 
 
+def test_ena_escapes_per_master_step():
+    """Escaped LB/UB ENA counts of every master step (kaos_get_boundary_ena)
+    equal the oracle's, with ions and ENAs leaving through both ends."""
+    mi, spec, tube, vg = grids.config_escaping(neut_n0=3e16)
+    tube.nsnormCLB = 30.0
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=3)
+    o = Oracle(mi, tube, vg)
+    o.load(q, vpar, v1, v2)
+    s = Solver(mi, [tube], vg)
+    s.load(0, q, vpar, v1, v2)
+    o.step(1)
+    s.step(1)
+    tot = np.zeros(2, dtype=np.int64)
+    for _ in range(10):
+        o.step(2)
+        s.step(2)
+        np.testing.assert_array_equal(s.boundary(), o.boundary())
+        be = o.boundary_ena()
+        np.testing.assert_array_equal(s.boundary_ena(), be)
+        assert s.count() == o.count()
+        tot += be
+    assert tot[0] > 20 and tot[1] > 20
+    po, ps = o.particles(), s.particles()
+    for k in ("z", "vpar", "vperp1", "vperp2"):
+        assert rel_norm(ps[k], po[k]) < TRAJ_TOL, k
+
+
 def test_fp64_charge_exchange_across_packing():
     """Charge exchange every step over ten master steps (slots converted to
     ENAs and escaped ions both marked dead, the arrays packed at the eighth

@@ -154,6 +154,31 @@ def test_particle_number_conservation_and_F_d3v():
     np.testing.assert_allclose(NqRT, cnt * tube.nsnormfac / tube.d3xC, rtol=1e-15)
 
 
+def test_ena_bookkeeping_at_master_steps():
+    """Every master step: ENAs after = ENAs before + ions converted - ENAs
+    escaped (BoundaryConditionsSub's ENA masks, :305-416), where the ions
+    converted = ions before - ions after - ions escaped + ions injected;
+    ENAs leave through both boundaries."""
+    mi, spec, tube, vg = grids.config_escaping(neut_n0=3e16)
+    tube.nsnormCLB = 30.0
+    o = Oracle(mi, tube, vg)
+    o.load(*grids.initial_particles(tube, spec, mi, seed=3))
+    o.step(1)
+    lbe = ube = 0
+    for _ in range(10):
+        ni1, ne1 = o.count()
+        o.step(1)                      # a master step (every second step)
+        ni2, ne2 = o.count()
+        lb, ub, lbi, ubi = o.boundary()
+        el, eu = o.boundary_ena()
+        conv = ni1 - ni2 - lb - ub + lbi + ubi
+        assert conv >= 0
+        assert ne2 == ne1 + conv - el - eu
+        lbe, ube = lbe + el, ube + eu
+        o.step(1)
+    assert lbe > 20 and ube > 20
+
+
 def test_moments_of_drifting_maxwellian():
     """Bin-centre moments of a drifting Maxwellian approach the analytic
     drift and temperature (first-step statistics, before any push)."""
