@@ -28,6 +28,45 @@ def _w(path: str, arr, dtype) -> None:
         f.write(np.asfortranarray(a).tobytes(order="F"))
 
 
+def moment_filter(x, pt: int) -> np.ndarray:
+    """MomentFilterSub (_8_7_1_MomentFilter.f90:25-147) on the host: the
+    mean of the H = nint((pt-1)/2) cells above (with the cell itself) and
+    of the H below, averaged; one-sided near the ends.  Sums run in the
+    reference's order, so the result is the library's bit for bit."""
+    a = [float(v) for v in np.asarray(x, dtype=np.float64)]
+    nq = len(a)
+    H = int(np.floor((pt - 1) / 2.0 + 0.5))
+    lb, ub = 0, nq - 1
+    out = np.zeros(nq)
+
+    def run(start, step, count):   # a[start] + a[start+step] + ... in order
+        s = a[start]
+        for k in range(1, count):
+            s += a[start + k * step]
+        return s
+
+    for q in range(nq):
+        if q <= lb - 1 + H:
+            a1 = run(q, 1, H + 1) / (H + 1)
+            if q == lb:
+                out[q] = a1
+            elif q == lb + 1:
+                out[q] = (a1 + a[lb]) / 2.0
+            else:
+                out[q] = (a1 + run(q - 1, -1, q - lb) / (q - lb)) / 2.0
+        if lb - 1 + H < q < ub - H:
+            out[q] = (run(q, 1, H + 1) / (H + 1) + run(q - 1, -1, H) / H) / 2.0
+        if q >= ub - H:
+            a2 = run(q, -1, H + 1) / (H + 1)
+            if q == ub:
+                out[q] = a2
+            elif q == ub - 1:
+                out[q] = (a[ub] + a2) / 2.0
+            else:
+                out[q] = (run(q + 1, 1, ub - q) / (ub - q) + a2) / 2.0
+    return out
+
+
 def file_name(nn: int, s: int, f: int, name: str, qind: Optional[int] = None) -> str:
     if qind is None:
         return f"{nn}_{s}_{f}_{name}fort.bin"
@@ -37,14 +76,18 @@ def file_name(nn: int, s: int, f: int, name: str, qind: Optional[int] = None) ->
 def write_master_step(outdir: str, nn: int, solver, tube_index: int, tube,
                       vgrid, three_d: bool, time_s: float, ndatfac: int,
                       s: int = 1, f: int = 1, hist: Optional[np.ndarray] = None,
-                      Te: Optional[np.ndarray] = None) -> Dict[str, str]:
+                      Te: Optional[np.ndarray] = None, mi=None) -> Dict[str, str]:
     """Write the DataExport2 files of master step `nn` for one tube from a
     `kaos_b200.lib.Solver` (or anything with .moments(which, tube)).
     `hist` is the full count histogram of the step ([nq][...] as returned by
     counts(full=True)); when given, N2PerpphRT (3D) or NphRT (2D) and d3vCTp
     are written per cell, in density units (count * nsnormfac / d3x) as
     IonParticleCountsSub stores them (_8_3_1_IonParticleCounts.f90:440-451).
-    Returns {name: path}."""
+    With `mi` (the run's ModelInput) and MOMENTFILTERflag = 1, the filtered
+    first and parallel second moments the collision model reads
+    (_8_6_6_1_IonNeutralCollisionFrequencyA.f90:42-95) are written too
+    (M1ParFiltAvrgRT, M1Perp1/2FiltAvrgRT, M2ParFiltAvrgRT,
+    _8_0_2_DataExport2.f90:359-410).  Returns {name: path}."""
     os.makedirs(outdir, exist_ok=True)
     out: Dict[str, str] = {}
     nq = tube.nq
@@ -72,6 +115,12 @@ def write_master_step(outdir: str, nn: int, solver, tube_index: int, tube,
         put("M1PerpphRT", m(KAOS_M1PERP))
     put("M1ParphRT", m(KAOS_M1PAR))
     put("M0FiltAvrgRT", m(KAOS_M0FILT))
+    if mi is not None and mi.MOMENTFILTERflag == 1:
+        if three_d:
+            put("M1Perp1FiltAvrgRT", moment_filter(m(KAOS_M1PERP1), mi.M1Perp1MAfilterPt))
+            put("M1Perp2FiltAvrgRT", moment_filter(m(KAOS_M1PERP2), mi.M1Perp2MAfilterPt))
+        put("M1ParFiltAvrgRT", moment_filter(m(KAOS_M1PAR), mi.M1ParMAfilterPt))
+        put("M2ParFiltAvrgRT", moment_filter(m(KAOS_M2PAR), mi.M2ParMAfilterPt))
     put("nuIonNeutRT", m(KAOS_NUPOI))
     put("M2phRT", m(KAOS_M2))
     if three_d:
