@@ -67,6 +67,20 @@ def moment_filter(x, pt: int) -> np.ndarray:
     return out
 
 
+def sigma_ion_neutral(M0, M2par) -> np.ndarray:
+    """Lindsay-Stebbings charge-exchange factor per cell,
+    (4.07 - 0.269 ln E)^2 (1 - exp(-415/E))^0.8 with E = M2par in keV
+    (sigmaIonNeutRT, _8_6_6_1_IonNeutralCollisionFrequencyA.f90:104-127;
+    the cross-section is this times 1e-16 cm^2); 0 where M0 or M2par is 0."""
+    import math
+    out = np.zeros(len(M0))
+    for q, (m0, m2) in enumerate(zip(np.asarray(M0, float), np.asarray(M2par, float))):
+        if m0 != 0.0 and m2 != 0.0:
+            e = (6.242e18) * (1e-3) * float(m2)
+            out[q] = (4.07 - 0.269 * math.log(e)) ** 2 * (1.0 - math.exp(-415.0 / e)) ** 0.8
+    return out
+
+
 def file_name(nn: int, s: int, f: int, name: str, qind: Optional[int] = None) -> str:
     if qind is None:
         return f"{nn}_{s}_{f}_{name}fort.bin"
@@ -87,7 +101,8 @@ def write_master_step(outdir: str, nn: int, solver, tube_index: int, tube,
     first and parallel second moments the collision model reads
     (_8_6_6_1_IonNeutralCollisionFrequencyA.f90:42-95) are written too
     (M1ParFiltAvrgRT, M1Perp1/2FiltAvrgRT, M2ParFiltAvrgRT,
-    _8_0_2_DataExport2.f90:359-410).  Returns {name: path}."""
+    _8_0_2_DataExport2.f90:359-410), and with QEXCHANGEflag = 1 the
+    charge-exchange factor sigmaIonNeutRT (:416-430).  Returns {name: path}."""
     os.makedirs(outdir, exist_ok=True)
     out: Dict[str, str] = {}
     nq = tube.nq
@@ -121,6 +136,10 @@ def write_master_step(outdir: str, nn: int, solver, tube_index: int, tube,
             put("M1Perp2FiltAvrgRT", moment_filter(m(KAOS_M1PERP2), mi.M1Perp2MAfilterPt))
         put("M1ParFiltAvrgRT", moment_filter(m(KAOS_M1PAR), mi.M1ParMAfilterPt))
         put("M2ParFiltAvrgRT", moment_filter(m(KAOS_M2PAR), mi.M2ParMAfilterPt))
+    if mi is not None and mi.QEXCHANGEflag == 1:
+        m2 = (moment_filter(m(KAOS_M2PAR), mi.M2ParMAfilterPt)
+              if mi.MOMENTFILTERflag == 1 else m(KAOS_M2PAR))
+        put("sigmaIonNeutRT", sigma_ion_neutral(m(KAOS_M0), m2))
     put("nuIonNeutRT", m(KAOS_NUPOI))
     put("M2phRT", m(KAOS_M2))
     if three_d:

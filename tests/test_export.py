@@ -70,3 +70,26 @@ def test_filtered_moment_files(tmp_path):
     # the library's own filtered M0 is the same filter
     np.testing.assert_array_equal(export.moment_filter(o.moments(KAOS_M0), mi.M0MAfilterPt),
                                   o.moments(KAOS_M0FILT))
+
+
+def test_sigma_file_with_charge_exchange(tmp_path):
+    from kaos_b200.model_input import KAOS_M2PAR
+    mi, spec, tube, vg = grids.config_small(n_particles=1500, three_d=True, nq=12,
+                                            collisions=True)
+    o = Oracle(mi, tube, vg)
+    o.load(*grids.initial_particles(tube, spec, mi, seed=4))
+    o.step(1)
+    files = export.write_master_step(str(tmp_path), 1, _OracleAsSolver(o), 0, tube, vg,
+                                     True, 0.0, mi.ndatfac, mi=mi)
+    sig = export.read(files["sigmaIonNeutRT"])
+    m0 = o.moments(KAOS_M0)
+    m2 = export.moment_filter(o.moments(KAOS_M2PAR), mi.M2ParMAfilterPt)
+    assert sig.shape == (tube.nq,)
+    for q in range(tube.nq):
+        if m0[q] == 0.0 or m2[q] == 0.0:
+            assert sig[q] == 0.0
+        else:
+            e = 6.242e18 * 1e-3 * m2[q]    # keV
+            assert sig[q] == pytest.approx((4.07 - 0.269 * np.log(e)) ** 2
+                                           * (1.0 - np.exp(-415.0 / e)) ** 0.8, rel=1e-14)
+    assert np.all(sig[m0 > 0] > 0)
