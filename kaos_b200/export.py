@@ -90,7 +90,8 @@ def file_name(nn: int, s: int, f: int, name: str, qind: Optional[int] = None) ->
 def write_master_step(outdir: str, nn: int, solver, tube_index: int, tube,
                       vgrid, three_d: bool, time_s: float, ndatfac: int,
                       s: int = 1, f: int = 1, hist: Optional[np.ndarray] = None,
-                      Te: Optional[np.ndarray] = None, mi=None) -> Dict[str, str]:
+                      Te: Optional[np.ndarray] = None, mi=None,
+                      ns0: Optional[float] = None) -> Dict[str, str]:
     """Write the DataExport2 files of master step `nn` for one tube from a
     `kaos_b200.lib.Solver` (or anything with .moments(which, tube)).
     `hist` is the full count histogram of the step ([nq][...] as returned by
@@ -102,7 +103,9 @@ def write_master_step(outdir: str, nn: int, solver, tube_index: int, tube,
     (_8_6_6_1_IonNeutralCollisionFrequencyA.f90:42-95) are written too
     (M1ParFiltAvrgRT, M1Perp1/2FiltAvrgRT, M2ParFiltAvrgRT,
     _8_0_2_DataExport2.f90:359-410), and with QEXCHANGEflag = 1 the
-    charge-exchange factor sigmaIonNeutRT (:416-430).  Returns {name: path}."""
+    charge-exchange factor sigmaIonNeutRT (:416-430).  `ns0`, the run's
+    reference ion density at the lower boundary [m^-3], is written as ns0GT
+    (:54-58) when given.  Returns {name: path}."""
     os.makedirs(outdir, exist_ok=True)
     out: Dict[str, str] = {}
     nq = tube.nq
@@ -114,6 +117,8 @@ def write_master_step(outdir: str, nn: int, solver, tube_index: int, tube,
 
     put("TimeT", [time_s])
     put("ndatfacGT", [ndatfac], np.int64)
+    if ns0 is not None:
+        put("ns0GT", [ns0])
     put("qGCGT", tube.qGC)
     put("pGCGT", np.full(nq, tube.pG))
     put("rGCGT", tube.rGC)

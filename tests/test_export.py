@@ -26,7 +26,8 @@ def test_export_layout_roundtrip(tmp_path):
     o.step(1)
     hist = o.counts(full=True)
     files = export.write_master_step(str(tmp_path), 1, _OracleAsSolver(o), 0, tube, vg,
-                                     True, 0.0, mi.ndatfac, hist=hist)
+                                     True, 0.0, mi.ndatfac, hist=hist, ns0=spec.n0)
+    assert export.read(files["ns0GT"])[0] == spec.n0
     assert os.path.basename(files["M0phRT"]) == "1_1_1_M0phRTfort.bin"
     assert os.path.basename(files["3_TeNT"]) == "1_1_1_3_TeNTfort.bin"
     np.testing.assert_array_equal(export.read(files["M0phRT"]), o.moments(KAOS_M0))
