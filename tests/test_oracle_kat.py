@@ -179,6 +179,24 @@ def test_ena_bookkeeping_at_master_steps():
     assert lbe > 20 and ube > 20
 
 
+def test_injected_ions_convert_before_their_first_push():
+    """Dense neutrals at the lower boundary convert ions injected at a
+    master step on the next step, before any push: their k4 point is the
+    injection point, so the ENAs they become are finite."""
+    mi, spec, tube, vg = grids.config_escaping(neut_n0=3e18)
+    tube.nsnormCLB = 30.0
+    o = Oracle(mi, tube, vg)
+    o.load(*grids.initial_particles(tube, spec, mi, seed=3))
+    o.step(2)                      # master step at n = 2 injects 30 ions
+    ni, ne = o.count()
+    o.step(1)                      # charge exchange first, then the push
+    ni2, ne2 = o.count()
+    assert ne2 - ne >= 30 and ni2 < ni
+    e = o.enas()
+    for k in e:
+        assert np.all(np.isfinite(e[k])), k
+
+
 def test_moments_of_drifting_maxwellian():
     """Bin-centre moments of a drifting Maxwellian approach the analytic
     drift and temperature (first-step statistics, before any push)."""
