@@ -38,7 +38,8 @@ extern "C" {
 #define KAOS_ERR_CAPACITY 2 /* particle capacity of a tube exceeded        */
 #define KAOS_ERR_NAN 3      /* non-finite particle state detected          */
 #define KAOS_ERR_CUDA 4     /* CUDA runtime error                          */
-#define KAOS_ERR_TIMEOUT 5  /* bounded device wait gave up                  */
+#define KAOS_ERR_TIMEOUT 5  /* reserved: no kernel here waits on another, */
+                            /* so this build never returns it             */
 #define KAOS_ERR_STATE 6    /* call out of order (e.g. step before load)   */
 
 /* ---- precision modes ---------------------------------------------------- */
@@ -378,8 +379,9 @@ int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode);
 /* Text of the last error on this handle (static storage; never NULL). */
 const char *kaos_last_error(kaos_handle *h);
 
-/* Device status word: nonzero bits report non-finite state (1), capacity
- * overflow (2), bounded-wait timeout (4) seen on the device. */
+/* Device status word: nonzero bits report non-finite state (1) and capacity
+ * overflow (2) seen on the device; bit 4 is reserved for a bounded-wait
+ * timeout, which no kernel of this build can raise (none waits on another). */
 int kaos_get_status(kaos_handle *h, uint32_t *status);
 
 void kaos_destroy(kaos_handle *h);
@@ -388,24 +390,27 @@ void kaos_destroy(kaos_handle *h);
  * Start-of-step statistics without any device allocation.  This entry point
  * has no counterpart in the reference; it serves callers that cannot call
  * cudaMalloc -- a host running under a fixed device-memory pool of its own,
- * code issuing work while a stream is being captured into a CUDA graph, or
- * a process sharing a GPU under an external memory cap.  It bins n ions
- * (field-line q, V||, Vperp1, Vperp2: device arrays) into the nq cells
- * bounded by the nq+1 device edges d_qedges (lower boundary first) and the
- * velocity grid vg (host arrays), and writes the per-cell moments exactly as
- * kaos_get_moments reports them after a first step: d_moments is a device
- * array [11][nq] holding the selectors KAOS_M0 .. KAOS_NQ, d_counts (device,
- * may be NULL) the nq per-cell ion counts.  `stream` is a cudaStream_t
- * (NULL: the default stream).
+ * or a process sharing a GPU under an external memory cap.  It bins n ions
+ * (field-line q, V||, Vperp1, Vperp2: device arrays; Vperp2 may be NULL only
+ * on a 2D grid) into the nq cells bounded by the nq+1 device edges d_qedges
+ * (lower boundary first) and the velocity grid vg (host arrays, passed to
+ * the kernels by value), and writes the per-cell moments as kaos_get_moments
+ * reports them for the first step after a load: d_moments is a device array
+ * [11][nq] holding the selectors KAOS_M0 .. KAOS_NQ, d_counts (device, may
+ * be NULL) the nq per-cell ion counts.  On a 2D grid an ion whose speed lies
+ * outside the grid is left out of the velocity marginals, where a handle
+ * keeps the ion's previous bin (the stale-index rule), so the two agree
+ * only on the first step after a load.  `stream` is a cudaStream_t (NULL:
+ * the default stream).
  *
  * Scratch histograms live in one file-scope device array of at most 512
  * cells x (1 + 3 x 128) counters (about 0.79 MB), held by every GPU that
  * loads the library until the process exits.  nq > 512 or more than 128
  * velocity cells per axis return KAOS_ERR_CAPACITY.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress) with
- * the device current; make that first call before any stream capture.  All
- * calls share the array and each clears it first, so calls that overlap on
- * the GPU race: serialise them.
+ * device looks up that array's device address (cudaGetSymbolAddress) and
+ * the device's SM count with the device current.  All calls share the
+ * array and each clears it first, so calls that overlap on the GPU race:
+ * serialise them.
  */
 int kaos_moments_noalloc(const kaos_params_c *p, const kaos_vgrid_c *vg,
                          int32_t nq, const double *d_qedges,

@@ -1941,15 +1941,15 @@ void kaos_destroy(kaos_handle *h) {
 // Allocation-free statistics entry point (kaos_moments_noalloc).
 //
 // Some callers cannot call cudaMalloc: a Fortran or C host that runs under a
-// fixed device-memory budget handed out by its own pool, code running while
-// a stream is being captured into a CUDA graph (allocation is not a
-// capturable operation), and processes that share a GPU under an externally
-// enforced memory cap.  For them the start-of-step statistics -- per-cell
-// counts and the moment integrals of IonParticleCountsSub and the
-// ZerothIonMoment .. SecondParIonMoment routines -- run here with every
-// intermediate histogram in one file-scope device array instead of
-// allocated scratch.  The caller passes the particle inputs and the
-// outputs; this code allocates nothing.
+// fixed device-memory budget handed out by its own pool, and processes that
+// share a GPU under an externally enforced memory cap.  For them the
+// start-of-step statistics -- per-cell counts and the moment integrals of
+// IonParticleCountsSub and the ZerothIonMoment .. SecondParIonMoment
+// routines -- run here with every intermediate histogram in one file-scope
+// device array instead of allocated scratch.  The caller passes the
+// particle inputs and the outputs; this code allocates nothing.  The
+// velocity grid travels by value in the kernel arguments (no host-to-device
+// copy of a host buffer).
 //
 // The array holds NOALLOC_MAX_CELLS cells x (1 + 3 * MAXV) 32-bit counters
 // (about 0.79 MB) and lives in every GPU that loads the library until the
@@ -1963,23 +1963,35 @@ constexpr int NOALLOC_MAX_CELLS = 512;
 constexpr size_t NOALLOC_WORDS = (size_t)NOALLOC_MAX_CELLS * (1 + 3 * MAXV);
 
 static __device__ __align__(256) unsigned int g_noalloc_scratch[NOALLOC_WORDS];
-static __device__ __align__(256) VGridC g_noalloc_vgrid;
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mutex;
 unsigned int *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
-VGridC *g_noalloc_vg_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+int g_noalloc_nsm[NOALLOC_MAX_DEVICES] = {0};
+
+// The three axes' FP64 edges of the by-value grid, copied into shared
+// memory (searched there by every thread).
+__device__ __forceinline__ void noalloc_edges(const VGridC &vg, double *s1,
+                                              double *s2, double *sp) {
+  for (int k = threadIdx.x; k <= MAXV; k += blockDim.x) {
+    s1[k] = vg.e1[k];
+    s2[k] = vg.e2[k];
+    sp[k] = vg.epar[k];
+  }
+}
 
 // per-particle cell / velocity-bin search and counting into the scratch
-__global__ void k_noalloc_bin(unsigned *scr, const VGridC *vg, const double *qedges,
+__global__ void k_noalloc_bin(unsigned *scr, const VGridC vg, const double *qedges,
                               int nq, const double *q, const double *vpar,
                               const double *v1, const double *v2, int64_t n) {
   extern __shared__ double E[];
+  __shared__ double S1[MAXV + 1], S2[MAXV + 1], SP[MAXV + 1];
   // orientation: q increases upward when the lower boundary has q <= 0
   const double sgn = qedges[0] <= 0.0 ? 1.0 : -1.0;
   for (int k = threadIdx.x; k <= nq; k += blockDim.x) E[k] = sgn * qedges[k];
+  noalloc_edges(vg, S1, S2, SP);
   __syncthreads();
-  const int n1 = vg->n1, n2 = vg->n2, npar = vg->npar, d3 = vg->three_d;
+  const int n1 = vg.n1, n2 = vg.n2, npar = vg.npar, d3 = vg.three_d;
   unsigned *cnt = scr, *mpar = scr + NOALLOC_MAX_CELLS,
            *m1 = mpar + (size_t)NOALLOC_MAX_CELLS * MAXV,
            *m2 = m1 + (size_t)NOALLOC_MAX_CELLS * MAXV;
@@ -1989,9 +2001,9 @@ __global__ void k_noalloc_bin(unsigned *scr, const VGridC *vg, const double *qed
     if (c < 0) continue;
     atomicAdd(cnt + c, 1u);
     const double a = v1[j], b = v2 ? v2[j] : 0.0;
-    const int bp = vbin(vg->epar, npar, vpar[j]);
-    const int b1 = vbin(vg->e1, n1, d3 ? a : sqrt(a * a + b * b));
-    const int b2 = d3 ? vbin(vg->e2, n2, b) : 0;
+    const int bp = vbin(SP, npar, vpar[j]);
+    const int b1 = vbin(S1, n1, d3 ? a : vperp_mag(a, b));
+    const int b2 = d3 ? vbin(S2, n2, b) : 0;
     if (bp < 0 || b1 < 0 || b2 < 0) continue;
     atomicAdd(mpar + (size_t)c * MAXV + bp, 1u);
     atomicAdd(m1 + (size_t)c * MAXV + b1, 1u);
@@ -1999,10 +2011,13 @@ __global__ void k_noalloc_bin(unsigned *scr, const VGridC *vg, const double *qed
   }
 }
 
-__global__ void k_noalloc_moments(const unsigned *scr, const VGridC *vg, int nq,
+__global__ void k_noalloc_moments(const unsigned *scr, const VGridC vg, int nq,
                                   const double *d3x, double nsnormfac, double ms,
                                   int cenpar, int cenperp, double *out,
                                   int64_t *counts) {
+  __shared__ double S1[MAXV + 1], S2[MAXV + 1], SP[MAXV + 1];
+  noalloc_edges(vg, S1, S2, SP);
+  __syncthreads();
   const unsigned *cnt = scr, *mpar = scr + NOALLOC_MAX_CELLS,
                  *m1 = mpar + (size_t)NOALLOC_MAX_CELLS * MAXV,
                  *m2 = m1 + (size_t)NOALLOC_MAX_CELLS * MAXV;
@@ -2010,8 +2025,8 @@ __global__ void k_noalloc_moments(const unsigned *scr, const VGridC *vg, int nq,
     const double w = nsnormfac / d3x[Q];
     double M[10];
     cell_moments(w, (double)cnt[Q], mpar + (size_t)Q * MAXV, m1 + (size_t)Q * MAXV,
-                 m2 + (size_t)Q * MAXV, vg->epar, vg->e1, vg->e2, vg->npar,
-                 vg->n1, vg->n2, vg->three_d, cenpar, cenperp, ms, M);
+                 m2 + (size_t)Q * MAXV, SP, S1, S2, vg.npar, vg.n1, vg.n2,
+                 vg.three_d, cenpar, cenperp, ms, M);
     for (int k = 0; k < 10; ++k) out[(size_t)k * nq + Q] = M[k];
     out[(size_t)KAOS_NQ * nq + Q] = (double)cnt[Q] * w;
     if (counts) counts[Q] = cnt[Q];
@@ -2031,8 +2046,10 @@ extern "C" int kaos_moments_noalloc(const kaos_params_c *p,
   if (!p || !vgc || !d_qedges || !d_d3x || !d_moments || n < 0 ||
       (n > 0 && (!d_q || !d_vpar || !d_vperp1)))
     return KAOS_ERR_PARAM;
-  if (nq < 1 || nq > NOALLOC_MAX_CELLS) return KAOS_ERR_CAPACITY;
   const int d3 = p->ION2VPERPflag == 1;
+  // a 3D grid bins Vperp2 on its own axis: the array is required
+  if (d3 && n > 0 && !d_vperp2) return KAOS_ERR_PARAM;
+  if (nq < 1 || nq > NOALLOC_MAX_CELLS) return KAOS_ERR_CAPACITY;
   if (vgc->n1 < 1 || vgc->n1 > MAXV || vgc->npar < 1 || vgc->npar > MAXV ||
       (d3 && (vgc->n2 < 1 || vgc->n2 > MAXV || !vgc->e2)) || !vgc->e1 || !vgc->epar)
     return KAOS_ERR_CAPACITY;
@@ -2040,19 +2057,22 @@ extern "C" int kaos_moments_noalloc(const kaos_params_c *p,
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
     return KAOS_ERR_CUDA;
   // set-up once per device, with that device current: host code needs the
-  // device address of the array (its name here is only a host stand-in)
+  // device address of the array (its name here is only a host stand-in),
+  // and the grid of the binning kernel is sized by the device's SM count
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_ptr[dev]) {
-      void *a = nullptr, *b = nullptr;
+      void *a = nullptr;
+      int nsm = 0;
       if (cudaGetSymbolAddress(&a, g_noalloc_scratch) != cudaSuccess) return KAOS_ERR_CUDA;
-      if (cudaGetSymbolAddress(&b, g_noalloc_vgrid) != cudaSuccess) return KAOS_ERR_CUDA;
-      g_noalloc_vg_ptr[dev] = (VGridC *)b;
+      if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+          nsm < 1)
+        return KAOS_ERR_CUDA;
+      g_noalloc_nsm[dev] = nsm;
       g_noalloc_ptr[dev] = (unsigned *)a;
     }
   }
   unsigned *scr = g_noalloc_ptr[dev];
-  VGridC *dvg = g_noalloc_vg_ptr[dev];
   cudaStream_t s = (cudaStream_t)stream;
   VGridC vg{};
   vg.three_d = d3;
@@ -2062,17 +2082,15 @@ extern "C" int kaos_moments_noalloc(const kaos_params_c *p,
   for (int k = 0; k <= vg.n1; ++k) vg.e1[k] = vgc->e1[k];
   for (int k = 0; k <= vg.npar; ++k) vg.epar[k] = vgc->epar[k];
   for (int k = 0; d3 && k <= vg.n2; ++k) vg.e2[k] = vgc->e2[k];
-  // the grid goes through the staging copy of pageable memory: the host
-  // copy may leave scope when this returns
-  if (cudaMemcpyAsync(dvg, &vg, sizeof(VGridC), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemsetAsync(scr, 0, NOALLOC_WORDS * sizeof(unsigned), s) != cudaSuccess)
+  if (cudaMemsetAsync(scr, 0, NOALLOC_WORDS * sizeof(unsigned), s) != cudaSuccess)
     return KAOS_ERR_CUDA;
   if (n > 0) {
-    int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    // 8 blocks of 256 threads per SM stride over the ions
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)g_noalloc_nsm[dev] * 8);
     k_noalloc_bin<<<blocks, 256, (size_t)(nq + 1) * sizeof(double), s>>>(
-        scr, dvg, d_qedges, nq, d_q, d_vpar, d_vperp1, d_vperp2, n);
+        scr, vg, d_qedges, nq, d_q, d_vpar, d_vperp1, d_vperp2, n);
   }
-  k_noalloc_moments<<<1, 256, 0, s>>>(scr, dvg, nq, d_d3x, nsnormfac, p->ms,
+  k_noalloc_moments<<<1, 256, 0, s>>>(scr, vg, nq, d_d3x, nsnormfac, p->ms,
                                       p->PHASEENERGYPARIONMOMENTCENTERflag == 1,
                                       p->PHASEENERGYPERPIONMOMENTCENTERflag == 1,
                                       d_moments, d_counts);

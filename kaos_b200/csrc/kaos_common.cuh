@@ -32,6 +32,7 @@ constexpr int MAXV = 128;          // max velocity cells per axis
 constexpr int DEAD = -3;           // ion slot converted to an ENA
 constexpr int BELOW = -1;          // reference Qind 0  (below LB)
 constexpr int ABOVE = -2;          // reference Qind -1 (above UB)
+// status bits; ST_TIMEOUT is reserved (no kernel here waits on another)
 constexpr uint32_t ST_NAN = 1u, ST_CAP = 2u, ST_TIMEOUT = 4u;
 
 struct VGridC {
@@ -103,6 +104,13 @@ struct Accum {
 __device__ __forceinline__ double warp_sum(double x) {
   for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
   return x;
+}
+
+// |Vperp| = sqrt(V1^2 + V2^2) with every product and the sum rounded on
+// its own (no fused multiply-add): the value the 2D velocity-bin search
+// compares, the same on every path and in the CPU oracle.
+__device__ __forceinline__ double vperp_mag(double a, double b) {
+  return sqrt(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
 }
 
 __host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b) {

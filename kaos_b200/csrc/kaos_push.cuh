@@ -622,7 +622,9 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
     double v1 = I.v1[j], v2 = I.v2[j];
     double aea = I.aea[j], ag = I.ag[j];
     if (a.prologue) field_prologue(a, T, E, Cc, I.qk4[j], qprev, aea, ag);
-    const double vp2 = v1 * v1 + v2 * v2;
+    // Vperp^2 without a fused multiply-add: its square root is the 2D grid's
+    // binned speed (vperp_mag), the same value on every path
+    const double vp2 = __dadd_rn(__dmul_rn(v1, v1), __dmul_rn(v2, v2));
     // ---- k1: KineticUpdateA -------------------------------------------
     const Geo<double> g1 = geo(rho, z);
     const int qi = cell_search_from(E, T.nq, T.sgn * g1.q, qprev);

@@ -658,7 +658,7 @@ __global__ void k_inject(InjArgs a) {
       vpar = a.ub ? -r : r;
     }
     if (a.stat) v1 = v2 = vpar = 0.0;  // STATICINJECTIONflag
-    const double vp = sqrt(v1 * v1 + v2 * v2);
+    const double vp = vperp_mag(v1, v2);
     int bp = vbin(c_vg.epar, c_vg.npar, vpar);
     int b1 = vbin(c_vg.e1, c_vg.n1, d3 ? v1 : vp);
     int b2 = d3 ? vbin(c_vg.e2, c_vg.n2, v2) : 0;
@@ -740,7 +740,7 @@ __device__ __forceinline__ void store_ion(const Ions &I, const TubeD &T,
   I.id[k] = id;
   if (I.vb) {
     const int bp = vbin(c_vg.epar, c_vg.npar, vpar);
-    const int b1 = vbin(c_vg.e1, c_vg.n1, sqrt(v1 * v1 + v2 * v2));
+    const int b1 = vbin(c_vg.e1, c_vg.n1, vperp_mag(v1, v2));
     I.vb[k] = ((b1 + 1) << 16) | (bp + 1);
   }
   if (mixed) {

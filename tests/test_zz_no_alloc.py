@@ -1,8 +1,7 @@
 """The allocation-free statistics entry point (kaos_moments_noalloc).
 
 Callers that cannot allocate device memory (a host with its own fixed
-device pool, work issued during stream capture, a GPU shared under a memory
-cap) get the start-of-step counts and moments from this entry point, whose
+device pool, a GPU shared under a memory cap) get the start-of-step counts and moments from this entry point, whose
 scratch histograms live in a static device array.  This test drives it
 through the C-ABI on device buffers the test owns, twice in a row (the
 second call must clear what the first left behind), and checks both results
@@ -77,3 +76,10 @@ def test_noalloc_rejects_oversize_grid():
                                 None, None, None, None, 0, C.addressof(dummy),
                                 None, None)
     assert rc == 2  # KAOS_ERR_CAPACITY
+    # a 3D grid needs the Vperp2 array whenever there are ions to bin
+    rc = L.kaos_moments_noalloc(C.addressof(pc), C.addressof(vgc), tube.nq,
+                                C.addressof(dummy), C.addressof(dummy), 1.0,
+                                C.addressof(dummy), C.addressof(dummy),
+                                C.addressof(dummy), None, 1, C.addressof(dummy),
+                                None, None)
+    assert rc == 1  # KAOS_ERR_PARAM
