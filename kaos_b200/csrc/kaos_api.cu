@@ -340,6 +340,8 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
     smem += (size_t)(5 * nq + 1) * sizeof(double) + (size_t)10 * nq * sizeof(float);
   smem += (size_t)BIN_WIN * (1 + h->vg.npar + h->vg.n1 + (h->three_d ? h->vg.n2 : 0)) *
           sizeof(unsigned);  // block-private binning window
+  const bool bins_variant = a.bin || a.prologue || a.bin_only || !h->three_d;
+  if (h->mixed && bins_variant) smem += BINS_SMEM_BYTES;  // FP64 edges + tables
   const int rs = h->mixed ? h->regsel : 0, ps = h->persistent;
   // kernel variant: [master-step work][three_d][register budget][persistent];
   // the budgets: 64 registers (4 blocks of 256 threads per SM), 80 (3
@@ -542,7 +544,7 @@ Fields ion_fields(kaos_handle *h, int from, int to) {
     if (s) F.f[F.n++] = Field{s, d, sz};
   };
   if (h->mixed) {
-    add(A.co, B.co, 8); add(A.fvpar, B.fvpar, 4); add(A.fv, B.fv, 8);
+    add(A.x, B.x, 8); add(A.vpar, B.vpar, 8); add(A.v12, B.v12, 16);
     add(A.ffl, B.ffl, 8); add(A.fqk4, B.fqk4, 4);
   } else {
     add(A.rho, B.rho, 8); add(A.z, B.z, 8); add(A.vpar, B.vpar, 8);
@@ -564,8 +566,8 @@ void spare_slots(kaos_handle *h, int t, double *d[4], int32_t **qi) {
   Ions &S = h->ion[1 - h->cur];
   const int64_t o = h->th[t].off;
   if (h->mixed) {
-    d[0] = (double *)(S.co + o);
-    d[1] = (double *)(S.fv + o);
+    d[0] = S.x + o;
+    d[1] = S.vpar + o;
     d[2] = (double *)(S.ffl + o);
   } else {
     d[0] = S.rho + o;
@@ -636,7 +638,7 @@ int launch_boundary(kaos_handle *h, int compact) {
     b.lb_out = h->d_lb_out;
     b.ub_out = h->d_ub_out;
     b.qind_w = h->ion[h->cur].qind;
-    b.co_w = h->mixed ? h->ion[h->cur].co : nullptr;
+    b.x_w = h->mixed ? h->ion[h->cur].x : nullptr;
     CK(cudaMemsetAsync(h->d_lb_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
     CK(cudaMemsetAsync(h->d_ub_out, 0, h->ntubes * sizeof(unsigned long long), h->s));
     CK(cudaMemsetAsync(h->d_lb_in, 0, h->ntubes * sizeof(unsigned long long), h->s));
@@ -1273,9 +1275,9 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   for (int b = 0; b < 2; ++b) {
     Ions &I = h->ion[b];
     if (h->mixed) {
-      if ((rc = dalloc(h, &I.co, cap))) return rc;
-      if ((rc = dalloc(h, &I.fvpar, cap))) return rc;
-      if ((rc = dalloc(h, &I.fv, cap))) return rc;
+      if ((rc = dalloc(h, &I.x, cap))) return rc;
+      if ((rc = dalloc(h, &I.vpar, cap))) return rc;
+      if ((rc = dalloc(h, &I.v12, cap))) return rc;
       if ((rc = dalloc(h, &I.ffl, cap))) return rc;
       if ((rc = dalloc(h, &I.fqk4, cap))) return rc;
     } else {
@@ -1785,6 +1787,7 @@ int kaos_get_particles(kaos_handle *h, int32_t tube, double *q, double *vpar,
   a.nl = nl;
   a.qGL = h->ct.qGL + T.coff;
   a.qGH = h->ct.qGH + T.coff;
+  a.nq = T.nq;
   a.mixed = h->mixed;
   a.nb = (int)ceil_div(nl, (int64_t)EXP_THREADS * EXP_ITEMS);
   double *dq[4];

@@ -5,10 +5,11 @@
 //  * ions: structure of arrays, tube t owns [tube.off, tube.off + tube.cap).
 //    FP64 mode stores the meridian-plane position (rho, z) -- the ion motion
 //    is confined to its flux-tube meridian (phi = phiG) -- plus V||, Vperp1,
-//    Vperp2 and the cached field accelerations.  Mixed mode stores the
-//    position as an integer cell + FP32 offset in q, and FP32 velocities,
-//    the pairs that are read together interleaved (cell|offset,
-//    Vperp1|Vperp2, AEA|AG).
+//    Vperp2 and the cached field accelerations.  Mixed mode keeps its state
+//    in FP64 accumulators and does its arithmetic in FP32: the position as
+//    one FP64 cell coordinate (integer part = cell, fraction = offset in q
+//    within the cell), V|| and the (Vperp1, Vperp2) pair in FP64, the
+//    cached field accelerations (AEA, AG) and q_k4 in FP32.
 //  * per-cell tables: concatenated over tubes, tube t at [tube.coff, +nq).
 //  * velocity-grid edges: __constant__ memory (shared by all tubes).
 #pragma once
@@ -32,6 +33,9 @@ constexpr int MAXV = 128;          // max velocity cells per axis
 constexpr int DEAD = -3;           // ion slot converted to an ENA
 constexpr int BELOW = -1;          // reference Qind 0  (below LB)
 constexpr int ABOVE = -2;          // reference Qind -1 (above UB)
+// mixed mode: the cell coordinate of a slot marked DEAD (any value below
+// XDEAD_LIM; a live or escaped ion's coordinate is never that far out)
+constexpr double XDEAD = -1e30, XDEAD_LIM = -1e29;
 // status bits; ST_TIMEOUT is reserved (no kernel here waits on another)
 constexpr uint32_t ST_NAN = 1u, ST_CAP = 2u, ST_TIMEOUT = 4u;
 
@@ -67,16 +71,18 @@ struct CellTables {
   int64_t ncell_total;
 };
 
-// Ion particle arrays.  FP64 mode uses the d* arrays, mixed the f* ones.
+// Ion particle arrays.  vpar (V||, FP64) serves both modes; FP64 mode adds
+// rho, z, v1, v2, aea, ag, qk4, mixed mode x, v12, ffl, fqk4.
 struct Ions {
-  double *rho, *z, *vpar, *v1, *v2, *aea, *ag, *qk4;  // FP64 mode
+  double *rho, *z, *vpar, *v1, *v2, *aea, *ag, *qk4;  // FP64 mode (+ vpar)
   double *rho4, *z4;   // FP64 + charge exchange: the k4 point of the step
-  // mixed mode: fields read together are stored together (one 8-byte
-  // access each): co = (position cell, FP32 offset bits), fv = (Vperp1,
-  // Vperp2), ffl = (AEA, AG)
-  int2 *co;
-  float2 *fv, *ffl;
-  float *fvpar, *fqk4;
+  // mixed mode: x = cell + offset in q within the cell (FP64; XDEAD marks
+  // a dead slot), v12 = (Vperp1, Vperp2) in FP64, and in FP32 the pair read
+  // together ffl = (AEA, AG) and q at the k4 point
+  double *x;
+  double2 *v12;
+  float2 *ffl;
+  float *fqk4;
   int32_t *qind;       // start-of-step cell Qindk1 (0-based, sentinels)
   int32_t *vb;         // 2D grid: stale (vperp,vpar) bins, packed
   uint64_t *id;        // persistent particle id (RNG key, order key)
@@ -111,6 +117,12 @@ __device__ __forceinline__ double warp_sum(double x) {
 // compares, the same on every path and in the CPU oracle.
 __device__ __forceinline__ double vperp_mag(double a, double b) {
   return sqrt(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+}
+
+// Mixed mode: the cell of a cell coordinate x (clamped to the tube: an
+// escaped ion keeps its end cell and an offset outside [0, 1]).
+__device__ __forceinline__ int x_cell(double x, int nq) {
+  return min(max(__double2int_rd(x), 0), nq - 1);
 }
 
 __host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b) {

@@ -262,9 +262,9 @@ __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) 
       // ion position and velocity at the end of the previous step
       double rho, z, vpar, v1, v2, qk4;
       if (a.mixed) {
-        const int2 co = a.ion.co[j];
-        const int cc = co.x;
-        const double oo = (double)__int_as_float(co.y);
+        const double xx = a.ion.x[j];
+        const int cc = x_cell(xx, T.nq);
+        const double oo = xx - (double)cc;
         const double qq = a.ct.qGL[T.coff + cc] +
                           oo * (a.ct.qGH[T.coff + cc] - a.ct.qGL[T.coff + cc]);
         const double ug = a.ct.uL[T.coff + cc] +
@@ -273,8 +273,8 @@ __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) 
         const double s2 = u / T.pG;
         rho = u * RE * sqrt(s2);
         z = u * RE * qq * u * u;
-        vpar = a.ion.fvpar[j];
-        const float2 v = a.ion.fv[j];
+        vpar = a.ion.vpar[j];
+        const double2 v = a.ion.v12[j];
         v1 = v.x;
         v2 = v.y;
         qk4 = a.ion.fqk4[j];
@@ -321,7 +321,7 @@ __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) 
         atomicOr(a.status, ST_CAP);
       }
       a.ion.qind[j] = DEAD;
-      if (a.mixed) a.ion.co[j].x = DEAD;
+      if (a.mixed) a.ion.x[j] = XDEAD;
     }
     __syncthreads();
   }

@@ -421,15 +421,19 @@ __device__ __forceinline__ void field_prologue32(const ForceFlags &ff,
 }
 
 // Velocity-bin search of the mixed push from a lookup table: VTAB uniform
-// slots over the axis hold the bin of each slot's left end, and a short
-// walk over the edges finishes the search.  The walk establishes both edge
-// conditions of vbin (v <= e[b+1], and v > e[b] unless b = 0), so the result
-// equals vbin's whatever the table holds.
+// slots over the axis hold the bin of each slot's left end (built from the
+// FP32 edges), and a short walk over the FP64 edges finishes the search.
+// The walk establishes both edge conditions of vbin (v <= e[b+1], and
+// v > e[b] unless b = 0) in FP64, so the result equals vbin's on the FP64
+// edges whatever the table holds.
 constexpr int VTAB = 256;
 struct VBinTab {
   float e0, iw;              // first edge, VTAB / (last edge - first edge)
   unsigned char t[VTAB];     // bin at each slot's left end (n <= 128)
 };
+// Dynamic shared memory of the mixed push's bin searches: alignment slack,
+// three FP64 edge arrays and three lookup tables.
+constexpr size_t BINS_SMEM_BYTES = 16 + 3 * (MAXV + 1) * sizeof(double) + 3 * sizeof(VBinTab);
 
 // All threads of the block; edges e[0..n] in shared memory already visible,
 // and the caller synchronises before the table is used.
@@ -444,10 +448,10 @@ __device__ __forceinline__ void build_vbin_tab(VBinTab &T, const float *e, int n
   }
 }
 
-__device__ __forceinline__ int vbin_tab(const VBinTab &T, const float *e, int n,
-                                        float v) {
+__device__ __forceinline__ int vbin_tab(const VBinTab &T, const double *e, int n,
+                                        double v) {
   if (!(v >= e[0] && v <= e[n])) return -1;
-  const int s = min(max((int)((v - T.e0) * T.iw), 0), VTAB - 1);
+  const int s = min(max((int)(((float)v - T.e0) * T.iw), 0), VTAB - 1);
   int b = T.t[s];
   // one predicated step up settles almost every value (the table gives the
   // bin of the slot's left end); the loops finish the rare rest exactly
@@ -479,18 +483,21 @@ __device__ __forceinline__ float ex2f(float x) {
 // log2 Sigma = log2(Vperp^2)/2 + log2(2 pi/lambda) - log2 Om.
 // The Gaussians are the same Box-Muller pair of one Philox draw as
 // gauss2_32.  hk (8 per cell): K1 K2 c1 c2 log2(1/Om0) lambda
-// log2(2 pi/lambda) 0.
+// log2(2 pi/lambda) 0.  The kicks come back in dv1, dv2 (zero outside the
+// stochastic regime); the caller adds them to its FP64 Vperp.
 __device__ __forceinline__ void heat32(const PushArgs &a, uint32_t step,
                                        const float *hk, uint64_t id,
                                        float invsumds, float ylim, float Om,
-                                       float vabs, float &v1, float &v2) {
+                                       float vabs, float vp2, float &dv1,
+                                       float &dv2) {
+  dv1 = dv2 = 0.0f;
   const float y = Om * vabs * invsumds;  // (Om s)^2
   if (!(y <= ylim)) return;
   const float4 h0 = *(const float4 *)hk, h1 = *(const float4 *)(hk + 4);
   const float LOm = lg2f(Om);
   float b = 0.25f * lg2f(y);
   if (h1.y != 0.0f) {  // lambda != 0
-    const float ls = fmaf(0.5f, lg2f(v1 * v1 + v2 * v2), h1.z) - LOm;
+    const float ls = fmaf(0.5f, lg2f(vp2), h1.z) - LOm;
     if (ls >= 0.0f) b -= 1.5f * ls;
   }
   const float lx = LOm + h1.x;
@@ -504,8 +511,8 @@ __device__ __forceinline__ void heat32(const PushArgs &a, uint32_t step,
   const float t = fmaxf(-1.38629436f * lg2f(u1), 1e-30f);
   const float R = t * rsq(t);
   const float ang = 6.2831853f * u2;
-  v1 = fmaf(h0.x * e1 * R, cosa(ang), v1);
-  v2 = fmaf(h0.y * e2 * R, sina(ang), v2);
+  dv1 = h0.x * e1 * R * cosa(ang);
+  dv2 = h0.y * e2 * R * sina(ang);
 }
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0 by Newton from u0 (the
@@ -739,17 +746,18 @@ __device__ __forceinline__ float apar_bf(const Geo<float> &g, float vperp2,
   return s * (f.cm * m - f.cg * fabsf(ag) + f.ce2 * fabsf(aea)) + f.ce1 * aea;
 }
 
-// Start-of-step velocity bins of one ion: (V⊥1, V⊥2, V∥) on the 3D grid;
-// on the 2D grid (|V⊥|, V∥) with the previous bin kept for a value outside
-// the grid (the stale-index rule), stored back when it changed.
+// Start-of-step velocity bins of one ion from its FP64 velocities and the
+// FP64 edges: (V⊥1, V⊥2, V∥) on the 3D grid; on the 2D grid (|V⊥|, V∥)
+// with the previous bin kept for a value outside the grid (the stale-index
+// rule), stored back when it changed.
 template <bool THREE_D>
 __device__ __forceinline__ void start_bins(const PushArgs &a, const Ions &I,
-                                           int64_t j, const float *VE1,
-                                           const float *VE2, const float *VEP,
+                                           int64_t j, const double *VE1,
+                                           const double *VE2, const double *VEP,
                                            const VBinTab &VT1, const VBinTab &VT2,
-                                           const VBinTab &VTP,
-                                           float vpar, float v1, float v2,
-                                           float vp2, int &b1, int &b2, int &bp) {
+                                           const VBinTab &VTP, double vpar,
+                                           double v1, double v2, int &b1, int &b2,
+                                           int &bp) {
   b2 = -1;
   if (THREE_D) {
     bp = vbin_tab(VTP, VEP, c_vg.npar, vpar);
@@ -758,7 +766,7 @@ __device__ __forceinline__ void start_bins(const PushArgs &a, const Ions &I,
   } else {
     const int old = I.vb[j];
     const int np_ = vbin_tab(VTP, VEP, c_vg.npar, vpar);
-    const int n1_ = vbin_tab(VT1, VE1, c_vg.n1, sqrtf(vp2));
+    const int n1_ = vbin_tab(VT1, VE1, c_vg.n1, vperp_mag(v1, v2));
     bp = np_ >= 0 ? np_ : (old & 0xffff) - 1;
     b1 = n1_ >= 0 ? n1_ : (old >> 16) - 1;
     const int nw = ((b1 + 1) << 16) | (bp + 1);
@@ -767,9 +775,24 @@ __device__ __forceinline__ void start_bins(const PushArgs &a, const Ions &I,
 }
 
 // ---------------------------------------------------------------------------
-// Mixed kernel: position = (cell, FP32 offset in q); FP32 velocities and RK
-// stages; FP64 for the q reconstruction, the quartic root (Newton from a
-// per-cell linear guess) and the renormalised q of the new position.
+// Mixed kernel: FP32 arithmetic on FP64 state.  The position is one FP64
+// cell coordinate x = cell + offset in q within the cell; V|| and the Vperp
+// pair are FP64.  Every RK stage, force evaluation and the heating kick run
+// in FP32; FP64 is kept for the q reconstruction, the quartic root (Newton
+// from a per-cell linear guess), the dominant displacement term h V|| e1,
+// the renormalised q of the new position, the accumulation of the FP32
+// velocity increments into the FP64 velocities, and all reductions.  The
+// start-of-step bins compare the FP64 velocities with the FP64 edges, as
+// the FP64 path does.
+//
+// V|| along the new field direction: with e1, e2, e4, eN the field
+// directions at the start, k2, k4 and new points, the FP64 path computes
+// eN . (V|| e1 + h/6 (a1 e1 + 4 a2 e2 + a4 e4)).  All of e1..e4 lie within
+// ~1e-6 rad of eN, so e_k . eN = 1 - O(1e-12): the update is
+//   V||N = V|| + h/6 (a1 + 4 a2 + a4) - V|| dal^2 / 2,
+// dal = angle between e1 and eN = 3 (1 + cos^2) / (1 + 3 cos^2) dtheta along
+// the dipole line (d/dtheta of atan2(3 cos sin, 3 cos^2 - 1)), an FP32
+// increment added to the FP64 V||.
 // NT threads per block and MINB resident blocks per SM set the register
 // budget (256 x 4: 64 registers, 256 x 3: 80, 128 x 7: 72); the autotuner
 // picks one.
@@ -790,21 +813,28 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   float2 *FE = (float2 *)(HK + 8 * nqmax);
   unsigned *HC = (unsigned *)(FE + nqmax);
   const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
+  const float hh6 = h * h6;
+  const double hd = a.h;
   const uint32_t step = a.dstep ? *a.dstep : a.step;
   const float fRE = (float)RE;
   const ForceC fc = force_c(a.ff);
   Ions I = a.ion;
   TubeD T;
   int tcur = -1;
-  // velocity-cell edges for the bin searches in shared memory
-  __shared__ float VE1[MAXV + 1], VE2[MAXV + 1], VEP[MAXV + 1];
-  __shared__ VBinTab VT1, VT2, VTP;
+  // velocity-cell edges for the bin searches in shared memory (FP64 edges
+  // for the comparisons, FP32 lookup tables for the first guess), after the
+  // binning window; only the variants that bin are launched with room for
+  // them (BINS_SMEM_BYTES)
+  double *VE1 = (double *)(((uintptr_t)(HC + nqmax + bin_win_size()) + 15) &
+                           ~(uintptr_t)15);
+  double *VE2 = VE1 + (MAXV + 1), *VEP = VE2 + (MAXV + 1);
+  VBinTab *VTS = (VBinTab *)(VEP + (MAXV + 1));
+  VBinTab &VT1 = VTS[0], &VT2 = VTS[1], &VTP = VTS[2];
   if (bin || !THREE_D) {
-    load_vgrid_smem(c_vg.f1, c_vg.f2, c_vg.fpar, VE1, VE2, VEP);
-    __syncthreads();
-    build_vbin_tab(VTP, VEP, c_vg.npar);
-    build_vbin_tab(VT1, VE1, c_vg.n1);
-    if (THREE_D) build_vbin_tab(VT2, VE2, c_vg.n2);
+    load_vgrid_smem(c_vg.e1, c_vg.e2, c_vg.epar, VE1, VE2, VEP);
+    build_vbin_tab(VTP, c_vg.fpar, c_vg.npar);
+    build_vbin_tab(VT1, c_vg.f1, c_vg.n1);
+    if (THREE_D) build_vbin_tab(VT2, c_vg.f2, c_vg.n2);
     // the first barrier of the item loop orders the tables before any use
   }
   // one work item per block, or a persistent grid striding over the items
@@ -843,7 +873,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   if (a.cxc)
     for (int k = threadIdx.x; k < T.nq; k += blockDim.x) HC[k] = 0u;
   BinWin W{};
-  if (bin) W = bin_win_init(HC + nqmax, max(a.ion.co[T.off + beg].x, 0), T.nq);
+  if (bin) {
+    const double xf = a.ion.x[T.off + beg];
+    W = bin_win_init(HC + nqmax, xf < XDEAD_LIM ? 0 : x_cell(xf, T.nq), T.nq);
+  }
   __syncthreads();
   const float invsumds = (float)(1.0 / T.sumdsICR);
   const double ipG = 1.0 / T.pG;
@@ -852,42 +885,44 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   const float ylim = (float)((2.0 * PI / a.h) * (2.0 * PI / a.h));
   // Software pipeline: the state of the next ion of this thread is loaded
   // before the current one is pushed, so its HBM latency overlaps the work.
-  int n_c = DEAD;
-  float n_o = 0.f, n_vp = 0.f, n_v1 = 0.f, n_v2 = 0.f, n_ea = 0.f, n_ag = 0.f;
+  double n_x = XDEAD, n_vp = 0.0;
+  double2 n_v = make_double2(0.0, 0.0);
+  float2 n_f = make_float2(0.f, 0.f);
   uint64_t n_id = 0;
   float n_qk = 0.f;  // q_k4 of the master-step field re-interpolation
   if (beg + threadIdx.x < end) {
     const int64_t j = T.off + beg + threadIdx.x;
-    const int2 co = I.co[j];
-    const float2 v = I.fv[j], f = I.ffl[j];
-    n_c = co.x; n_o = __int_as_float(co.y); n_vp = I.fvpar[j];
-    n_v1 = v.x; n_v2 = v.y; n_ea = f.x; n_ag = f.y;
+    n_x = I.x[j];
+    n_vp = I.vpar[j];
+    n_v = I.v12[j];
+    n_f = I.ffl[j];
     if (a.icr) n_id = I.id[j];
     if (prologue) n_qk = I.fqk4[j];
   }
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const int64_t j = T.off + i;
-    const int c0 = n_c;
-    const float o0 = n_o;
-    const float vpar = n_vp;
-    float v1 = n_v1, v2 = n_v2;
-    float aea = n_ea, ag = n_ag;
+    const double x0 = n_x;
+    const double vpar = n_vp;
+    const double v1 = n_v.x, v2 = n_v.y;
+    float aea = n_f.x, ag = n_f.y;
     const uint64_t pid = n_id;
     const float qk0 = n_qk;
     if (i + blockDim.x < end) {
       const int64_t jn = j + blockDim.x;
-      const int2 co = I.co[jn];
-      const float2 v = I.fv[jn], f = I.ffl[jn];
-      n_c = co.x; n_o = __int_as_float(co.y); n_vp = I.fvpar[jn];
-      n_v1 = v.x; n_v2 = v.y; n_ea = f.x; n_ag = f.y;
+      n_x = I.x[jn];
+      n_vp = I.vpar[jn];
+      n_v = I.v12[jn];
+      n_f = I.ffl[jn];
       if (a.icr) n_id = I.id[jn];
       if (prologue) n_qk = I.fqk4[jn];
     }
-    if (c0 == DEAD) continue;
+    if (x0 < XDEAD_LIM) continue;  // slot marked DEAD
+    const int c0 = x_cell(x0, T.nq);
+    const double o0 = x0 - (double)c0;  // exact
     if (prologue) field_prologue32(a.ff, T, E, Cc, FE, qk0, c0, qs_ms, aea, ag);
     // ---- start-of-step position: q, then (r, theta) by FP64 Newton -------
-    const double q0 = fma((double)o0, DQ[c0], QL[c0]);
-    const double u = quartic_newton<true>(q0, ipG, fma((double)o0, UD[c0], UL[c0]), 2);
+    const double q0 = fma(o0, DQ[c0], QL[c0]);
+    const double u = quartic_newton<true>(q0, ipG, fma(o0, UD[c0], UL[c0]), 2);
     const double s2 = u * ipG;  // sin^2(theta)
     // sqrt(s2): FP32 seed and one FP64 Newton step (relative error ~1e-14)
     double ys = (double)rsq((float)s2);
@@ -898,7 +933,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     const double rho0 = r * st, z0 = r * ct;
     // an offset strictly inside (0, 1) puts q0 inside cell c0 (its FP64
     // rounding is far below the margin): no edge search
-    const int qi = (o0 > 1e-6f && o0 < 1.0f - 1e-6f)
+    const int qi = (o0 > 1e-9 && o0 < 1.0 - 1e-9)
                        ? c0 : cell_search_from(E, T.nq, T.sgn * q0, c0);
     // ---- k1 geometry in FP32 ---------------------------------------------
     Geo<float> g1;
@@ -910,32 +945,50 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     g1.isl = rsq(g1.ell);
     g1.er = 3.0f * g1.ct * g1.st * g1.isl;
     g1.ez = (3.0f * g1.ct * g1.ct - 1.0f) * g1.isl;
-    const float vp2 = v1 * v1 + v2 * v2;
+    const float vparf = (float)vpar, v1f = (float)v1, v2f = (float)v2;
+    const float vp2 = v1f * v1f + v2f * v2f;
+    const float rf = (float)rho0, zf = (float)z0;
+    // ---- the dominant displacement term h V|| e1 in FP64 (the direction
+    // from the FP64 cos/sin, 1/sqrt(ell) from the FP32 value and one FP64
+    // Newton step), taken now so that only its end point stays live --------
+    const double ell64 = fma(3.0 * ct, ct, 1.0);
+    double yl = (double)g1.isl;
+    yl = yl * fma(-0.5 * ell64 * yl, yl, 1.5);
+    const double hv = hd * vpar * yl;
+    const double xr0 = fma(hv, 3.0 * ct * st, rho0);
+    const double xz0 = fma(hv, fma(3.0 * ct, ct, -1.0), z0);
     if (bin_only) {
       int b1, b2, bp;
-      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, VT1, VT2, VTP, vpar, v1, v2, vp2, b1, b2, bp);
+      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, VT1, VT2, VTP, vpar, v1, v2, b1, b2, bp);
       if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
       if (a.write_qind) I.qind[j] = qi;
       continue;
     }
     const float a1 = apar_bf(g1, vp2, aea, ag, fc);
-    float v1n = v1, v2n = v2;
+    double v1n = v1, v2n = v2;  // after the wave-heating kick
     if (a.icr && qi >= 0) {
-      const float rf = (float)r;
+      const float rr = (float)r;
       const float sl = g1.ell * g1.isl;
       const float ir3 = g1.ir * g1.ir * g1.ir;
       const float Om = qs_ms * (float)MDIP * sl * ir3;
-      const float invOm = c_invOm * (rf * rf * rf) * g1.isl;
       const float *hk = HK + 8 * qi;
       if (!a.icrcoh) {
-        heat32(a, step, hk, pid, invsumds, ylim, Om, fabsf(vpar), v1n, v2n);
+        float dv1, dv2;
+        heat32(a, step, hk, pid, invsumds, ylim, Om, fabsf(vparf), vp2, dv1, dv2);
+        v1n = v1 + (double)dv1;
+        v2n = v2 + (double)dv2;
       } else {
+        const float invOm = c_invOm * (rr * rr * rr) * g1.isl;
         const HeatC<float> hc{hk[0], hk[1], hk[2], hk[3], hk[4], hk[5]};
-        heat<float>(a, step, hc, pid, invsumds, Om, invOm, fabsf(vpar), v1n, v2n);
+        float w1 = v1f, w2 = v2f;
+        heat<float>(a, step, hc, pid, invsumds, Om, invOm, fabsf(vparf), w1, w2);
+        v1n = (double)w1;
+        v2n = (double)w2;
       }
     }
-    const float rf = (float)rho0, zf = (float)z0;
-    const float VRr = vpar * g1.er, VRz = vpar * g1.ez;
+    // stored at once: the kicked pair holds no registers through the RK
+    if (a.icr) I.v12[j] = make_double2(v1n, v2n);
+    const float VRr = vparf * g1.er, VRz = vparf * g1.ez;
     const Geo<float> g2 = geo(fmaf(hh, VRr, rf), fmaf(hh, VRz, zf));
     const float a2 = apar_bf(g2, vp2, aea, ag, fc);
     const float A1r = a1 * g1.er, A1z = a1 * g1.ez;
@@ -943,14 +996,11 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     const float a4 = apar_bf(g4, vp2, aea, ag, fc);
     if (a.write_qk4) I.fqk4[j] = g4.q;
     const float A2r = a2 * g2.er, A2z = a2 * g2.ez;
-    const float A4r = a4 * g4.er, A4z = a4 * g4.ez;
-    const float VNr = VRr + h6 * (A1r + 4.0f * A2r + A4r);
-    const float VNz = VRz + h6 * (A1z + 4.0f * A2z + A4z);
-    // displacement h/6 (V_R + 4 (V_R + h/2 A1) + (V_R + h A2)) in FP32
-    const float dr = h6 * (6.0f * VRr + 2.0f * h * A1r + h * A2r);
-    const float dz = h6 * (6.0f * VRz + 2.0f * h * A1z + h * A2z);
+    // ---- displacement h/6 (V_R + 4 (V_R + h/2 A1) + (V_R + h A2)) ---------
+    // = h V|| e1 (FP64, above) + h^2/6 (2 A1 + A2) (FP32)
+    const float ddr = hh6 * (2.0f * A1r + A2r), ddz = hh6 * (2.0f * A1z + A2z);
     // ---- renormalisation in FP64: q of the new point --------------------
-    const double xr = rho0 + (double)dr, xz = z0 + (double)dz;
+    const double xr = xr0 + (double)ddr, xz = xz0 + (double)ddz;
     const double r2 = xr * xr + xz * xz;
     double y = (double)rsq((float)r2);
     y = y * fma(-0.5 * r2 * y, y, 1.5);
@@ -961,24 +1011,25 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     const int cs = qi >= 0 ? qi : c0;
     double od = (qN - QL[cs]) * IDQ[cs];
     int cpos = cs;
-    if (!(od > 1e-6 && od < 1.0 - 1e-6)) {
+    if (!(od > 1e-9 && od < 1.0 - 1e-9)) {
       const int cN = cell_search_from(E, T.nq, T.sgn * qN, cs);
       cpos = cN >= 0 ? cN : (cN == BELOW ? 0 : T.nq - 1);
       od = (qN - QL[cpos]) * IDQ[cpos];
     }
-    const float oN = (float)od;
-    // ---- V|| along the new field direction (FP32) -----------------------
-    const Geo<float> gN = geo((float)xr, (float)xz);
-    const float vparN = gN.er * VNr + gN.ez * VNz;
+    const double xN = (double)cpos + od;
+    // ---- V|| along the new field direction ------------------------------
+    const float dth = (zf * fmaf(h, VRr, ddr) - rf * fmaf(h, VRz, ddz)) * (g1.ir * g1.ir);
+    const float dal = 3.0f * fmaf(g1.ct, g1.ct, 1.0f) * (g1.isl * g1.isl) * dth;
+    const float dv = fmaf(h6, a1 + 4.0f * a2 + a4, -0.5f * vparf * dal * dal);
+    const double vparN = vpar + (double)dv;
     if (bin || !THREE_D) {
       int b1, b2, bp;
-      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, VT1, VT2, VTP, vpar, v1, v2, vp2, b1, b2, bp);
+      start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, VT1, VT2, VTP, vpar, v1, v2, b1, b2, bp);
       if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
     }
-    if (!isfinite(vparN) || !isfinite(oN)) atomicOr(a.status, ST_NAN);
-    I.co[j] = make_int2(cpos, __float_as_int(oN));
-    I.fvpar[j] = vparN;
-    if (a.icr) I.fv[j] = make_float2(v1n, v2n);
+    if (!isfinite(vparN) || !isfinite(xN)) atomicOr(a.status, ST_NAN);
+    I.x[j] = xN;
+    I.vpar[j] = vparN;
     if (prologue) I.ffl[j] = make_float2(aea, ag);
     if (a.write_qind) I.qind[j] = qi;
     if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);

@@ -434,9 +434,9 @@ struct BcArgs {
   unsigned long long *lb_out, *ub_out;  // per tube escape counts
   Fields fields;
   int ena;  // 1: operate on the ENA segments (tube.eoff) instead of ions
-  // k_bc_mark: the slot arrays marked DEAD (co: mixed precision only)
+  // k_bc_mark: the slot arrays marked DEAD (x: mixed precision only)
   int32_t *qind_w;
-  int2 *co_w;
+  double *x_w;
 };
 
 __device__ __forceinline__ bool keep_slot(int q) {
@@ -503,7 +503,7 @@ __global__ void k_bc_mark(BcArgs a) {
         lb += (q[k] == BELOW);
         ub += (q[k] == ABOVE);
         a.qind_w[j] = DEAD;
-        if (a.co_w) a.co_w[j].x = DEAD;
+        if (a.x_w) a.x_w[j] = XDEAD;
       }
     }
   }
@@ -579,7 +579,9 @@ __global__ void k_bc_scatter(BcArgs a, const int64_t *nlive_old) {
       const int64_t src = toff + i, dst = toff + base + woff + wr;
       for (int f = 0; f < a.fields.n; ++f) {
         const Field &F = a.fields.f[f];
-        if (F.size == 8)
+        if (F.size == 16)
+          ((uint4 *)F.dst)[dst] = ((const uint4 *)F.src)[src];
+        else if (F.size == 8)
           ((uint64_t *)F.dst)[dst] = ((const uint64_t *)F.src)[src];
         else
           ((uint32_t *)F.dst)[dst] = ((const uint32_t *)F.src)[src];
@@ -664,10 +666,9 @@ __global__ void k_inject(InjArgs a) {
     int b2 = d3 ? vbin(c_vg.e2, c_vg.n2, v2) : 0;
     if (a.ion.vb) a.ion.vb[j] = ((b1 + 1) << 16) | (bp + 1);
     if (a.mixed) {
-      a.ion.co[j] = make_int2(
-          Q, __float_as_int((float)((qc - a.ct.qGL[g]) / (a.ct.qGH[g] - a.ct.qGL[g]))));
-      a.ion.fvpar[j] = (float)vpar;
-      a.ion.fv[j] = make_float2((float)v1, (float)v2);
+      a.ion.x[j] = (double)Q + (qc - a.ct.qGL[g]) / (a.ct.qGH[g] - a.ct.qGL[g]);
+      a.ion.vpar[j] = vpar;
+      a.ion.v12[j] = make_double2(v1, v2);
       a.ion.ffl[j] = make_float2((float)aea, (float)ag);
       a.ion.fqk4[j] = (float)qc;
     } else {
@@ -726,8 +727,8 @@ struct InitArgs {
 };
 
 // One new ion j of tube T in cell c at q with field-aligned velocity: the
-// per-ion state every path starts from (Qindk1, id, 2D bins; mixed: cell,
-// offset and FP32 velocities; FP64: meridian-plane position from the
+// per-ion state every path starts from (Qindk1, id, 2D bins; mixed: the
+// cell coordinate and the velocities; FP64: meridian-plane position from the
 // quartic root by Newton from the cell's linear guess, converged to FP64).
 __device__ __forceinline__ void store_ion(const Ions &I, const TubeD &T,
                                           const CellTables &ct, int64_t j,
@@ -744,9 +745,9 @@ __device__ __forceinline__ void store_ion(const Ions &I, const TubeD &T,
     I.vb[k] = ((b1 + 1) << 16) | (bp + 1);
   }
   if (mixed) {
-    I.co[k] = make_int2(c, __float_as_int((float)((q - qL) / (qH - qL))));
-    I.fvpar[k] = (float)vpar;
-    I.fv[k] = make_float2((float)v1, (float)v2);
+    I.x[k] = (double)c + (q - qL) / (qH - qL);
+    I.vpar[k] = vpar;
+    I.v12[k] = make_double2(v1, v2);
     I.fqk4[k] = (float)q;
   } else {
     const double fr = (q - qL) / (qH - qL);
@@ -902,11 +903,11 @@ __device__ __forceinline__ void convect_ions(const ConvArgs &a) {
     if (a.ion.qind[j] == DEAD) continue;
     double q, u_old;
     if (a.mixed) {
-      const int2 co = a.ion.co[j];
-      const int c = co.x;
-      if (c == DEAD) continue;
+      const double x = a.ion.x[j];
+      if (x < XDEAD_LIM) continue;
+      const int c = x_cell(x, T.nq);
       const int64_t g = T.coff + c;
-      const double o = (double)__int_as_float(co.y);
+      const double o = x - (double)c;
       q = a.ct.qGL[g] + o * (a.ct.qGH[g] - a.ct.qGL[g]);
       u_old = quartic_newton(q, ip_old, a.ct.uL[g] + o * (a.ct.uH[g] - a.ct.uL[g]), 4);
     } else {
@@ -918,8 +919,8 @@ __device__ __forceinline__ void convect_ions(const ConvArgs &a) {
     const double u_new = quartic_newton(q, ip_new, u_old, 6);
     const double f = sqrt(bnorm(q, u_new) / bnorm(q, u_old));
     if (a.mixed) {
-      const float2 v = a.ion.fv[j];
-      a.ion.fv[j] = make_float2((float)(f * (double)v.x), (float)(f * (double)v.y));
+      const double2 v = a.ion.v12[j];
+      a.ion.v12[j] = make_double2(f * v.x, f * v.y);
     } else {
       const double rr = u_new * RE, st = sqrt(u_new * ip_new), ctv = q * u_new * u_new;
       double rho = rr * st, z = rr * ctv;
@@ -971,8 +972,8 @@ namespace kaos {
 
 // ---------------------------------------------------------------------------
 // kaos_get_particles on the device: field-line q in FP64 from the stored
-// position (mixed: cell + FP32 offset; FP64: the meridian-plane point), the
-// velocities widened to FP64 and Qindk1, for the live ions only (slots
+// position (mixed: the cell coordinate; FP64: the meridian-plane point), the
+// FP64 velocities and Qindk1, for the live ions only (slots
 // converted to ENAs are skipped) in particle order.  Three passes: live
 // count per block, exclusive scan of the block counts, in-order write.
 constexpr int EXP_THREADS = 256, EXP_ITEMS = 8;  // 2048 ions per block
@@ -981,6 +982,7 @@ struct ExportArgs {
   Ions ion;
   int64_t off, nl;           // the tube's segment and live slots
   const double *qGL, *qGH;   // the tube's cell edges (mixed)
+  int nq;                    // the tube's cells (mixed)
   int mixed, nb;
   unsigned *blkcnt;
   unsigned long long *blkoff, *total;
@@ -1053,11 +1055,11 @@ __global__ void __launch_bounds__(EXP_THREADS) k_exp_write(ExportArgs a) {
       const int64_t o = (int64_t)(done + woff + __popc(bal & ((1u << l) - 1u)));
       double q, vp, v1, v2;
       if (a.mixed) {
-        const int2 co = a.ion.co[j];
-        const int c = co.x;
-        q = fma((double)__int_as_float(co.y), a.qGH[c] - a.qGL[c], a.qGL[c]);
-        vp = a.ion.fvpar[j];
-        const float2 v = a.ion.fv[j];
+        const double x = a.ion.x[j];
+        const int c = x_cell(x, a.nq);
+        q = fma(x - (double)c, a.qGH[c] - a.qGL[c], a.qGL[c]);
+        vp = a.ion.vpar[j];
+        const double2 v = a.ion.v12[j];
         v1 = v.x;
         v2 = v.y;
       } else {
