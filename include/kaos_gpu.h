@@ -301,6 +301,28 @@ int kaos_get_timing(kaos_handle *h, double *ms, int64_t *launches);
  * included. */
 int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches);
 
+/* Diagnostic sampler of the library's device random-number generators, for
+ * distribution tests; no counterpart in the reference (whose generators,
+ * gfortran's unseeded random_number behind GaussianRNGSub and
+ * PoissonRNGSub, _3_1_GaussianRNG.f90:27-37 and _3_2_PoissonRNG.f90:27-42,
+ * are not reproducible).  Draw i (i = 0 .. n-1) is evaluated on the device
+ * by the same function the kernels call and written to the host array out:
+ *   KAOS_SAMPLE_PHILOX  4 values: the Philox4x32-10 words of counter
+ *                       (id0 + i low, high, step, c3) and key `seed`;
+ *   KAOS_SAMPLE_GAUSS32 2 values: the FP32 Gaussian pair of the mixed
+ *                       push's heating kick for particle id0 + i at step;
+ *   KAOS_SAMPLE_GAUSS64 2 values: the FP64 Gaussian pair of the FP64 push's
+ *                       heating kick for particle id0 + i at step;
+ *   KAOS_SAMPLE_POISSON 1 value: the collision-count draw with mean
+ *                       `lambda` for cell id0 + i at master step `step`.
+ * out holds 4, 2, 2 or 1 doubles per draw; n <= 2^26. */
+#define KAOS_SAMPLE_PHILOX 0
+#define KAOS_SAMPLE_GAUSS32 1
+#define KAOS_SAMPLE_GAUSS64 2
+#define KAOS_SAMPLE_POISSON 3
+int kaos_sample_rng(int32_t kind, uint64_t seed, uint64_t id0, uint32_t step,
+                    uint32_t c3, double lambda, int64_t n, double *out);
+
 /* Run the computational steps from CUDA graphs (1) or launch every kernel
  * directly (0, default).  With graphs on, each kind of step (ordinary runs
  * of up to 8 steps, the step before a master step, the master step) is

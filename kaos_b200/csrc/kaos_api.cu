@@ -840,6 +840,45 @@ int launch_boundary_ena(kaos_handle *h) {
   return KAOS_OK;
 }
 
+// kaos_sample_rng: draw i of the chosen generator, evaluated by the device
+// functions the kernels call.
+struct SampleArgs {
+  int kind;
+  uint64_t seed, id0;
+  uint32_t step, c3;
+  double lambda;
+  int64_t n;
+  double *out;
+  uint32_t rk[20];  // Philox key schedule of the seed (as PushArgs.rk)
+};
+
+int sample_width(int kind) {
+  return kind == KAOS_SAMPLE_PHILOX ? 4 : (kind == KAOS_SAMPLE_POISSON ? 1 : 2);
+}
+
+__global__ void k_sample_rng(SampleArgs a) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t id = a.id0 + (uint64_t)i;
+    if (a.kind == KAOS_SAMPLE_PHILOX) {
+      const kaos_u32x4 w = kaos_philox((uint32_t)id, (uint32_t)(id >> 32), a.step, a.c3, a.seed);
+      for (int k = 0; k < 4; ++k) a.out[4 * i + k] = (double)w.v[k];
+    } else if (a.kind == KAOS_SAMPLE_GAUSS32) {
+      float g1, g2;
+      gauss2_mix(a.rk, id, a.step, g1, g2);
+      a.out[2 * i] = g1;
+      a.out[2 * i + 1] = g2;
+    } else if (a.kind == KAOS_SAMPLE_GAUSS64) {
+      double g1, g2;
+      gauss2_64(a.seed, id, a.step, KAOS_RNG_HEAT, g1, g2);
+      a.out[2 * i] = g1;
+      a.out[2 * i + 1] = g2;
+    } else {
+      a.out[i] = (double)poisson_draw(a.seed, (uint32_t)id, a.step, a.lambda);
+    }
+  }
+}
+
 __global__ void k_set_step(uint32_t *d, uint32_t v) { *d = v; }
 __global__ void k_next_step(uint32_t *d) { *d += 1u; }
 
@@ -1918,6 +1957,37 @@ int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches) {
   if (ms) *ms = h->push_ms;
   if (launches) *launches = h->npev;
   return KAOS_OK;
+}
+
+int kaos_sample_rng(int32_t kind, uint64_t seed, uint64_t id0, uint32_t step,
+                    uint32_t c3, double lambda, int64_t n, double *out) {
+  if (kind < KAOS_SAMPLE_PHILOX || kind > KAOS_SAMPLE_POISSON || n < 0 ||
+      n > ((int64_t)1 << 26) || (n > 0 && !out) ||
+      (kind == KAOS_SAMPLE_POISSON && !(lambda >= 0.0 && lambda <= 700.0)))
+    return KAOS_ERR_PARAM;
+  if (n == 0) return KAOS_OK;
+  const int per = sample_width(kind);
+  double *d = nullptr;
+  if (cudaMalloc(&d, (size_t)n * per * sizeof(double)) != cudaSuccess) return KAOS_ERR_CUDA;
+  SampleArgs a{};
+  a.kind = kind;
+  a.seed = seed;
+  a.id0 = id0;
+  a.step = step;
+  a.c3 = c3;
+  a.lambda = lambda;
+  a.n = n;
+  a.out = d;
+  for (int r = 0; r < 10; ++r) {  // Philox key schedule of the seed
+    a.rk[2 * r] = (uint32_t)seed + (uint32_t)r * KAOS_PHILOX_W0;
+    a.rk[2 * r + 1] = (uint32_t)(seed >> 32) + (uint32_t)r * KAOS_PHILOX_W1;
+  }
+  k_sample_rng<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 16), 256>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpy(out, d, (size_t)n * per * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? KAOS_OK : KAOS_ERR_CUDA;
 }
 
 void kaos_destroy(kaos_handle *h) {

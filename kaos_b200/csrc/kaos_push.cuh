@@ -337,16 +337,17 @@ __device__ __forceinline__ void heat(const PushArgs &a, uint32_t step,
 }
 
 // Philox4x32-10 (include/kaos_philox.h) with the key schedule, the same for
-// every particle, read from the kernel arguments: the same output words.
-__device__ __forceinline__ kaos_u32x4 philox_rk(const PushArgs &a, uint32_t c0,
+// every particle, read from the kernel arguments (rk: key words of round r
+// at rk[2r], rk[2r+1]): the same output words.
+__device__ __forceinline__ kaos_u32x4 philox_rk(const uint32_t (&rk)[20], uint32_t c0,
                                                 uint32_t c1, uint32_t c2,
                                                 uint32_t c3) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
     const uint64_t p0 = (uint64_t)KAOS_PHILOX_M0 * c0;
     const uint64_t p1 = (uint64_t)KAOS_PHILOX_M1 * c2;
-    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ a.rk[2 * r];
-    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ a.rk[2 * r + 1];
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ rk[2 * r];
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ rk[2 * r + 1];
     c1 = (uint32_t)p1;
     c3 = (uint32_t)p0;
     c0 = n0;
@@ -475,6 +476,26 @@ __device__ __forceinline__ float ex2f(float x) {
   return r;
 }
 
+// The Gaussian pair of the mixed push's heating kick: Box-Muller
+// (GaussianRNGSub's transform, _3_1_GaussianRNG.f90:33, both branches) in
+// FP32 from the high 23 bits of Philox words 0 and 2 of the draw keyed by
+// (seed, particle id, step, heating stream), with the hardware logarithm,
+// reciprocal square root, sine and cosine.  Also evaluated by the
+// diagnostic sampler kaos_sample_rng.
+__device__ __forceinline__ void gauss2_mix(const uint32_t (&rk)[20], uint64_t id,
+                                           uint32_t step, float &g1, float &g2) {
+  const kaos_u32x4 w = philox_rk(rk, (uint32_t)id, (uint32_t)(id >> 32), step,
+                                 KAOS_RNG_HEAT << 24);
+  const float u1 = u01_bits(w.v[0]), u2 = u01_bits(w.v[2]);
+  // -2 ln u1 > 0; the hardware logarithm's absolute error (~2^-22) can give
+  // a tiny negative value for u1 just below 1
+  const float t = fmaxf(-1.38629436f * lg2f(u1), 1e-30f);
+  const float R = t * rsq(t);
+  const float ang = 6.2831853f * u2;
+  g1 = R * cosa(ang);
+  g2 = R * sina(ang);
+}
+
 // The stochastic WaveHeatingSub kick in the mixed push, in log form: the
 // product K_i x^(-c_i) (Om s)^(1/2) of heat() is one base-2 exponential,
 //   kick_i = K_i G_i 2^(-c_i log2(Om/Om0) + log2(Om |V||| / sum ds)/4 - pen),
@@ -503,16 +524,10 @@ __device__ __forceinline__ void heat32(const PushArgs &a, uint32_t step,
   const float lx = LOm + h1.x;
   const float e1 = ex2f(fmaf(-h0.z, lx, b));
   const float e2 = (h0.w == h0.z) ? e1 : ex2f(fmaf(-h0.w, lx, b));
-  kaos_u32x4 w = philox_rk(a, (uint32_t)id, (uint32_t)(id >> 32), step,
-                           KAOS_RNG_HEAT << 24);
-  const float u1 = u01_bits(w.v[0]), u2 = u01_bits(w.v[2]);
-  // -2 ln u1 > 0; the hardware logarithm's absolute error (~2^-22) can give
-  // a tiny negative value for u1 just below 1
-  const float t = fmaxf(-1.38629436f * lg2f(u1), 1e-30f);
-  const float R = t * rsq(t);
-  const float ang = 6.2831853f * u2;
-  dv1 = h0.x * e1 * R * cosa(ang);
-  dv2 = h0.y * e2 * R * sina(ang);
+  float G1, G2;
+  gauss2_mix(a.rk, id, step, G1, G2);
+  dv1 = h0.x * e1 * G1;
+  dv2 = h0.y * e2 * G2;
 }
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0 by Newton from u0 (the

@@ -335,6 +335,26 @@ __global__ void __launch_bounds__(256) k_cell_moments(TubeArgs a,
   }
 }
 
+// PoissonRNGSub (_3_2_PoissonRNG.f90:31-38): the number of uniforms whose
+// running product stays above exp(-mean), the uniforms drawn from the
+// Poisson stream keyed by (seed, cell Q, master step nn), two per Philox
+// draw (at most 1e5 uniforms).  Also evaluated by the diagnostic sampler
+// kaos_sample_rng.
+__device__ __forceinline__ int64_t poisson_draw(uint64_t seed, uint32_t Q,
+                                                uint32_t nn, double mean) {
+  const double e = exp(-mean);
+  double prod = 1.0;
+  int64_t k = -1;
+  uint32_t it = 0;
+  while (prod > e && it < 100000u) {
+    kaos_u32x4 w = kaos_philox(Q, nn, it >> 1, (KAOS_RNG_POIS << 24), seed);
+    prod *= (it & 1u) ? kaos_u01(w.v[2], w.v[3]) : kaos_u01(w.v[0], w.v[1]);
+    ++k;
+    ++it;
+  }
+  return k;
+}
+
 // Model-A collision counts of one master step (IonNeutralCollision
 // FrequencyASub _8_6_6_1_...:28-301) from the moments of k_cell_moments.
 // One block per tube.
@@ -388,17 +408,7 @@ __global__ void k_collision_counts(TubeArgs a) {
       double vrel = sqrt(dx * dx + dy * dy + dz * dz);
       if (sigma != 0.0) {
         double mean = c.nsnormCNeut[g] * sigma * vrel * a.h;
-        // PoissonRNGSub (_3_2_PoissonRNG.f90:31-38): product of uniforms
-        double e = exp(-mean), prod = 1.0;
-        int64_t k = -1;
-        uint32_t it = 0;
-        while (prod > e && it < 100000u) {
-          kaos_u32x4 w = kaos_philox((uint32_t)Q, nn, it >> 1, (KAOS_RNG_POIS << 24), a.seed);
-          prod *= (it & 1u) ? kaos_u01(w.v[2], w.v[3]) : kaos_u01(w.v[0], w.v[1]);
-          ++k;
-          ++it;
-        }
-        nu = (double)k;
+        nu = (double)poisson_draw(a.seed, (uint32_t)Q, nn, mean);
         double cnt = (double)a.acc.cnt[g];
         if (nu > cnt) nu = cnt;
       }

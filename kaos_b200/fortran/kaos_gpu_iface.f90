@@ -298,6 +298,19 @@ module kaos_gpu_iface
       type(c_ptr), value :: d_moments, d_counts, stream
     end function kaos_moments_noalloc
 
+    ! diagnostic sampler of the device generators; out: host array of
+    ! 4 (Philox words), 2 (Gaussian pairs) or 1 (Poisson) doubles per draw
+    integer(c_int) function kaos_sample_rng(kind, seed, id0, step, c3, lambda, &
+        n, out) bind(C, name="kaos_sample_rng")
+      import :: c_int, c_int32_t, c_int64_t, c_double
+      integer(c_int32_t), value :: kind
+      integer(c_int64_t), value :: seed, id0
+      integer(c_int32_t), value :: step, c3
+      real(c_double), value :: lambda
+      integer(c_int64_t), value :: n
+      real(c_double), intent(out) :: out(*)
+    end function kaos_sample_rng
+
     type(c_ptr) function kaos_version() bind(C, name="kaos_version")
       import :: c_ptr
     end function kaos_version

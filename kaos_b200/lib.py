@@ -30,8 +30,12 @@ EXPORTS = [
     "kaos_version", "kaos_get_push_timing", "kaos_moments_noalloc",
     "kaos_get_launch", "kaos_set_ena_grid", "kaos_init_particles",
     "kaos_set_reduce", "kaos_set_rank", "kaos_set_id_base", "kaos_update_tube",
-    "kaos_get_moments_all",
+    "kaos_get_moments_all", "kaos_sample_rng",
 ]
+
+# kaos_sample_rng kinds and values per draw
+SAMPLE_PHILOX, SAMPLE_GAUSS32, SAMPLE_GAUSS64, SAMPLE_POISSON = 0, 1, 2, 3
+_SAMPLE_WIDTH = {0: 4, 1: 2, 2: 2, 3: 1}
 
 # int fn(void *ctx, uint32_t *buf, int64_t count, void *stream)
 REDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)
@@ -71,6 +75,8 @@ def load(path: str = LIBPATH):
     L.kaos_get_push_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
     L.kaos_moments_noalloc.argtypes = [vp, vp, i32, vp, vp, C.c_double, vp, vp,
                                         vp, vp, i64, vp, vp, vp]
+    L.kaos_sample_rng.argtypes = [i32, C.c_uint64, C.c_uint64, C.c_uint32,
+                                  C.c_uint32, C.c_double, i64, vp]
     L.kaos_set_graph.argtypes = [vp, i32]
     L.kaos_set_launch.argtypes = [vp, i32, i32]
     L.kaos_get_launch.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
@@ -91,6 +97,18 @@ def load(path: str = LIBPATH):
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+def sample_rng(kind, n, seed=1, id0=0, step=0, c3=0, lam=0.0):
+    """Draws of the device random-number generators (kaos_sample_rng):
+    array [n, width] (width 4 Philox words, 2 Gaussians, 1 Poisson count)."""
+    w = _SAMPLE_WIDTH[kind]
+    out = np.zeros((n, w))
+    rc = load().kaos_sample_rng(int(kind), int(seed), int(id0), int(step), int(c3),
+                                float(lam), int(n), _p(out))
+    if rc != 0:
+        raise KaosError(f"kaos_sample_rng failed (status {rc})")
+    return out
 
 
 class Solver:

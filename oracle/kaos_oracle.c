@@ -1724,6 +1724,15 @@ void orc_get_boundary_ena(orc *o, int64_t *v) {
 }
 
 /* single quartic evaluation for known-answer tests */
+/* The words of Philox4x32-10 (include/kaos_philox.h, the generator the
+ * library and this checker share) for one counter and key: the hook of the
+ * known-answer test against the published Random123 vectors. */
+void orc_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                uint64_t key, uint32_t *out4) {
+  kaos_u32x4 w = kaos_philox(c0, c1, c2, c3, key);
+  for (int k = 0; k < 4; ++k) out4[k] = w.v[k];
+}
+
 void orc_quartic(double q, double p, double phi, double *out6) {
   double r, th, x, y, z;
   quartic(q, p, phi, &r, &th, &x, &y, &z);

@@ -66,6 +66,8 @@ def _open(path):
     L.orc_get_boundary.argtypes = [vp, vp]
     L.orc_get_boundary_ena.argtypes = [vp, vp]
     L.orc_quartic.argtypes = [C.c_double, C.c_double, C.c_double, vp]
+    u32 = C.c_uint32
+    L.orc_philox.argtypes = [u32, u32, u32, u32, C.c_uint64, vp]
     L.orc_filter.argtypes = [vp, vp, C.c_int, C.c_int]
     L.orc_destroy.argtypes = [vp]
     L.orc_ambipolar.argtypes = [vp, vp, vp]
@@ -213,6 +215,14 @@ def ops_get():
 def ops_weighted(counts):
     """Weighted sum of one phase's {class: count}."""
     return sum(w * counts[c] for c, w in zip(OPS_CLASSES, OPS_WEIGHTS))
+
+
+def philox(counter, key):
+    """Philox4x32-10 words of a 4-word counter and a 64-bit key (low word
+    first), from the shared generator header."""
+    out = np.zeros(4, dtype=np.uint32)
+    lib().orc_philox(*[int(c) for c in counter], int(key), out.ctypes.data)
+    return out
 
 
 def quartic(q, p, phi=np.pi / 2):

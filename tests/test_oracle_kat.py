@@ -17,6 +17,7 @@ from kaos_b200 import grids
 from kaos_b200.model_input import (KAOS_M0, KAOS_M1PAR, KAOS_M1PERP1,
                                    KAOS_M2PAR, KAOS_M2PERP1, KAOS_NQ, KB, RE,
                                    ModelInput)
+from oracle import oracle as orc
 from oracle.oracle import Oracle, build, moment_filter, quartic
 
 
@@ -372,3 +373,23 @@ def test_convection_keeps_q_mu_and_vpar():
     r = np.hypot(p1["rho"], p1["z"])
     np.testing.assert_allclose(r / (p1["rho"] / r) ** 2 / RE, 4.05, rtol=1e-12)
     assert np.all(np.sign(p1["vperp1"]) == np.sign(p0["vperp1"]))
+
+
+# Published known-answer vectors of Philox4x32-10 (Salmon, Moraes, Dror,
+# Shaw, SC'11; Random123 distribution): counter (4 words), key (2 words),
+# output (4 words).
+PHILOX_KAT = [
+    ((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+    ((0xffffffff,) * 4, (0xffffffff, 0xffffffff),
+     (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+    ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+     (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1)),
+]
+
+
+@pytest.mark.parametrize("ctr,key,want", PHILOX_KAT)
+def test_philox_known_answers(ctr, key, want):
+    """The shared generator header (include/kaos_philox.h) against the
+    published Philox4x32-10 vectors."""
+    got = orc.philox(ctr, key[0] | (key[1] << 32))
+    assert [int(x) for x in got] == list(want)
