@@ -5,8 +5,9 @@ Workload (one line per run, rank 0 prints JSON): the precision A/B tube --
 L = 4 dipole flux tube from 1000 km to |q| = 1e-3, 256 cells, 3D velocity grid
 48x48x64 (geometric), 1e7 O+ macro-ions (seeded synthetic Maxwellian,
 T = 0.3 eV, n0 = 1e10 m^-3, H = 300 km), wave heating on (chi = 1.7,
-1e-3 eV/s at the base), dt = 0.005 s, master step every 50 steps (boundary
-removal/injection, ambipolar field, counts and moments).
+1e-3 eV/s at the base), ion-neutral collisions on, dt = 0.005 s, master
+step every 10 steps (boundary removal/injection, ambipolar field, counts and
+moments), so that the timed window holds whole master intervals.
 
 A "step" is one computational step of every particle of the tube.  The
 metric is particle-steps/s (higher is better).  `value` is the mixed-
@@ -36,6 +37,15 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s, mixed-prec vs FP64 on 1 B200, at stated moment error"
 N_PART = 10_000_000
+# master-step cadence of the timed runs (the reference's own cadence, the
+# lower-boundary cell transit time over h, is ~2000 steps on this tube)
+NDATFAC = 10
+# the per-moment error runs: the configuration's 500 steps
+ERR_STEPS = 500
+# algorithmic bytes per ion-step frozen for the mixed path when its state
+# was FP32 (cell + FP32 offset, FP32 velocities and fields, 20 B read + 20 B
+# written + 8 B of fields)
+FROZEN_MIXED_BYTES = 48
 
 # F_alg: FP64 flop-equivalents of one ion push-step of the reference
 # formulation on this tube, counted by the op-counting build of the oracle
@@ -96,8 +106,8 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def build_workload(precision, n_part=N_PART, heating=True, collisions=False,
-                   ndatfac=50):
+def build_workload(precision, n_part=N_PART, heating=True, collisions=True,
+                   ndatfac=NDATFAC):
     from kaos_b200 import grids
     mi, spec, tube, vg = grids.config_c2(n_particles=n_part, heating=heating,
                                          collisions=collisions,
@@ -108,9 +118,9 @@ def build_workload(precision, n_part=N_PART, heating=True, collisions=False,
 
 def bytes_per_particle_step(mixed, heating, collisions):
     """Algorithmic HBM bytes per ion per ordinary step (reads + writes)."""
-    if mixed:  # cell, offset, V||, Vperp1, Vperp2, AEA, AG (4 B each)
-        rd, wr = 7 * 4, (5 if heating else 3) * 4
-        if collisions:  # Qindk1 + q at k4 written for the charge exchange
+    if mixed:  # FP64 state: cell coordinate, V||, (Vperp1, Vperp2); FP32 AEA, AG
+        rd, wr = 8 + 8 + 16 + 8, 8 + 8 + (16 if heating else 0)
+        if collisions:  # Qindk1 + q at k4 (FP32) written for the charge exchange
             wr += 8
     else:      # rho, z, V||, Vperp1, Vperp2, AEA, AG (8 B) + Qindk1 (4 B)
         rd, wr = 7 * 8 + 4, (5 if heating else 3) * 8 + 4
@@ -142,7 +152,7 @@ def graph_warmup(args, ndatfac):
     return max(args.warmup, 2 * ndatfac)
 
 
-def run_ours(args, precision, graph=False, ndatfac=50, steps=None):
+def run_ours(args, precision, graph=False, ndatfac=NDATFAC, steps=None):
     from kaos_b200 import build as kbuild
     from kaos_b200.lib import Solver
     kbuild.build()
@@ -180,7 +190,8 @@ def run_large(args, precision, steps):
     CUDA graphs."""
     from kaos_b200 import grids
     from kaos_b200.lib import Solver
-    mi, spec, tube, vg = grids.config_c3(args.large_particles, precision=precision)
+    mi, spec, tube, vg = grids.config_c3(args.large_particles, precision=precision,
+                                         ndatfac=NDATFAC)
     s = Solver(mi, [tube], vg)
     s.init_particles(0, tube._counts, seed=20261203, **grids.C3_TAIL)
     s.set_graph(True)
@@ -204,7 +215,8 @@ def run_batched(args, precision, steps):
     graphs, the autotuner's launch shape."""
     from kaos_b200 import grids
     from kaos_b200.lib import Solver
-    mi, specs, tubes, vg = grids.config_c4(args.batched_tubes, precision=precision)
+    mi, specs, tubes, vg = grids.config_c4(args.batched_tubes, precision=precision,
+                                           ndatfac=NDATFAC)
     s = Solver(mi, tubes, vg)
     for k, t in enumerate(tubes):
         s.init_particles(k, t._counts, seed=20261203 + k)
@@ -233,7 +245,7 @@ def run_c5(args, precision, steps):
     from CUDA graphs except the master steps that apply a move."""
     from kaos_b200 import grids
     from kaos_b200.lib import Solver
-    mi, specs, tubes, vg, evg = grids.config_c5(precision=precision)
+    mi, specs, tubes, vg, evg = grids.config_c5(precision=precision, ndatfac=NDATFAC)
     s = Solver(mi, tubes, vg)
     s.set_ena_grid(evg)
     for k, t in enumerate(tubes):
@@ -251,7 +263,7 @@ def run_c5(args, precision, steps):
             s.step(nd)
             ms += s.timing()[0]
             for k in range(len(tubes)):  # E x B drift to the next L-shell
-                Ls[k] += grids.CONV_C5_DL
+                Ls[k] += grids.conv_c5_dl(nd, mi.h)
                 cur[k] = grids.moved_tube(specs[k], mi, cur[k], Ls[k])
                 s.update_tube(k, cur[k])
         return ms
@@ -268,19 +280,100 @@ def run_c5(args, precision, steps):
                 steps=nint * nd, launch=launch, entries=len(tubes))
 
 
-def mixed_moment_error(s32, s64):
-    """Norm-wise relative difference max|m32 - m64| / max|m64| per moment."""
+MOMENT_NAMES = ("M0", "M1par", "M1perp1", "M1perp2", "M2", "M2par", "M2perp1",
+                "M2perp2", "Nq", "EAmag", "nuPoi")
+
+
+def moment_ids():
     from kaos_b200 import model_input as M
-    names = {"M0": M.KAOS_M0, "M1par": M.KAOS_M1PAR, "M1perp1": M.KAOS_M1PERP1,
-             "M1perp2": M.KAOS_M1PERP2, "M2": M.KAOS_M2, "M2par": M.KAOS_M2PAR,
-             "M2perp1": M.KAOS_M2PERP1, "M2perp2": M.KAOS_M2PERP2, "Nq": M.KAOS_NQ,
-             "EAmag": M.KAOS_EAMAG, "nuPoi": M.KAOS_NUPOI}
+    return {"M0": M.KAOS_M0, "M1par": M.KAOS_M1PAR, "M1perp1": M.KAOS_M1PERP1,
+            "M1perp2": M.KAOS_M1PERP2, "M2": M.KAOS_M2, "M2par": M.KAOS_M2PAR,
+            "M2perp1": M.KAOS_M2PERP1, "M2perp2": M.KAOS_M2PERP2, "Nq": M.KAOS_NQ,
+            "EAmag": M.KAOS_EAMAG, "nuPoi": M.KAOS_NUPOI}
+
+
+def moment_errors(a, b):
+    """Norm-wise relative difference max|a - b| / max|b| per moment (a, b:
+    objects with .moments(selector))."""
     out = {}
-    for k, m in names.items():
-        a, b = s32.moments(m), s64.moments(m)
-        scale = float(np.max(np.abs(b)))
-        out[k] = float(np.max(np.abs(a - b)) / scale) if scale > 0 else 0.0
+    for k, m in moment_ids().items():
+        x, y = a.moments(m), b.moments(m)
+        scale = float(np.max(np.abs(y)))
+        out[k] = float(np.max(np.abs(x - y)) / scale) if scale > 0 else 0.0
     return out
+
+
+def error_run(args, heating, collisions, n_part, with_oracle=False):
+    """The mixed path against the FP64 path (and, on a small sample, the
+    FP64 oracle) over the configuration's 500 steps from the same ions and
+    random streams: the error of every moment at every master step from
+    step 100 on (maximum over those steps) and at the last one."""
+    from kaos_b200 import grids
+    from kaos_b200.lib import Solver
+    from kaos_b200.model_input import KAOS_PREC_FP64, KAOS_PREC_MIXED
+    runs = {}
+    init = None
+    for prec in (KAOS_PREC_FP64, KAOS_PREC_MIXED):
+        mi, spec, tube, vg = grids.config_c2(n_particles=n_part, heating=heating,
+                                             collisions=collisions, precision=prec,
+                                             ndatfac=NDATFAC)
+        init = grids.initial_particles(tube, spec, mi, seed=20261203)
+        s = Solver(mi, [tube], vg)
+        s.load(0, *init)
+        runs[prec] = s
+    orc = None
+    if with_oracle:
+        from oracle.oracle import Oracle
+        mi, spec, tube, vg = grids.config_c2(n_particles=n_part, heating=heating,
+                                             collisions=collisions,
+                                             precision=KAOS_PREC_FP64, ndatfac=NDATFAC)
+        orc = Oracle(mi, tube, vg)
+        orc.load(*init)
+    worst = {k: 0.0 for k in MOMENT_NAMES}
+    worst_o = {k: 0.0 for k in MOMENT_NAMES}
+    done, last, last_o = 0, None, None
+    while done < ERR_STEPS:
+        k = NDATFAC if done else 1
+        k = min(k, ERR_STEPS - done)
+        for s in runs.values():
+            s.step(k)
+        if orc is not None:
+            orc.step(k)
+        done += k
+        if done < 100 or done % NDATFAC:
+            continue
+        last = moment_errors(runs[KAOS_PREC_MIXED], runs[KAOS_PREC_FP64])
+        worst = {m: max(worst[m], last[m]) for m in MOMENT_NAMES}
+        if orc is not None:
+            last_o = moment_errors(runs[KAOS_PREC_MIXED], orc)
+            worst_o = {m: max(worst_o[m], last_o[m]) for m in MOMENT_NAMES}
+    for s in runs.values():
+        s.close()
+    out = {"ions": n_part, "steps": ERR_STEPS, "master_every": NDATFAC,
+           "vs_fp64_max_over_master_steps_from_100": worst,
+           "vs_fp64_at_last_step": last}
+    if orc is not None:
+        out["vs_oracle_max_over_master_steps_from_100"] = worst_o
+        out["vs_oracle_at_last_step"] = last_o
+    return out
+
+
+def moment_error_block(args):
+    """Every moment of the mixed path against the FP64 path on the full
+    tube (1e7 ions), with heating and collisions on (the timed workload) and
+    off, and against the FP64 oracle on a 2e4-ion sample of the tube."""
+    on = error_run(args, True, True, args.particles)
+    off = error_run(args, False, False, args.particles)
+    orc = error_run(args, True, True, 20000, with_oracle=True)
+    def mx(d):
+        return max(d.values())
+    return {"heating_collisions_on": on, "heating_collisions_off": off,
+            "oracle_sample": orc,
+            "max_vs_fp64_on": mx(on["vs_fp64_max_over_master_steps_from_100"]),
+            "max_vs_fp64_off": mx(off["vs_fp64_max_over_master_steps_from_100"]),
+            "max_vs_oracle_sample": mx(orc["vs_oracle_max_over_master_steps_from_100"]),
+            "definition": "max over cells |m_mixed - m_ref| / max over cells |m_ref|, "
+                          "per moment, at every master step from step 100 to 500"}
 
 
 def run_e2e(args, precision, launch):
@@ -333,28 +426,96 @@ def run_e2e(args, precision, launch):
                            "state": 1e3 * (t3 - t2)})
 
 
-def cpu_baseline(args, sample_particles=20000, sample_steps=5):
+def workload_config(args, n_ions):
+    """The `config` object of both arms' lines (same workload)."""
+    return {"workload": "precision A/B tube: L=4, 256 cells, 3D grid 48x48x64, "
+                        f"{int(n_ions)} O+ per GPU, heating "
+                        f"{'off' if args.no_heating else 'on'}, collisions "
+                        f"{'on' if args.collisions else 'off'}, dt 5 ms, "
+                        f"master step every {NDATFAC} steps",
+            "master_step_every": NDATFAC,
+            "l2": "inputs > L2 (particle arrays 1-1.5 GB); no flush",
+            "parallelism": f"tube per GPU x{args.gpus}"}
+
+
+def cpu_baseline(args, sample_particles=20000, sample_steps=NDATFAC):
     """The CPU oracle (FP64 restatement of the reference loop, direct
-    binning) on a bounded sample of the same workload, one host thread."""
+    binning) on a bounded sample of the same workload, one host thread, over
+    one whole master interval; beside it the literal reference algorithm
+    (O(Nq Nv Np) counting, IonParticleCountsSub _8_3_1_...:311-357) on the
+    plain FP64 configuration, all host cores."""
     from oracle.oracle import Oracle
     from kaos_b200 import grids
     from kaos_b200.model_input import KAOS_PREC_FP64
     mi, spec, tube, vg = grids.config_c2(n_particles=sample_particles,
                                          heating=not args.no_heating,
                                          collisions=args.collisions,
-                                         precision=KAOS_PREC_FP64)
+                                         precision=KAOS_PREC_FP64, ndatfac=NDATFAC)
     q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=20261203)
     o = Oracle(mi, tube, vg)
     o.load(q, vpar, v1, v2)
-    o.step(1)
+    o.step(NDATFAC)
     t0 = time.perf_counter()
     o.step(sample_steps)
     dt = time.perf_counter() - t0
     n, _ = o.count()
-    return dict(value=n * sample_steps / dt, unit="particle-steps/s", cores=1,
-                kind="port",
-                sample=f"{n} O+ of the same tube x {sample_steps} steps "
-                       "(oracle, direct binning, 1 thread)")
+    out = dict(value=n * sample_steps / dt, unit="particle-steps/s", cores=1,
+               kind="port",
+               sample=f"{n} O+ of the same tube x {sample_steps} steps holding one "
+                      "master step (oracle, direct binning, 1 thread)")
+    out["literal_c1"] = literal_baseline()
+    return out
+
+
+def _literal_worker(job, barrier, out):
+    """One host core: the oracle with the reference's literal counting loops
+    on its own sample of the plain FP64 configuration (master step every 20
+    steps), timed over one master interval."""
+    seed, npart, steps = job
+    from oracle.oracle import Oracle
+    from kaos_b200 import grids
+    mi, spec, tube, vg = grids.config_c1(n_particles=npart)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=seed)
+    o = Oracle(mi, tube, vg)
+    o.set_literal(True)
+    o.load(q, vpar, v1, v2)
+    o.step(1)
+    n0, _ = o.count()
+    barrier.wait()
+    t0 = time.time()
+    o.step(steps)
+    t1 = time.time()
+    n1, _ = o.count()
+    out.put((0.5 * (n0 + n1) * steps, t0, t1))
+
+
+def parallel_oracle(worker, jobs):
+    """Run one oracle job per host core (spawned processes, started
+    together); all particle-steps / the span from the first start to the
+    last end."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    barrier, out = ctx.Barrier(len(jobs)), ctx.Queue()
+    procs = [ctx.Process(target=worker, args=(j, barrier, out)) for j in jobs]
+    for p in procs:
+        p.start()
+    res = [out.get(timeout=900) for _ in procs]
+    for p in procs:
+        p.join()
+    work = sum(r[0] for r in res)
+    span = max(r[2] for r in res) - min(r[1] for r in res)
+    return work / span, span
+
+
+def literal_baseline(npart=10000, steps=20):
+    cores = len(os.sched_getaffinity(0))
+    jobs = [(20261203 + k, npart, steps) for k in range(cores)]
+    v, span = parallel_oracle(_literal_worker, jobs)
+    return {"value": v, "unit": "particle-steps/s", "cores": cores,
+            "kind": "port", "algorithm": "literal O(Nq Nv Np) counting",
+            "sample": f"plain FP64 configuration (L=4, 128 cells, 2D grid 64x32): "
+                      f"{cores} processes x {npart} O+ x {steps} steps (steps 2-21, "
+                      "master step at 20)", "span_s": span}
 
 
 def _reference_worker(job, barrier, out):
@@ -366,7 +527,7 @@ def _reference_worker(job, barrier, out):
     from kaos_b200.model_input import KAOS_PREC_FP64
     mi, spec, tube, vg = grids.config_c2(n_particles=npart, heating=heating,
                                          collisions=collisions,
-                                         precision=KAOS_PREC_FP64)
+                                         precision=KAOS_PREC_FP64, ndatfac=NDATFAC)
     q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=seed)
     o = Oracle(mi, tube, vg)
     o.load(q, vpar, v1, v2)
@@ -384,9 +545,8 @@ def reference_arm(args):
     """--impl reference: the CPU restatement of the reference loop (the
     reference itself is Fortran+MPI and cannot be built in this image) on
     every host core: one process per core, each advancing its own bounded
-    sample of the workload; throughput = all particle-steps / the span from
-    the first start to the last end."""
-    import multiprocessing as mp
+    sample of the workload over the same steps and cadence; throughput =
+    all particle-steps / the span from the first start to the last end."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
@@ -394,31 +554,20 @@ def reference_arm(args):
     cores = len(os.sched_getaffinity(0))
     jobs = [(20261203 + k, npart, args.warmup, args.steps, not args.no_heating,
              args.collisions) for k in range(cores)]
-    ctx = mp.get_context("spawn")
-    barrier, out = ctx.Barrier(cores), ctx.Queue()
-    procs = [ctx.Process(target=_reference_worker, args=(j, barrier, out)) for j in jobs]
-    for p in procs:
-        p.start()
-    res = [out.get(timeout=900) for _ in procs]
-    for p in procs:
-        p.join()
-    work = sum(r[0] for r in res)
-    span = max(r[2] for r in res) - min(r[1] for r in res)
-    v = work / span
+    v, span = parallel_oracle(_reference_worker, jobs)
     return {
         "impl": "reference", "metric": METRIC, "value": v,
         "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * span / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"precision A/B tube, L=4, 256 cells, 48x48x64, "
-                               f"{cores} x {npart} O+ samples (of 1e7), heating "
-                               f"{'off' if args.no_heating else 'on'}, collisions "
-                               f"{'on' if args.collisions else 'off'}, dt 5 ms"},
+        "config": workload_config(args, N_PART),
         "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores,
                          "kind": "port",
-                         "sample": f"{cores} processes x {npart} O+ x {args.steps} steps, "
-                                   "oracle FP64, direct binning"},
+                         "sample": f"{cores} processes x {npart} O+ of the tube x "
+                                   f"{args.steps} steps after {args.warmup}, oracle "
+                                   "FP64, direct binning (faster than the reference's "
+                                   "literal counting loops)"},
         "e2e": {"value": v, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -509,12 +658,12 @@ def main():
     r32 = run_ours(args, KAOS_PREC_MIXED)
     torch.cuda.synchronize()
     stop.set()
-    # error of every moment of the mixed path against the FP64 path (same
-    # particles, same random streams, last master step)
-    moment_error = mixed_moment_error(r32["solver"], r64["solver"]) if full else None
     if full:
         r64["solver"].close()
     r32["solver"].close()
+    # error of every moment of the mixed path against the FP64 path and the
+    # FP64 oracle (same ions, same random streams), master steps 100-500
+    moment_error = moment_error_block(args) if full else None
     # the same steps replayed from CUDA graphs, and at cadence 1 (every step
     # a master step: removal/injection, fields, counts and moments each step)
     rg = rc1 = None
@@ -532,6 +681,7 @@ def main():
     value = world * r32["n"] * args.steps / (ms * 1e-3)
     mixed_bytes = bytes_per_particle_step(True, not args.no_heating, args.collisions)
     achieved = mixed_bytes * r32["n"] / (r32["push_ms"] * 1e-3) / 1e9
+    achieved_frozen = FROZEN_MIXED_BYTES * r32["n"] / (r32["push_ms"] * 1e-3) / 1e9
     peak, peak_kind = peaks()
     e2e = None
     if not args.skip_e2e and full:  # before the large tube's allocations
@@ -544,7 +694,7 @@ def main():
         large = {"workload": "large single tube: L=6, 512 cells 800 km to the equator, "
                              f"3D grid 64x64x96, {int(l32['n'])} O+ (90 % 0.3 eV Maxwellian "
                              "+ 10 % kappa=3 5 eV tail, generated on the device), heating "
-                             "and collisions on, LB injection, dt 5 ms",
+                             "and collisions on, LB injection from the Maxwellian flux, dt 5 ms",
                  "steps": lsteps, "mixed": l32["value"] * world,
                  "mixed_ms_per_step": l32["ms"], "fp64": l64["value"] * world,
                  "fp64_ms_per_step": l64["ms"],
@@ -598,19 +748,15 @@ def main():
             "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic",
-            "config": {"workload": "precision A/B tube: L=4, 256 cells, 3D grid 48x48x64, "
-                                   f"{int(r32['n'])} O+ per GPU, heating "
-                                   f"{'off' if args.no_heating else 'on'}, collisions "
-                                   f"{'on' if args.collisions else 'off'}, dt 5 ms, "
-                                   "master step every 50 steps",
-                       "precision": "mixed (FP32 state + RK, FP64 quartic/renormalisation/reductions)",
-                       "l2": "inputs > L2 (particle arrays 0.5-1 GB); no flush",
-                       "push_launch": {"ions_per_item": r32["launch"][0],
-                                       "persistent": bool(r32["launch"][1] & 1),
-                                       "registers": (64, 80, 72)[(r32["launch"][1] >> 1) & 3],
-                                       "threads_per_block": 128 if r32["launch"][1] & 4 else 256,
-                                       "chosen_by": "fixed" if args.launch else "autotuner"},
-                       "parallelism": f"tube per GPU x{world}"},
+            "config": dict(workload_config(args, r32["n"]), **{
+                "precision": "mixed: FP32 arithmetic (forces, RK stages, heating) on FP64 "
+                             "state (cell coordinate, V||, Vperp pair), FP64 quartic / "
+                             "renormalisation / reductions",
+                "push_launch": {"ions_per_item": r32["launch"][0],
+                                "persistent": bool(r32["launch"][1] & 1),
+                                "registers": (64, 80, 72)[(r32["launch"][1] >> 1) & 3],
+                                "threads_per_block": 128 if r32["launch"][1] & 4 else 256,
+                                "chosen_by": "fixed" if args.launch else "autotuner"}}),
             "fp64": None if not full else {
                 "value": r64["value"] * world, "ms_per_step": r64["ms"] / args.steps,
                 "push_ms": r64["push_ms"]},
@@ -634,10 +780,18 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_push32 (mixed push)",
+                         "kernel": "k_push32 (mixed push), average over the timed "
+                                   "window's launches (ordinary and master steps)",
                          "bytes_per_particle": mixed_bytes,
+                         "frozen_bytes_per_particle": FROZEN_MIXED_BYTES,
+                         "achieved_at_frozen_bytes": achieved_frozen,
+                         "frac_at_frozen_bytes": achieved_frozen / peak,
+                         "bytes_note": "the mixed state is FP64 (cell coordinate, V||, "
+                                       "Vperp pair: 32 B read + 32 B written) so that every "
+                                       "moment matches the FP64 path; the frozen 48 B "
+                                       "counted the earlier FP32 state",
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                           "per ion on a 6e6-ion launch, scaled to this launch"},
+                                           "per ion of a 6e6-ion launch, scaled to this launch"},
             "cpu_baseline": cpu,
             "e2e": None if e2e is None else {
                 "value": e2e["value"] * world, "unit": "particle-steps/s",

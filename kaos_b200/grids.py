@@ -253,9 +253,10 @@ def config_c3(n_particles=100_000_000, precision=KAOS_PREC_MIXED, ndatfac=50):
     (|q| >= 1e-3), 3D grid 64x64x96, 1e8 O+ (90 % 0.3 eV Maxwellian core +
     10 % kappa = 3, 5 eV tail: C3_TAIL with kaos_init_particles), heating
     (chi 1.7, 1e-3 eV/s at the base) and O neutrals (1e14 m^-3, H 60 km) on,
-    LB injection, UB outflow removal, dt 0.005 s."""
+    LB injection with V|| drawn from the Maxwellian flux into the tube
+    (FLUXINJECTIONflag), UB outflow removal, dt 0.005 s."""
     mi = ModelInput(h=0.005, ndatfac=ndatfac, ION2VPERPflag=1, ICRflag=1,
-                    QEXCHANGEflag=1, precision=precision)
+                    QEXCHANGEflag=1, FLUXINJECTIONflag=1, precision=precision)
     spec = TubeSpec(L=6.0, nq=512, alt_lb=800e3, n_particles=n_particles,
                     q_ub=1e-3, heat_rate_eV_s=1e-3, chi=1.7, neut_n0=1e14,
                     neut_H=60e3)
@@ -323,9 +324,14 @@ def config_c5(ntubes=64, n_ions=20_000_000, precision=KAOS_PREC_MIXED,
     return mi, specs, tubes, vg, evg
 
 
-# L-shell change of a tube per master step under a 0.5 km/s E x B drift at
-# the equator (dL = v dt / RE, dt = 50 steps of 5 ms)
-CONV_C5_DL = 500.0 * 50 * 0.005 / RE
+def conv_c5_dl(ndatfac, h=0.005, v=500.0):
+    """L-shell change of a tube per master interval of ndatfac steps under
+    an E x B drift v [m/s] at the equator (dL = v ndatfac h / RE)."""
+    return v * ndatfac * h / RE
+
+
+# the change per master interval of 50 steps of 5 ms at 0.5 km/s
+CONV_C5_DL = conv_c5_dl(50)
 
 
 def config_escaping(neut_n0=0.0):

@@ -35,3 +35,13 @@ def test_species_ena_convection_config():
     moved = grids.moved_tube(specs[0], mi, tubes[0], specs[0].L + grids.CONV_C5_DL)
     np.testing.assert_array_equal(moved.qGL, tubes[0].qGL)
     assert moved.pG == specs[0].L + grids.CONV_C5_DL
+
+
+def test_large_tube_config():
+    mi, spec, tube, vg = grids.config_c3(n_particles=1_000_000)
+    assert tube.nq == 512 and spec.L == 6.0
+    assert (vg.n1, vg.n2, vg.npar) == (64, 64, 96)
+    # heating, collisions, and LB injection sampled from the Maxwellian flux
+    assert mi.ICRflag == 1 and mi.QEXCHANGEflag == 1 and mi.FLUXINJECTIONflag == 1
+    assert mi.LBCONDITIONflag == 1 and tube.nsnormCLB > 0
+    assert abs(grids.conv_c5_dl(10) * RE - 500.0 * 10 * 0.005) < 1e-9
