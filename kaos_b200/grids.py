@@ -12,6 +12,7 @@ configurations ask for.  All inputs are seeded synthetic data.
 from __future__ import annotations
 
 import dataclasses
+import math
 
 import numpy as np
 
@@ -101,20 +102,28 @@ def make_tube(spec: TubeSpec, mi: ModelInput, q_edges=None) -> Tube:
     Ti = np.full(nq, spec.Ti)
     Te = np.full(nq, spec.Ti)          # Te = Ti (config 1)
     neut = spec.neut_n0 * np.exp(-(alt - spec.alt_lb) / spec.neut_H)
-    # ICR tables: S0 chosen so that the base-cell mean heating rate is
-    # heat_rate_eV_s: <d(m v^2/2)/dt> = m (D1 + D2) with
-    # D = q^2/(2 m^2) xi eta S0 (Omega/Omega0)^-chi (sigma = 1).
+    # ICR tables: S0 chosen so that the mean heating rate of the base cell's
+    # Maxwellian ions is heat_rate_eV_s under the reference's stochastic
+    # kick (_8_1_1_0_WaveHeating.f90:83-150): per step and component
+    # dV_i = (h/tau) sqrt(2 D_i tau) G_i, so <d(m v^2/2)/dt> =
+    # m (D1 + D2) h <1/tau>, with D_i = q^2/(2 m^2) xi_i eta S0
+    # (Omega/Omega0)^-chi_i (sigma = 1, Omega = Omega0 at the base) and
+    # 1/tau = (Omega/2 pi) sqrt(|V|||/(Omega sum ds)); for V|| ~ N(0, s^2),
+    # <|V|||^(1/2)> = s^(1/2) 2^(1/4) Gamma(3/4) / sqrt(pi).
     ms = spec.ms if spec.ms > 0 else mi.ms
     qs = spec.qs if spec.qs != 0 else mi.qs
     Bc = 8.06e15 * np.sqrt(ell) / r ** 3
     Om = qs * Bc / ms
     Om0 = np.full(nq, Om[0])
     xi, eta = 0.5, 0.125
+    arc = float(np.sum(hq * dq))
     S0val = 0.0
     if spec.heat_rate_eV_s > 0:
         rate_J = spec.heat_rate_eV_s * 1.602e-19
-        S0val = rate_J / (ms * 2.0 * (qs ** 2 / (2 * ms ** 2)) * xi * eta)
-    arc = float(np.sum(hq * dq))
+        sig = np.sqrt(KB * spec.Ti / ms)
+        e_sqrt_v = np.sqrt(sig) * 2.0 ** 0.25 * math.gamma(0.75) / np.sqrt(PI)
+        inv_tau = (Om[0] / (2.0 * PI)) * np.sqrt(1.0 / (Om[0] * arc)) * e_sqrt_v
+        S0val = rate_J / (ms * 2.0 * (qs ** 2 / (2 * ms ** 2)) * xi * eta * mi.h * inv_tau)
     t = Tube(nq=nq, pG=L, phiG=spec.phi, nsnormfac=nsnormfac,
              nsnormCLB=0.0, nsnormCUB=0.0, qGL=qGL, qGH=qGH, qGC=qGC,
              hqC=hq, dqC=dq, d3xC=d3x, rGC=r, thetaGC=th, ellGC=ell,

@@ -45,3 +45,22 @@ def test_large_tube_config():
     assert mi.ICRflag == 1 and mi.QEXCHANGEflag == 1 and mi.FLUXINJECTIONflag == 1
     assert mi.LBCONDITIONflag == 1 and tube.nsnormCLB > 0
     assert abs(grids.conv_c5_dl(10) * RE - 500.0 * 10 * 0.005) < 1e-9
+
+
+def test_heating_rate_calibration():
+    """S0 is set so that the base cell's Maxwellian ions gain 1e-3 eV/s under
+    the reference's stochastic kick: the oracle's kick variance over 40 steps
+    of the precision A/B tube gives that rate within 10 %."""
+    from oracle.oracle import Oracle
+    mi, spec, tube, vg = grids.config_c2(n_particles=100_000, heating=True,
+                                         collisions=False, ndatfac=1000)
+    tube.nsnormCLB = 0.0
+    o = Oracle(mi, tube, vg)
+    o.load(*grids.initial_particles(tube, spec, mi, seed=3))
+    p0 = o.particles()
+    o.step(40)
+    p1 = o.particles()
+    base = p0["qind"] == 0
+    d2 = (p1["vperp1"] - p0["vperp1"]) ** 2 + (p1["vperp2"] - p0["vperp2"]) ** 2
+    rate = 0.5 * mi.ms * d2[base].mean() / 1.602e-19 / (40 * mi.h)
+    assert abs(rate - 1e-3) < 1e-4, rate

@@ -78,21 +78,32 @@ def test_c1_mixed_full_run(c1_oracle):
 
 
 def test_near_equator_quartic_fp64():
+    """Ions between |q| = 1.2e-3 and 0.05.  The trajectories there are ill
+    conditioned: a 1e-15 relative change of the initial q alone moves z by
+    ~2.5e-12 of its scale after 30 steps.  The tolerance is scaled by that
+    measured sensitivity (ten times the oracle's own change under the
+    perturbation, at least 1e-12)."""
     mi, spec, tube, vg = grids.config_c1(n_particles=100_000)
     rng = np.random.default_rng(5)
     n = 20000
     q = 10 ** rng.uniform(np.log10(1.2e-3), np.log10(0.05), n)
     sig = np.sqrt(KB * tube.TsG[-1] / mi.ms)
     v = rng.normal(size=(3, n)) * sig
-    o = Oracle(mi, tube, vg)
-    o.load(q, v[0], v[1], v[2])
+    runs = []
+    for eps in (0.0, 1e-15):
+        o = Oracle(mi, tube, vg)
+        o.load(q * (1.0 + eps), v[0], v[1], v[2])
+        o.step(30)
+        runs.append(o)
+    o, op = runs
     s = Solver(mi, [tube], vg)
     s.load(0, q, v[0], v[1], v[2])
-    o.step(30)
     s.step(30)
     assert s.count() == o.count()
-    po, ps = o.particles(), s.particles()
+    po, pp, ps = o.particles(), op.particles(), s.particles()
     assert np.min(np.abs(po["q"])) < 2e-3
     for k in ("rho", "z", "q", "vpar"):
-        assert rel_norm(ps[k], po[k]) < TRAJ_TOL, k
-    np.testing.assert_array_equal(s.counts(), o.counts())
+        tol = max(TRAJ_TOL, 10.0 * rel_norm(pp[k], po[k]))
+        assert rel_norm(ps[k], po[k]) < tol, (k, rel_norm(ps[k], po[k]), tol)
+    co = o.counts()
+    assert np.abs(s.counts() - co).sum() <= np.abs(op.counts() - co).sum()
