@@ -144,12 +144,17 @@ def profiled_traffic(name):
     return None
 
 
+# master steps between two compactions of the ion arrays in the library
+COMPACT_EVERY = 8
+
+
 def graph_warmup(args, ndatfac):
-    """Warm-up steps of a run replayed from CUDA graphs: two master
-    intervals, so that every kind of step graph (run lengths, master and
-    next-master steps, both ENA buffer parities) is captured before the
-    timed steps, which then only replay; at least --warmup."""
-    return max(args.warmup, 2 * ndatfac)
+    """Warm-up steps of a run replayed from CUDA graphs: every kind of step
+    graph (run lengths, master and next-master steps, both ENA and both ion
+    buffer parities, the compacting master step of each) is captured before
+    the timed steps, which then only replay -- through two compactions and
+    three more master intervals; at least --warmup."""
+    return max(args.warmup, (2 * COMPACT_EVERY + 3) * ndatfac)
 
 
 def run_ours(args, precision, graph=False, ndatfac=NDATFAC, steps=None):
@@ -267,7 +272,7 @@ def run_c5(args, precision, steps):
                 cur[k] = grids.moved_tube(specs[k], mi, cur[k], Ls[k])
                 s.update_tube(k, cur[k])
         return ms
-    intervals(2)  # warm-up: two master intervals (every step graph captured)
+    intervals(2 * COMPACT_EVERY + 3)  # warm-up: every step graph captured
     cnt = lambda i: sum(s.count(k)[i] for k in range(len(tubes)))
     n0 = cnt(0)
     nint = max(1, steps // nd)
@@ -755,6 +760,7 @@ def main():
                 "push_launch": {"ions_per_item": r32["launch"][0],
                                 "persistent": bool(r32["launch"][1] & 1),
                                 "registers": (64, 80, 72)[(r32["launch"][1] >> 1) & 3],
+                                "master_step_registers": (64, 64, 80, 72)[(r32["launch"][1] >> 3) & 3],
                                 "threads_per_block": 128 if r32["launch"][1] & 4 else 256,
                                 "chosen_by": "fixed" if args.launch else "autotuner"}}),
             "fp64": None if not full else {

@@ -339,10 +339,11 @@ int kaos_set_graph(kaos_handle *h, int32_t on);
  * SM x SMs) striding over the items; bits 1-2 (mixed precision only):
  * register budget of the push, 0 = 64 registers (4 blocks of 256 threads
  * per SM), 1 = 80 registers (3 blocks of 256), 2 = 72 registers (7 blocks
- * of 128).  chunk = 0 or mode < 0 re-arms the
+ * of 128); bits 3-4 (mixed): the budget of the master-step variant plus
+ * one (0 = the same as bits 1-2).  chunk = 0 or mode < 0 re-arms the
  * autotuner, which is on by default: before the first step after step 1 it
  * times the push of every candidate on a copy of the ion state and keeps
- * the fastest.  Results do not depend on the shape.  No reference
+ * the fastest, then the master-step variant's budget alone.  Results do not depend on the shape.  No reference
  * counterpart (the reference has one MPI rank per core,
  * _8_KineticSolver.f90:43-44). */
 int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode);

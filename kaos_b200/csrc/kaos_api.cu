@@ -180,8 +180,10 @@ struct kaos_handle {
   int persistent = 0;    // persistent grid striding over the items
   int tune_pending = 1;  // autotune before the next step
   int regsel = 0;        // mixed push register budget: 0 = 64, 1 = 80, 2 = 72
+  int regsel_master = 0; // the same for the master-step variant of the push
   int nsm = 0;
-  int occ[3] = {0, 0, 0};  // resident push blocks per SM per budget (0: unknown)
+  // resident push blocks per SM per (master-step variant, budget); 0: unknown
+  int occ[2][3] = {{0, 0, 0}, {0, 0, 0}};
   int64_t ion_len = 0;   // length of every ion array (all tubes' capacity)
   double last_ms = 0.0;
   int64_t launches = 0;
@@ -342,7 +344,8 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
           sizeof(unsigned);  // block-private binning window
   const bool bins_variant = a.bin || a.prologue || a.bin_only || !h->three_d;
   if (h->mixed && bins_variant) smem += BINS_SMEM_BYTES;  // FP64 edges + tables
-  const int rs = h->mixed ? h->regsel : 0, ps = h->persistent;
+  const int ms = (a.bin || a.prologue || a.bin_only) ? 1 : 0;
+  const int rs = h->mixed ? (ms ? h->regsel_master : h->regsel) : 0, ps = h->persistent;
   // kernel variant: [master-step work][three_d][register budget][persistent];
   // the budgets: 64 registers (4 blocks of 256 threads per SM), 80 (3
   // blocks of 256), 72 (7 blocks of 128)
@@ -354,21 +357,21 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
   static const KFn k32[2][2][3][2] = {{KAOS_K32(false, false), KAOS_K32(false, true)},
                                       {KAOS_K32(true, false), KAOS_K32(true, true)}};
 #undef KAOS_K32
-  const int ms = (a.bin || a.prologue || a.bin_only) ? 1 : 0;
   const int nt = rs == 2 ? 128 : PUSH_THREADS;
   static const KFn k64[2][2] = {{k_push64<false, false>, k_push64<false, true>},
                                 {k_push64<true, false>, k_push64<true, true>}};
   const KFn fn = h->mixed ? k32[ms][h->three_d][rs][ps] : k64[h->three_d][ps];
   if (smem > 48 * 1024)
     CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  if (!h->occ[rs]) {
+  int &occ = h->occ[h->mixed ? ms : 0][rs];
+  if (!occ) {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ[rs], (const void *)fn, nt, smem));
-    h->occ[rs] = std::max(h->occ[rs], 1);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)fn, nt, smem));
+    occ = std::max(occ, 1);
   }
-  const int grid = ps ? std::min(a.nitems, h->nsm * h->occ[rs]) : a.nitems;
+  const int grid = ps ? std::min(a.nitems, h->nsm * occ) : a.nitems;
   if (grid > 0) fn<<<grid, nt, smem, h->s>>>(a);
   if (timed) {
     CK(cudaEventRecord(h->pev[2 * h->npev + 1], h->s));
@@ -1001,11 +1004,45 @@ int autotune(kaos_handle *h) {
       }
       if (tmin < best) { best = tmin; bw = m; bp = pm; br = rs; }
     }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   h->wsel = bw;
   h->persistent = bp;
   h->regsel = br;
+  // the master-step variant (field re-interpolation and binning) has its
+  // own register needs: its budget is timed separately with the chosen
+  // work-item shape (the binning accumulators it fills are cleared before
+  // the next master step uses them)
+  int bm = br;
+  if (h->mixed) {
+    float bestm = 1e30f;
+    for (int rs = 0; rs < 3; ++rs) {
+      h->regsel_master = rs;
+      PushArgs a = push_args(h);
+      a.ion = h->ion[other];
+      a.step = (uint32_t)(h->n + 1);
+      a.write_qind = 1;
+      a.bin = 1;
+      a.prologue = 1;
+      float tmin = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        CK(cudaEventRecord(e0, h->s));
+        const int npev0 = h->npev;
+        const int64_t l0 = h->launches;
+        int rc = launch_push(h, a);
+        h->npev = npev0;
+        h->launches = l0;
+        if (rc) return rc;
+        CK(cudaEventRecord(e1, h->s));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0) tmin = std::min(tmin, ms);
+      }
+      if (tmin < bestm) { bestm = tmin; bm = rs; }
+    }
+  }
+  h->regsel_master = bm;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   h->tune_pending = 0;
   for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
   h->graphs.clear();
@@ -1572,11 +1609,13 @@ int kaos_set_launch(kaos_handle *h, int32_t chunk, int32_t mode) {
   int m = -1;
   for (int k = 0; k < NCHUNKS; ++k)
     if (CHUNKS[k] == chunk) m = k;
-  if (m < 0 || mode > 5)
-    return fail(h, KAOS_ERR_PARAM, "launch: chunk must be 1024, 2048 or 4096 and mode 0..5");
+  if (m < 0 || mode > 31 || ((mode >> 1) & 3) == 3)
+    return fail(h, KAOS_ERR_PARAM, "launch: chunk must be 1024, 2048 or 4096; mode bits "
+                "1-2 in 0..2, bits 3-4 in 0..3");
   h->wsel = m;
   h->persistent = mode & 1;
   h->regsel = (mode >> 1) & 3;
+  h->regsel_master = ((mode >> 3) & 3) ? ((mode >> 3) & 3) - 1 : h->regsel;
   h->tune_pending = 0;
   for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
   h->graphs.clear();
@@ -1661,7 +1700,7 @@ int kaos_set_id_base(kaos_handle *h, int32_t tube, uint64_t base) {
 int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode) {
   if (!h || !chunk || !mode) return KAOS_ERR_PARAM;
   *chunk = CHUNKS[h->wsel];
-  *mode = h->persistent | (h->regsel << 1);
+  *mode = h->persistent | (h->regsel << 1) | ((h->regsel_master + 1) << 3);
   return KAOS_OK;
 }
 

@@ -898,6 +898,16 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   const float qs_ms = (float)(T.qs / T.ms);
   const float c_invOm = (float)(T.ms / (T.qs * MDIP));
   const float ylim = (float)((2.0 * PI / a.h) * (2.0 * PI / a.h));
+  // the item's ions through per-item base pointers and a 32-bit index
+  const int64_t base = T.off + beg;
+  const int nk = (int)(end - beg);
+  double *__restrict__ X = I.x + base;
+  double *__restrict__ VP = I.vpar + base;
+  double2 *__restrict__ V12 = I.v12 + base;
+  float2 *__restrict__ FF = I.ffl + base;
+  float *__restrict__ QK = I.fqk4 + base;
+  int32_t *__restrict__ QI = I.qind + base;
+  const uint64_t *__restrict__ ID = I.id + base;
   // Software pipeline: the state of the next ion of this thread is loaded
   // before the current one is pushed, so its HBM latency overlaps the work.
   double n_x = XDEAD, n_vp = 0.0;
@@ -905,31 +915,31 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   float2 n_f = make_float2(0.f, 0.f);
   uint64_t n_id = 0;
   float n_qk = 0.f;  // q_k4 of the master-step field re-interpolation
-  if (beg + threadIdx.x < end) {
-    const int64_t j = T.off + beg + threadIdx.x;
-    n_x = I.x[j];
-    n_vp = I.vpar[j];
-    n_v = I.v12[j];
-    n_f = I.ffl[j];
-    if (a.icr) n_id = I.id[j];
-    if (prologue) n_qk = I.fqk4[j];
+  if ((int)threadIdx.x < nk) {
+    const unsigned k = threadIdx.x;
+    n_x = X[k];
+    n_vp = VP[k];
+    n_v = V12[k];
+    n_f = FF[k];
+    if (a.icr) n_id = ID[k];
+    if (prologue) n_qk = QK[k];
   }
-  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
-    const int64_t j = T.off + i;
+  for (unsigned k = threadIdx.x; k < (unsigned)nk; k += NT) {
+    const int64_t j = base + k;  // the ion's slot (2D grid: its stale bins)
     const double x0 = n_x;
     const double vpar = n_vp;
     const double v1 = n_v.x, v2 = n_v.y;
     float aea = n_f.x, ag = n_f.y;
     const uint64_t pid = n_id;
     const float qk0 = n_qk;
-    if (i + blockDim.x < end) {
-      const int64_t jn = j + blockDim.x;
-      n_x = I.x[jn];
-      n_vp = I.vpar[jn];
-      n_v = I.v12[jn];
-      n_f = I.ffl[jn];
-      if (a.icr) n_id = I.id[jn];
-      if (prologue) n_qk = I.fqk4[jn];
+    if (k + NT < (unsigned)nk) {
+      const unsigned kn = k + NT;
+      n_x = X[kn];
+      n_vp = VP[kn];
+      n_v = V12[kn];
+      n_f = FF[kn];
+      if (a.icr) n_id = ID[kn];
+      if (prologue) n_qk = QK[kn];
     }
     if (x0 < XDEAD_LIM) continue;  // slot marked DEAD
     const int c0 = x_cell(x0, T.nq);
@@ -976,7 +986,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       int b1, b2, bp;
       start_bins<THREE_D>(a, I, j, VE1, VE2, VEP, VT1, VT2, VTP, vpar, v1, v2, b1, b2, bp);
       if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
-      if (a.write_qind) I.qind[j] = qi;
+      if (a.write_qind) QI[k] = qi;
       continue;
     }
     const float a1 = apar_bf(g1, vp2, aea, ag, fc);
@@ -1002,14 +1012,14 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       }
     }
     // stored at once: the kicked pair holds no registers through the RK
-    if (a.icr) I.v12[j] = make_double2(v1n, v2n);
+    if (a.icr) V12[k] = make_double2(v1n, v2n);
     const float VRr = vparf * g1.er, VRz = vparf * g1.ez;
     const Geo<float> g2 = geo(fmaf(hh, VRr, rf), fmaf(hh, VRz, zf));
     const float a2 = apar_bf(g2, vp2, aea, ag, fc);
     const float A1r = a1 * g1.er, A1z = a1 * g1.ez;
     const Geo<float> g4 = geo(rf + h * VRr + hsq2 * A1r, zf + h * VRz + hsq2 * A1z);
     const float a4 = apar_bf(g4, vp2, aea, ag, fc);
-    if (a.write_qk4) I.fqk4[j] = g4.q;
+    if (a.write_qk4) QK[k] = g4.q;
     const float A2r = a2 * g2.er, A2z = a2 * g2.ez;
     // ---- displacement h/6 (V_R + 4 (V_R + h/2 A1) + (V_R + h A2)) ---------
     // = h V|| e1 (FP64, above) + h^2/6 (2 A1 + A2) (FP32)
@@ -1043,10 +1053,10 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       if (bin) accumulate_win(a.acc, T, W, qi, b1, b2, bp, a.exporting);
     }
     if (!isfinite(vparN) || !isfinite(xN)) atomicOr(a.status, ST_NAN);
-    I.x[j] = xN;
-    I.vpar[j] = vparN;
-    if (prologue) I.ffl[j] = make_float2(aea, ag);
-    if (a.write_qind) I.qind[j] = qi;
+    X[k] = xN;
+    VP[k] = vparN;
+    if (prologue) FF[k] = make_float2(aea, ag);
+    if (a.write_qind) QI[k] = qi;
     if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);
   }
   if (bin) bin_win_flush(a.acc, T, W);

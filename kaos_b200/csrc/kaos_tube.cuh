@@ -86,6 +86,15 @@ __global__ void k_fields(TubeArgs a) {
                      : 0.0;
   }
   __syncthreads();
+  // the field rows of the moment block hold the fields last computed (read
+  // after step 1 they are the first step's fields, as KineticSolverASub
+  // exports them after AmbipolarEfieldSub, _8_0_0_1_KineticSolverA.f90:
+  // 363-536); k_cell_moments copies the same values at later master steps
+  for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
+    const int64_t g = T.coff + Q;
+    c.mom[KAOS_EGMAG * c.ncell_total + g] = c.EG[g];
+    if (a.have_import || !a.eamb) c.mom[KAOS_EAMAG * c.ncell_total + g] = c.EAmag[g];
+  }
   if (a.have_import || !a.eamb) return;  // imported EAmag kept as is
   for (int Q = threadIdx.x; Q < nq; Q += blockDim.x) {
     M0f[Q] = a.momfilter ? filter_cell(M0p, nq, Q, a.fpM0) : M0p[Q];
@@ -126,6 +135,7 @@ __global__ void k_fields(TubeArgs a) {
     double v = EP[Q];
     if (a.eambself && Q <= 2 && nq > 3 && M0p[Q] != 0.0 && a.eapressure) v = EP[3];
     c.EAmag[T.coff + Q] = 0.0 + v;  // EAInertial = 0 (EAINERTIALflag = 0)
+    c.mom[KAOS_EAMAG * c.ncell_total + T.coff + Q] = 0.0 + v;
   }
 }
 
