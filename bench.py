@@ -760,7 +760,9 @@ def main():
                 "push_launch": {"ions_per_item": r32["launch"][0],
                                 "persistent": bool(r32["launch"][1] & 1),
                                 "registers": (64, 80, 72)[(r32["launch"][1] >> 1) & 3],
-                                "master_step_registers": (64, 64, 80, 72)[(r32["launch"][1] >> 3) & 3],
+                                "master_step_registers":
+                                    ((64, 80, 72)[(r32["launch"][1] >> 1) & 3],
+                                     64, 80, 72)[(r32["launch"][1] >> 3) & 3],
                                 "threads_per_block": 128 if r32["launch"][1] & 4 else 256,
                                 "chosen_by": "fixed" if args.launch else "autotuner"}}),
             "fp64": None if not full else {

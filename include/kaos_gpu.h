@@ -396,7 +396,8 @@ int kaos_set_id_base(kaos_handle *h, int32_t tube, uint64_t base);
  */
 int kaos_update_tube(kaos_handle *h, int32_t tube, const kaos_tube_c *t);
 
-/* The launch shape in use (after autotuning). */
+/* The launch shape in use (after autotuning); mode bits 3-4 are 0 when
+ * the master-step variant uses the same register budget as the push. */
 int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode);
 
 /* Text of the last error on this handle (static storage; never NULL). */

@@ -1700,7 +1700,8 @@ int kaos_set_id_base(kaos_handle *h, int32_t tube, uint64_t base) {
 int kaos_get_launch(kaos_handle *h, int32_t *chunk, int32_t *mode) {
   if (!h || !chunk || !mode) return KAOS_ERR_PARAM;
   *chunk = CHUNKS[h->wsel];
-  *mode = h->persistent | (h->regsel << 1) | ((h->regsel_master + 1) << 3);
+  *mode = h->persistent | (h->regsel << 1) |
+          (h->regsel_master != h->regsel ? (h->regsel_master + 1) << 3 : 0);
   return KAOS_OK;
 }
 

@@ -989,7 +989,6 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       if (a.write_qind) QI[k] = qi;
       continue;
     }
-    const float a1 = apar_bf(g1, vp2, aea, ag, fc);
     double v1n = v1, v2n = v2;  // after the wave-heating kick
     if (a.icr && qi >= 0) {
       const float rr = (float)r;
@@ -1013,17 +1012,40 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     }
     // stored at once: the kicked pair holds no registers through the RK
     if (a.icr) V12[k] = make_double2(v1n, v2n);
+    // ---- the stage accelerations ----------------------------------------
+    // a|| = M + s C0 + ce1 AEA with the signed mirror term M (cos(theta) in
+    // place of s |cos|: smooth through the equator), the hemisphere sign s
+    // and the per-ion constant C0 = -|AG| + |AEA| (gravity and the unsigned
+    // ambipolar field; the cached fields do not change within a step).  The
+    // k2 and k4 points lie on the line x1 + ds e1 (|ds| = |V|| h| + ... is
+    // below ~300 m against a length scale r/3 > 2e6 m), so M there is
+    // M1 + dM/ds ds to a relative 1e-8 (1e-12 at the typical 10 m), below
+    // the FP32 rounding; with F = cos (2 + sin^2/ell) / (r sqrt(ell)),
+    // dF/ds = [s^2 c^2 (8 + 9 s^2/ell)/ell - (1 + c^2)(2 + s^2/ell)] / (ell r^2)
+    // (dr/ds = 2c/sqrt(ell), dtheta/ds = s/(r sqrt(ell)) along the dipole e).
+    const float il = g1.isl * g1.isl;  // 1/ell
+    const float sn2 = g1.st * g1.st, cs2 = g1.ct * g1.ct;
+    const float G2 = fmaf(sn2, il, 2.0f);
+    const float hm = fc.cm * 1.5f * vp2 * g1.ir;
+    const float M1 = hm * g1.ct * G2 * g1.isl;
+    const float dM = hm * g1.ir * il *
+                     fmaf(sn2 * cs2 * il, fmaf(9.0f * sn2, il, 8.0f), -(1.0f + cs2) * G2);
+    const float C0 = fc.ce2 * fabsf(aea) - fc.cg * fabsf(ag);
+    const float Ce = fc.ce1 * aea;
+    const float a1 = M1 + (g1.ct <= 0.0f ? -C0 : C0) + Ce;
     const float VRr = vparf * g1.er, VRz = vparf * g1.ez;
-    const Geo<float> g2 = geo(fmaf(hh, VRr, rf), fmaf(hh, VRz, zf));
-    const float a2 = apar_bf(g2, vp2, aea, ag, fc);
-    const float A1r = a1 * g1.er, A1z = a1 * g1.ez;
-    const Geo<float> g4 = geo(rf + h * VRr + hsq2 * A1r, zf + h * VRz + hsq2 * A1z);
-    const float a4 = apar_bf(g4, vp2, aea, ag, fc);
-    if (a.write_qk4) QK[k] = g4.q;
-    const float A2r = a2 * g2.er, A2z = a2 * g2.ez;
+    const float ds2 = hh * vparf, ds4 = fmaf(hsq2, a1, h * vparf);
+    const float z2 = fmaf(ds2, g1.ez, zf), z4 = fmaf(ds4, g1.ez, zf);
+    const float a2 = fmaf(dM, ds2, M1) + (z2 <= 0.0f ? -C0 : C0) + Ce;
+    const float a4 = fmaf(dM, ds4, M1) + (z4 <= 0.0f ? -C0 : C0) + Ce;
+    // q at the k4 point: dq/ds = -RE^2 sqrt(ell) / r^3 along e1
+    if (a.write_qk4)
+      QK[k] = fmaf(-(float)(RE * RE) * (g1.ell * g1.isl) * (g1.ir * g1.ir * g1.ir), ds4, g1.q);
     // ---- displacement h/6 (V_R + 4 (V_R + h/2 A1) + (V_R + h A2)) ---------
-    // = h V|| e1 (FP64, above) + h^2/6 (2 A1 + A2) (FP32)
-    const float ddr = hh6 * (2.0f * A1r + A2r), ddz = hh6 * (2.0f * A1z + A2z);
+    // = h V|| e1 (FP64, above) + h^2/6 (2 a1 + a2) e1 (FP32; the k2 point's
+    // direction differs from e1 by ~1e-6 rad, ~1e-10 m here)
+    const float ac = hh6 * (2.0f * a1 + a2);
+    const float ddr = ac * g1.er, ddz = ac * g1.ez;
     // ---- renormalisation in FP64: q of the new point --------------------
     const double xr = xr0 + (double)ddr, xz = xz0 + (double)ddz;
     const double r2 = xr * xr + xz * xz;

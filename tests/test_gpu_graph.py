@@ -95,7 +95,8 @@ def test_launch_shapes_bit_identical(mixed):
     ref = _run_shape(mixed, (2048, 0))
     shapes = [(1024, 1), (4096, 0), None]
     if mixed:
-        shapes += [(1024, 2), (4096, 3), (2048, 4), (1024, 5)]
+        # bits 3-4: the master-step variant's budget + 1 (64 with 80, 72 with 64)
+        shapes += [(1024, 2), (4096, 3), (2048, 4), (1024, 5), (2048, 2 | 8), (4096, 24)]
     for sh in shapes:
         o = _run_shape(mixed, sh)
         if sh is not None:
