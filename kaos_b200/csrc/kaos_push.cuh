@@ -132,7 +132,10 @@ __device__ __forceinline__ void accumulate_win(const Accum &acc, const TubeD &T,
     accumulate(acc, T, qi, b1, b2, bp, exporting);
     return;
   }
-  atomicAdd(W.s + wc, 1u);
+  // the cell count: one shared-memory atomic per distinct cell among the
+  // warp's ions (they mostly share one) instead of one per ion
+  const unsigned peers = __match_any_sync(__activemask(), wc);
+  if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(W.s + wc, (unsigned)__popc(peers));
   const bool d3 = c_vg.three_d;
   if (b1 < 0 || bp < 0 || (d3 && b2 < 0)) return;
   unsigned *mp = W.s + BIN_WIN, *m1 = mp + BIN_WIN * c_vg.npar,
@@ -422,14 +425,14 @@ __device__ __forceinline__ void field_prologue32(const ForceFlags &ff,
 }
 
 // Velocity-bin search of the mixed push from a lookup table: VTAB uniform
-// slots over the axis hold the bin of each slot's left end (built from the
-// FP32 edges), and a short walk over the FP64 edges finishes the search.
+// slots over the axis hold the bin of each slot's left end, and a short walk
+// over the FP64 edges finishes the search.
 // The walk establishes both edge conditions of vbin (v <= e[b+1], and
 // v > e[b] unless b = 0) in FP64, so the result equals vbin's on the FP64
 // edges whatever the table holds.
 constexpr int VTAB = 256;
 struct VBinTab {
-  float e0, iw;              // first edge, VTAB / (last edge - first edge)
+  double e0, iw;             // first edge, VTAB / (last edge - first edge)
   unsigned char t[VTAB];     // bin at each slot's left end (n <= 128)
 };
 // Dynamic shared memory of the mixed push's bin searches: alignment slack,
@@ -438,13 +441,13 @@ constexpr size_t BINS_SMEM_BYTES = 16 + 3 * (MAXV + 1) * sizeof(double) + 3 * si
 
 // All threads of the block; edges e[0..n] in shared memory already visible,
 // and the caller synchronises before the table is used.
-__device__ __forceinline__ void build_vbin_tab(VBinTab &T, const float *e, int n) {
+__device__ __forceinline__ void build_vbin_tab(VBinTab &T, const double *e, int n) {
   if (threadIdx.x == 0) {
     T.e0 = e[0];
-    T.iw = (float)VTAB / (e[n] - e[0]);
+    T.iw = (double)VTAB / (e[n] - e[0]);
   }
   for (int k = threadIdx.x; k < VTAB; k += blockDim.x) {
-    const float v = e[0] + (e[n] - e[0]) * ((float)k / (float)VTAB);
+    const double v = e[0] + (e[n] - e[0]) * ((double)k / (double)VTAB);
     T.t[k] = (unsigned char)max(vbin(e, n, v), 0);
   }
 }
@@ -452,7 +455,10 @@ __device__ __forceinline__ void build_vbin_tab(VBinTab &T, const float *e, int n
 __device__ __forceinline__ int vbin_tab(const VBinTab &T, const double *e, int n,
                                         double v) {
   if (!(v >= e[0] && v <= e[n])) return -1;
-  const int s = min(max((int)(((float)v - T.e0) * T.iw), 0), VTAB - 1);
+  // slot floor((v - e0) iw): round-to-nearest of (v - e0) iw - 1/2 read from
+  // the low word of its sum with 1.5 * 2^52 (no conversion instruction)
+  const double sl = fma(v - T.e0, T.iw, -0.5) + 6755399441055744.0;
+  const int s = min(max((int)__double2loint(sl), 0), VTAB - 1);
   int b = T.t[s];
   // one predicated step up settles almost every value (the table gives the
   // bin of the slot's left end); the loops finish the rare rest exactly
@@ -847,9 +853,9 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   VBinTab &VT1 = VTS[0], &VT2 = VTS[1], &VTP = VTS[2];
   if (bin || !THREE_D) {
     load_vgrid_smem(c_vg.e1, c_vg.e2, c_vg.epar, VE1, VE2, VEP);
-    build_vbin_tab(VTP, c_vg.fpar, c_vg.npar);
-    build_vbin_tab(VT1, c_vg.f1, c_vg.n1);
-    if (THREE_D) build_vbin_tab(VT2, c_vg.f2, c_vg.n2);
+    build_vbin_tab(VTP, c_vg.epar, c_vg.npar);
+    build_vbin_tab(VT1, c_vg.e1, c_vg.n1);
+    if (THREE_D) build_vbin_tab(VT2, c_vg.e2, c_vg.n2);
     // the first barrier of the item loop orders the tables before any use
   }
   // one work item per block, or a persistent grid striding over the items
