@@ -32,7 +32,7 @@ constexpr int BC_THREADS = 256;
 // steps, or earlier when an injection could overflow a tube's capacity.
 constexpr int BC_COMPACT_EVERY = 8;
 // cells per tube: the per-cell tables of a tube live in shared memory (the
-// mixed push holds 84 bytes per cell, the collision-count kernel 64)
+// mixed push holds 92 bytes per cell, the collision-count kernel 64)
 constexpr int MAX_CELLS = 2048;
 // push work-item sizes the autotuner tries (ions per item); an item's ions
 // lie in one charge-exchange selection chunk
@@ -339,7 +339,7 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
   if (timed) CK(cudaEventRecord(h->pev[2 * h->npev], h->s));
   size_t smem = (size_t)(2 * nq + 1) * sizeof(double) + (size_t)nq * sizeof(unsigned);
   if (h->mixed)  // + one double of padding before the 16-byte aligned floats
-    smem += (size_t)(5 * nq + 1) * sizeof(double) + (size_t)10 * nq * sizeof(float);
+    smem += (size_t)(6 * nq + 1) * sizeof(double) + (size_t)10 * nq * sizeof(float);
   smem += (size_t)BIN_WIN * (1 + h->vg.npar + h->vg.n1 + (h->three_d ? h->vg.n2 : 0)) *
           sizeof(unsigned);  // block-private binning window
   const bool bins_variant = a.bin || a.prologue || a.bin_only || !h->three_d;
@@ -392,7 +392,7 @@ int zero_accum(kaos_handle *h) {
 
 // The per-cell tables of one tube, in the order of CellTables' pointers
 // listed by conv_table_ptr (the same values kaos_create builds).
-constexpr int CONV_TABLES = 27;
+constexpr int CONV_TABLES = 28;
 std::vector<std::vector<double>> tube_tables(const kaos_tube_c &T, const TubeD &d,
                                              const kaos_params_c &p) {
   std::vector<std::vector<double>> v(CONV_TABLES);
@@ -415,6 +415,7 @@ std::vector<std::vector<double>> tube_tables(const kaos_tube_c &T, const TubeD &
     v[24].push_back(0.5 * (T.ChiPerp1 ? T.ChiPerp1[c] : 0.0));
     v[25].push_back(0.5 * (T.ChiPerp2 ? T.ChiPerp2[c] : 0.0));
     v[26].push_back(T.OmegaG0 && T.OmegaG0[c] != 0.0 ? 1.0 / T.OmegaG0[c] : 0.0);
+    v[27].push_back(host_quartic_u(0.5 * (T.qGL[c] + T.qGH[c]), T.pG));
   }
   return v;
 }
@@ -424,7 +425,7 @@ const double *conv_table_ptr(const CellTables &c, int k) {
                                   c.thetaGC, c.ellGC, c.TeG, c.TsG, c.nsnormCNeut,
                                   c.lambdaPerp, c.EtaLH, c.XiPerp1, c.XiPerp2, c.S0,
                                   c.OmegaG0, c.ChiPerp1, c.ChiPerp2, c.uL, c.uH,
-                                  c.hK1, c.hK2, c.hc1, c.hc2, c.hiom0};
+                                  c.hK1, c.hK2, c.hc1, c.hc2, c.hiom0, c.uM};
   return p[k];
 }
 
@@ -1165,7 +1166,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   // ---- tubes: descriptors, concatenated per-cell tables -----------------
   std::vector<double> qGL, qGH, qGC, hqC, dqC, d3xC, rGC, thC, elC, TeG, TsG,
       neut, lam, eta, xi1, xi2, S0, Om0, chi1, chi2, uL, uH, hK1, hK2, hc1,
-      hc2, hiom0;
+      hc2, hiom0, uM;
   int64_t poff = 0, coff = 0, moff = 0, hoff = 0, eoff = 0;
   for (int t = 0; t < ntubes; ++t) {
     const kaos_tube_c &T = tubes[t];
@@ -1240,6 +1241,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     for (int k = 0; k < T.nq; ++k) {
       uL.push_back(host_quartic_u(T.qGL[k], T.pG));
       uH.push_back(host_quartic_u(T.qGH[k], T.pG));
+      uM.push_back(host_quartic_u(0.5 * (T.qGL[k] + T.qGH[k]), T.pG));
     }
     poff += T.capacity;
     coff += T.nq;
@@ -1267,7 +1269,7 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
   UP(TsG, TsG) UP(nsnormCNeut, neut) UP(lambdaPerp, lam) UP(EtaLH, eta)
   UP(XiPerp1, xi1) UP(XiPerp2, xi2) UP(S0, S0) UP(OmegaG0, Om0)
   UP(ChiPerp1, chi1) UP(ChiPerp2, chi2) UP(uL, uL) UP(uH, uH)
-  UP(hK1, hK1) UP(hK2, hK2) UP(hc1, hc1) UP(hc2, hc2) UP(hiom0, hiom0)
+  UP(hK1, hK1) UP(hK2, hK2) UP(hc1, hc1) UP(hc2, hc2) UP(hiom0, hiom0) UP(uM, uM)
   UP(Te, TeG)
 #undef UP
   if ((rc = dalloc(h, &c.EAmag, coff))) return rc;

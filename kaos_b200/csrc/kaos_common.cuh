@@ -65,6 +65,7 @@ struct CellTables {
   const double *lambdaPerp, *EtaLH, *XiPerp1, *XiPerp2, *S0, *OmegaG0,
       *ChiPerp1, *ChiPerp2;
   const double *uL, *uH;  // quartic root u = r/RE at the cell edges
+  const double *uM;       // ... and at the cell's midpoint in q
   const double *hK1, *hK2, *hc1, *hc2, *hiom0;  // wave-heating constants
   double *Te, *EAmag, *EG, *M0prev, *nuPoi;
   double *mom;            // [KAOS_NMOMENTS][ncell_total]

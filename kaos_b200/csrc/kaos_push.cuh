@@ -555,6 +555,23 @@ __device__ __forceinline__ double quartic_newton(double q, double ip, double u,
   return u;
 }
 
+// The same root from a guess within ~1e-4: one Newton step with the
+// derivative inverted in FP32, then a chord step reusing that inverse (the
+// derivative changes by ~1e-4 between the two points, so the chord step
+// contracts the error by that much more; ~1e-17 relative on the benchmark
+// tubes' per-cell quadratic guesses, whose error is below 3.2e-5).
+__device__ __forceinline__ double quartic_newton_chord(double q, double ip,
+                                                       double u) {
+  const double q2 = q * q;
+  double u2 = u * u;
+  double f = fma(q2 * u2, u2, fma(u, ip, -1.0));
+  const double r = (double)rcpa((float)fma(4.0 * q2 * u2, u, ip));
+  u = fma(-f, r, u);
+  u2 = u * u;
+  f = fma(q2 * u2, u2, fma(u, ip, -1.0));
+  return fma(-f, r, u);
+}
+
 // Cell search starting from the cell of the previous step (particles move a
 // small fraction of a cell per step); falls back to the bisection.
 __device__ __forceinline__ int cell_search_from(const double *E, int nq,
@@ -826,11 +843,11 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   extern __shared__ __align__(16) double sm[];
   const int nqmax = a.nqs;
   double *E = sm, *Cc = sm + nqmax + 1;
-  double *UL = Cc + nqmax, *UD = UL + nqmax, *QL = UD + nqmax, *IDQ = QL + nqmax,
-         *DQ = IDQ + nqmax;
+  double *UL = Cc + nqmax, *UD = UL + nqmax, *UC = UD + nqmax, *QL = UC + nqmax,
+         *IDQ = QL + nqmax, *DQ = IDQ + nqmax;
   // 8 floats per cell (heat32), 16-byte aligned; then the cell fields
   // (EAmag, EG) of the field re-interpolation
-  float *HK = (float *)(sm + ((7 * nqmax + 2) & ~1));
+  float *HK = (float *)(sm + ((8 * nqmax + 2) & ~1));
   float2 *FE = (float2 *)(HK + 8 * nqmax);
   unsigned *HC = (unsigned *)(FE + nqmax);
   const float h = (float)a.h, hh = 0.5f * h, h6 = h / 6.0f, hsq2 = 0.5f * h * h;
@@ -876,6 +893,8 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       IDQ[k] = 1.0 / (qh - ql);
       UL[k] = a.ct.uL[g];
       UD[k] = a.ct.uH[g] - a.ct.uL[g];
+      // quadratic in the offset through the edges and the midpoint
+      UC[k] = 4.0 * a.ct.uM[g] - 2.0 * (a.ct.uL[g] + a.ct.uH[g]);
       if (a.icr) {
         const double lam = a.ct.lambdaPerp[g];
         HK[8 * k + 0] = (float)a.ct.hK1[g];
@@ -953,7 +972,9 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     if (prologue) field_prologue32(a.ff, T, E, Cc, FE, qk0, c0, qs_ms, aea, ag);
     // ---- start-of-step position: q, then (r, theta) by FP64 Newton -------
     const double q0 = fma(o0, DQ[c0], QL[c0]);
-    const double u = quartic_newton<true>(q0, ipG, fma(o0, UD[c0], UL[c0]), 2);
+    // per-cell quadratic guess u(o) = uL + o (uH - uL) + o (1 - o) UC
+    const double u = quartic_newton_chord(
+        q0, ipG, fma(o0, fma(1.0 - o0, UC[c0], UD[c0]), UL[c0]));
     const double s2 = u * ipG;  // sin^2(theta)
     // sqrt(s2): FP32 seed and one FP64 Newton step (relative error ~1e-14)
     double ys = (double)rsq((float)s2);

@@ -968,7 +968,7 @@ __global__ void k_convect_many(ConvManyArgs m) {
 
 // The new per-cell tables and descriptors of the moved entries, from one
 // staging copy: blockIdx.y = the move, blockIdx.x = the table.
-constexpr int CONV_NTAB = 27;
+constexpr int CONV_NTAB = 28;
 struct TableApplyArgs {
   double *dst[CONV_NTAB];  // the per-cell tables (concatenated over entries)
   const double *stage;     // [move][table][nqmax]
