@@ -44,7 +44,8 @@ extern "C" {
 
 /* ---- precision modes ---------------------------------------------------- */
 #define KAOS_PREC_FP64 0  /* all particle arithmetic in FP64                */
-#define KAOS_PREC_MIXED 1 /* FP32 state + RK stages; FP64 quartic, position
+#define KAOS_PREC_MIXED 1 /* FP32 forces, RK stages and heating kicks on
+                             FP64 state (position, V||, Vperp); FP64 quartic,
                              renormalisation and reductions                  */
 
 /* ---- moment selectors for kaos_get_moments ------------------------------ */
