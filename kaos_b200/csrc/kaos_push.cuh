@@ -991,7 +991,8 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     Geo<float> g1;
     g1.ct = (float)ct;
     g1.st = (float)st;
-    g1.ir = rcpa((float)u * fRE);
+    const float rfl = (float)u * fRE;  // r in FP32
+    g1.ir = rcpa(rfl);
     g1.q = (float)q0;
     g1.ell = 1.0f + 3.0f * g1.ct * g1.ct;
     g1.isl = rsq(g1.ell);
@@ -999,7 +1000,9 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     g1.ez = (3.0f * g1.ct * g1.ct - 1.0f) * g1.isl;
     const float vparf = (float)vpar, v1f = (float)v1, v2f = (float)v2;
     const float vp2 = v1f * v1f + v2f * v2f;
-    const float rf = (float)rho0, zf = (float)z0;
+    // the FP32 meridian point (used for the k2/k4 hemisphere signs and the
+    // turn of the field direction) from values already in FP32
+    const float rf = g1.st * rfl, zf = g1.ct * rfl;
     // ---- the dominant displacement term h V|| e1 in FP64 (the direction
     // from the FP64 cos/sin, 1/sqrt(ell) from the FP32 value and one FP64
     // Newton step), taken now so that only its end point stays live --------
