@@ -403,6 +403,11 @@ __device__ __forceinline__ void ena_acc(const EnaArgs &a, const double x[3],
 __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
   extern __shared__ double sm[];
   double *E = sm;
+  // the ENA grid's edges for the bin searches in shared memory (threads
+  // read different edges: constant memory would serialise them)
+  __shared__ double EE1[MAXV + 1], EE2[MAXV + 1], EEP[MAXV + 1];
+  load_vgrid_smem(c_evg.e1, c_evg.e2, c_evg.epar, EE1, EE2, EEP);
+  __syncthreads();
   const double h = a.h, hh = 0.5 * h, h6 = h / 6.0, hsq2 = 0.5 * h * h;
   int tcur = -1;
   int item = blockIdx.x;
@@ -439,9 +444,9 @@ __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
     if (qi >= 0) {
       vps = fabs(epp[0] * V[0] + epp[1] * V[1] + epp[2] * V[2]);
       vphs = eph[0] * V[0] + eph[1] * V[1];
-      ip = ena_bin(c_evg.e1, c_evg.n1, vps, ip);
-      iq = ena_bin(c_evg.epar, c_evg.npar, vpar, iq);
-      iph = ena_bin(c_evg.e2, c_evg.n2, vphs, iph);
+      ip = ena_bin(EE1, c_evg.n1, vps, ip);
+      iq = ena_bin(EEP, c_evg.npar, vpar, iq);
+      iph = ena_bin(EE2, c_evg.n2, vphs, iph);
       const int nvb = ip | (iq << 10) | (iph << 20);
       if (nvb != vb) a.ena.vb[e] = nvb;
       // ENAParticleCountsSub (_8_3_2_ENAParticleCounts.f90:45-300)

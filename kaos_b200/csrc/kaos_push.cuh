@@ -555,6 +555,24 @@ __device__ __forceinline__ double quartic_newton(double q, double ip, double u,
   return u;
 }
 
+// The same root by Newton steps (derivative inverted in FP32, correctly
+// rounded) until the correction falls below 1e-15 of u -- the error left is
+// then ~1e-22 -- or maxit steps: for guesses of unknown quality (a tube moved
+// to a new L-shell, a cell's linear guess).
+__device__ __forceinline__ double quartic_newton_conv(double q, double ip, double u,
+                                                      int maxit) {
+  const double q2 = q * q;
+  for (int k = 0; k < maxit; ++k) {
+    const double u2 = u * u;
+    const double f = fma(q2 * u2, u2, fma(u, ip, -1.0));
+    const double fp = fma(4.0 * q2 * u2, u, ip);
+    const double du = f * (double)__frcp_rn((float)fp);
+    u -= du;
+    if (fabs(du) <= 1e-15 * u) break;
+  }
+  return u;
+}
+
 // The same root from a guess within ~1e-4: one Newton step with the
 // derivative inverted in FP32, then a chord step reusing that inverse (the
 // derivative changes by ~1e-4 between the two points, so the chord step

@@ -929,14 +929,14 @@ __device__ __forceinline__ void convect_ions(const ConvArgs &a) {
       const int64_t g = T.coff + c;
       const double o = x - (double)c;
       q = a.ct.qGL[g] + o * (a.ct.qGH[g] - a.ct.qGL[g]);
-      u_old = quartic_newton(q, ip_old, a.ct.uL[g] + o * (a.ct.uH[g] - a.ct.uL[g]), 4);
+      u_old = quartic_newton_conv(q, ip_old, a.ct.uL[g] + o * (a.ct.uH[g] - a.ct.uL[g]), 8);
     } else {
       const double rho = a.ion.rho[j], z = a.ion.z[j];
       const double r2 = rho * rho + z * z, r = sqrt(r2);
       q = (RE * RE) * (z / r) / r2;
       u_old = r / RE;
     }
-    const double u_new = quartic_newton(q, ip_new, u_old, 6);
+    const double u_new = quartic_newton_conv(q, ip_new, u_old, 8);
     const double f = sqrt(bnorm(q, u_new) / bnorm(q, u_old));
     if (a.mixed) {
       const double2 v = a.ion.v12[j];
