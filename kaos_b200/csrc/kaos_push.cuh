@@ -538,10 +538,8 @@ __device__ __forceinline__ void heat32(const PushArgs &a, uint32_t step,
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0 by Newton from u0 (the
 // function is increasing and convex for u > 0: the root is unique).  The
-// derivative is inverted in FP32 (correctly rounded, or the one-instruction
-// approximation when FAST); each step still contracts the error by ~1e-7 on
-// top of the quadratic term.
-template <bool FAST = false>
+// derivative is inverted in FP32 (correctly rounded); each step still
+// contracts the error by ~1e-7 on top of the quadratic term.
 __device__ __forceinline__ double quartic_newton(double q, double ip, double u,
                                                  int iters) {
   const double q2 = q * q;
@@ -549,7 +547,7 @@ __device__ __forceinline__ double quartic_newton(double q, double ip, double u,
     const double u2 = u * u;
     const double f = fma(q2 * u2, u2, fma(u, ip, -1.0));
     const double fp = fma(4.0 * q2 * u2, u, ip);
-    const float r = FAST ? rcpa((float)fp) : __frcp_rn((float)fp);
+    const float r = __frcp_rn((float)fp);
     u = fma(-f, (double)r, u);
   }
   return u;
@@ -783,9 +781,9 @@ __global__ void __launch_bounds__(256, 2) k_push64(PushArgs a) {
   }  // work items
 }
 
-// The force switches of apar as 0/1 factors: the same a|| without branches
-// (s * (m - |AG| + |AEA|) + AEA with the switched-off terms multiplied by 0;
-// the sign s = -1 south of the equator).
+// The force switches of apar as 0/1 factors for the mixed push: a|| =
+// s (cm m - cg |AG| + ce2 |AEA|) + ce1 AEA without branches (the sign s = -1
+// south of the equator).
 struct ForceC {
   float cm, cg, ce1, ce2;  // mirror, gravity, signed / unsigned ambipolar
 };
@@ -793,13 +791,6 @@ __device__ __forceinline__ ForceC force_c(const ForceFlags &f) {
   return ForceC{f.mirror ? 1.0f : 0.0f, f.grav ? 1.0f : 0.0f,
                 (f.eamb && f.eambsign) ? 1.0f : 0.0f,
                 (f.eamb && !f.eambsign) ? 1.0f : 0.0f};
-}
-__device__ __forceinline__ float apar_bf(const Geo<float> &g, float vperp2,
-                                         float aea, float ag, const ForceC &f) {
-  const float m = 1.5f * vperp2 * fabsf(g.ct) * g.ir *
-                  (2.0f + g.st * g.st * g.isl * g.isl) * g.isl;
-  const float s = g.ct <= 0.0f ? -1.0f : 1.0f;
-  return s * (f.cm * m - f.cg * fabsf(ag) + f.ce2 * fabsf(aea)) + f.ce1 * aea;
 }
 
 // Start-of-step velocity bins of one ion from its FP64 velocities and the
