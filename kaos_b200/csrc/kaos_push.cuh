@@ -986,7 +986,9 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
         q0, ipG, fma(o0, fma(1.0 - o0, UC[c0], UD[c0]), UL[c0]));
     const double s2 = u * ipG;  // sin^2(theta)
     // sqrt(s2): FP32 seed and one FP64 Newton step (relative error ~1e-14)
-    double ys = (double)rsq((float)s2);
+    const float s2f = (float)s2;
+    const float ysf = rsq(s2f);
+    double ys = (double)ysf;
     ys = ys * fma(-0.5 * s2 * ys, ys, 1.5);
     const double st = s2 * ys;
     const double ct = q0 * u * u;
@@ -996,13 +998,16 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     // rounding is far below the margin): no edge search
     const int qi = (o0 > 1e-9 && o0 < 1.0 - 1e-9)
                        ? c0 : cell_search_from(E, T.nq, T.sgn * q0, c0);
-    // ---- k1 geometry in FP32 ---------------------------------------------
+    // ---- k1 geometry in FP32, from FP32 values (cos = q u^2, sin = s2
+    // rsqrt(s2)): two FP64->FP32 conversions fewer on the busy XU pipe, for
+    // a few FP32 roundings in forces that carry FP32 rounding anyway -------
     Geo<float> g1;
-    g1.ct = (float)ct;
-    g1.st = (float)st;
-    const float rfl = (float)u * fRE;  // r in FP32
-    g1.ir = rcpa(rfl);
     g1.q = (float)q0;
+    const float uf = (float)u;
+    g1.ct = g1.q * uf * uf;
+    g1.st = s2f * ysf;
+    const float rfl = uf * fRE;  // r in FP32
+    g1.ir = rcpa(rfl);
     g1.ell = 1.0f + 3.0f * g1.ct * g1.ct;
     g1.isl = rsq(g1.ell);
     g1.er = 3.0f * g1.ct * g1.st * g1.isl;
