@@ -40,6 +40,15 @@ constexpr int NCHUNKS = 3;
 constexpr int CHUNKS[NCHUNKS] = {1024, 2048, 4096};
 static_assert(CX_CHUNK % 4096 == 0 && CX_CHUNK % (PUSH_THREADS * PUSH_ITEMS) == 0,
               "chunk sizes");
+// k_push_ena's shared memory: the tube's cell edges, the per-tube unit prefix
+static size_t ena_push_smem(int nq, int ntubes) {
+  return (size_t)(nq + 1) * sizeof(double) + (size_t)(ntubes + 1) * sizeof(int);
+}
+// k_cx_convert's shared memory: conversions still owed per cell, per-warp
+// per-cell counts (8 warps), the chunk's Qindk1
+static size_t cx_convert_smem(int nq) {
+  return ((size_t)9 * nq + CX_CHUNK) * sizeof(unsigned);
+}
 
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0: closed form of the
 // depressed resolvent cubic in hyperbolic form, then Newton polish.
@@ -127,6 +136,9 @@ struct kaos_handle {
   int *d_cxend = nullptr;
   int *d_tube_done = nullptr;  // per tube: charge-exchange cell scans done
   int *d_cx_list = nullptr, *d_cx_nlist = nullptr, *d_tube_active = nullptr;
+  int *d_cx_chunks = nullptr;       // chunks with conversions this step
+  unsigned *d_cx_nchunk = nullptr;  // their count, by step parity
+  int cx_blocks = 0;                // k_cx_convert: one resident wave
   // convection: device staging of the moves of one master step (allocated
   // at the first move) and its host side
   double *d_conv_stage = nullptr, *d_conv_pnew = nullptr;
@@ -737,6 +749,10 @@ CxArgs cx_args(kaos_handle *h) {
   a.tube_done = h->d_tube_done;
   a.list = h->d_cx_list;
   a.nlist = h->d_cx_nlist;
+  a.chunk_list = h->d_cx_chunks;
+  a.nchunk = h->d_cx_nchunk;
+  a.step = (uint32_t)(h->n + 1);
+  a.dstep = h->capturing ? h->d_step : nullptr;
   a.tube_active = h->d_tube_active;
   a.rank = h->rank;
   a.nranks = h->nranks;
@@ -747,15 +763,19 @@ CxArgs cx_args(kaos_handle *h) {
   return a;
 }
 
-// Blocks of a grid striding over n work items: a few per SM.
-static int strided_grid(kaos_handle *h, int n) {
+static int sm_count(kaos_handle *h) {
   if (!h->nsm) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       h->nsm = 148;
   }
-  return std::max(1, std::min(n, 4 * h->nsm));
+  return h->nsm;
+}
+
+// Blocks of a grid striding over n work items: a few per SM.
+static int strided_grid(kaos_handle *h, int n) {
+  return std::max(1, std::min(n, 4 * sm_count(h)));
 }
 
 // charge exchange at the start of a step (_8_KineticSolver.f90:95-166)
@@ -763,12 +783,14 @@ int launch_cx(kaos_handle *h) {
   CxArgs a = cx_args(h);
   const int nq = max_nq(h);
   // the per-chunk Qindk1 counts were accumulated by the previous push
-  // 1024 threads: one tile covers the chunks of a tube of up to 16.7 M ions
-  k_cx_scan<<<std::max(1, strided_grid(h, (int)h->ncell) / 2), 1024, 0, h->s>>>(
+  // a block per listed cell (the list length is on the device: one
+  // resident wave of 256-thread blocks, striding over the list)
+  k_cx_scan<<<(int)std::min<int64_t>(h->ncell, 8 * (int64_t)sm_count(h)), 256, 0, h->s>>>(
       a, h->d_cell_tube, h->d_cell_q);
-  // one block per chunk (a chunk with conversions walks its ions in order;
-  // blocks of chunks without live ions leave at once)
-  k_cx_convert<<<std::max(h->ncx, 1), 256, (size_t)9 * nq * sizeof(unsigned), h->s>>>(a);
+  // the scan has read every count: cleared for the next push; then a block
+  // per chunk with conversions
+  CK(cudaMemsetAsync(h->d_cxc, 0, (size_t)h->ncx * nq * sizeof(unsigned), h->s));
+  k_cx_convert<<<std::max(1, std::min(h->ncx, h->cx_blocks)), 256, cx_convert_smem(nq), h->s>>>(a);
   h->launches += 2;
   CK(cudaGetLastError());
   return KAOS_OK;
@@ -788,13 +810,17 @@ int launch_push_ena(kaos_handle *h, int bin) {
   a.tube_blk0 = h->d_tube_eblk0;
   a.nitems = h->neblk;
   a.chunk = PUSH_THREADS * PUSH_ITEMS;
+  a.sub = PUSH_ITEMS;
+  a.ntubes = h->ntubes;
+  a.ct_nqmax = max_nq(h);
   a.nena = h->d_nena;
   a.ct = h->ct;
   a.ena = h->ena[h->ecur];
   a.h = h->P.h;
   a.grav_GM = GG * ME;
   a.grav = h->P.GRAVflag == 1;
-  k_push_ena<<<strided_grid(h, h->neblk), PUSH_THREADS, (size_t)(max_nq(h) + 1) * sizeof(double), h->s2>>>(a);
+  k_push_ena<<<strided_grid(h, h->neblk * PUSH_ITEMS), PUSH_THREADS,
+               ena_push_smem(max_nq(h), h->ntubes), h->s2>>>(a);
   h->launches++;
   CK(cudaGetLastError());
   CK(cudaEventRecord(h->ejoin, h->s2));
@@ -1442,6 +1468,8 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
         (rc = dalloc(h, &h->d_tube_done, (size_t)ntubes)) ||
         (rc = dalloc(h, &h->d_cx_list, (size_t)h->ncell)) ||
         (rc = dalloc(h, &h->d_cx_nlist, 1)) ||
+        (rc = dalloc(h, &h->d_cx_chunks, cxt.size())) ||
+        (rc = dalloc(h, &h->d_cx_nchunk, 2)) ||
         (rc = dalloc(h, &h->d_tube_active, (size_t)ntubes)) ||
         (rc = dalloc(h, &h->d_cxc, cxt.size() * (size_t)max_nq(h))) ||
         (rc = dalloc(h, &h->d_cxo, cxt.size() * (size_t)max_nq(h))))
@@ -1452,13 +1480,17 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     const size_t nq = (size_t)max_nq(h);
     const std::pair<const void *, size_t> big[] = {
         {(const void *)k_collision_counts, 8 * nq * sizeof(double)},
-        {(const void *)k_cx_convert, 9 * nq * sizeof(unsigned)},
+        {(const void *)k_cx_convert, cx_convert_smem((int)nq)},
         {(const void *)k_fields, 3 * nq * sizeof(double)},
-        {(const void *)k_push_ena, (nq + 1) * sizeof(double)},
+        {(const void *)k_push_ena, ena_push_smem((int)nq, ntubes)},
         {(const void *)k_load, (nq + 1) * sizeof(double)}};
     for (const auto &b : big)
       if (b.second > 48 * 1024)
         CK(cudaFuncSetAttribute(b.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.second));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cx_convert, 256,
+                                                     cx_convert_smem((int)nq)));
+    h->cx_blocks = std::max(1, per_sm) * sm_count(h);
   }
   CK(cudaDeviceSynchronize());
   return KAOS_OK;

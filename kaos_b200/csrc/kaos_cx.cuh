@@ -30,18 +30,28 @@ struct CxArgs {
   Enas ena;
   int64_t *nena;
   unsigned *cxc;             // [chunk][nq_max] Qindk1 counts (from the push)
-  unsigned *cxo;             // [chunk][nq_max] exclusive prefix
+  unsigned *cxo;             // [chunk][nq_max] conversions still owed there
   unsigned *cxconv;          // per chunk: ions converted in it this step
   int64_t *cxbase;           // per chunk: ENA slot of its first conversion
   int *cxend;                // per cell (all tubes): chunks >= cxend convert none
   int *tube_done;            // per tube: cell scans finished this step
   int *list, *nlist;         // cells with conversions (need > 0), their count
+  // chunks with conversions this step, appended by the scan; their count
+  // by step parity (the conversion kernel of step n resets step n+1's)
+  int *chunk_list;
+  unsigned *nchunk;
+  uint32_t step;
+  const uint32_t *dstep;     // graph replay: the step number in device memory
   int *tube_active;          // per tube: listed cells
   int nqmax, mixed;
   int ncx;                   // selection chunks (all tubes)
   int rank, nranks;          // this rank's share of a split tube's conversions
   uint32_t *status;
 };
+
+__device__ __forceinline__ uint32_t cx_step(const CxArgs &a) {
+  return a.dstep ? *a.dstep : a.step;
+}
 
 // Ions a cell converts at this step on this rank: its share of
 // nint(nuIonNeutPoiT) when the tube is split over nranks.
@@ -51,7 +61,7 @@ __device__ __forceinline__ unsigned cx_need(const CxArgs &a, double nu) {
 }
 
 // exclusive scan over the chunks of a tube for one cell (one block per
-// (tube, cell) pair, block-wide scan); adds the conversions of this cell to
+// (tube, cell) pair, block-wide scan, blockDim.x chunks a pass); adds the conversions of this cell to
 // the per-chunk totals.
 // A cell with no conversion does nothing; the scan of a cell stops after the
 // tile of chunks in which its prefix reaches the conversion count, and
@@ -87,8 +97,10 @@ __device__ __forceinline__ void cx_scan_cell(const CxArgs &a, int t, int k,
     for (int v = 0; v < nw; ++v) { if (v < w) woff += wsum[v]; tot += wsum[v]; }
     const unsigned s = base + woff + x - n;  // exclusive prefix
     if (c < c1) {
-      a.cxo[(int64_t)c * a.nqmax + k] = s;
-      if (n && s < need) atomicAdd(&a.cxconv[c], min(n, need - s));
+      a.cxo[(int64_t)c * a.nqmax + k] = s < need ? need - s : 0u;
+      // the first cell to give the chunk a conversion lists it
+      if (n && s < need && atomicAdd(&a.cxconv[c], min(n, need - s)) == 0u)
+        a.chunk_list[atomicAdd(a.nchunk + (cx_step(a) & 1u), 1u)] = c;
     }
     __syncthreads();
     if (threadIdx.x == 0) base += tot;
@@ -136,16 +148,17 @@ __device__ __forceinline__ void cx_base_tube(const CxArgs &a, int t) {
 __global__ void k_cx_list(CxArgs a, const int *cell_tube, int64_t ncell) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ncell) return;
+  a.cxend[g] = 0;  // a cell off the list owes nothing in any chunk
   if (cx_need(a, a.ct.nuPoi[g]) == 0u) return;
   a.list[atomicAdd(a.nlist, 1)] = (int)g;
   atomicAdd(a.tube_active + cell_tube[g], 1);
 }
 
-// A block (1024 threads) per listed cell, striding over the list: the
-// cell's scan, then the last listed cell of a tube to finish (a per-tube
-// arrival counter) gives the tube its ENA slots and resets the counter.
+// A block (256 threads) per listed cell, striding over the list: the cell's
+// scan, then the last listed cell of a tube to finish (a per-tube arrival
+// counter) gives the tube its ENA slots and resets the counter.
 // Tubes without a listed cell convert nothing this step.
-__global__ void __launch_bounds__(1024) k_cx_scan(CxArgs a, const int *cell_tube,
+__global__ void __launch_bounds__(256) k_cx_scan(CxArgs a, const int *cell_tube,
                                                   const int *cell_q) {
   const int nl = *a.nlist;
   __shared__ int last;
@@ -188,158 +201,227 @@ __device__ __forceinline__ int next_own_item(int first) {
   return first + (((int)blockIdx.x - first) % G + G) % G;
 }
 
-// in-order conversion of the first need[Q] eligible ions per cell; the
-// converted ions of a chunk take consecutive ENA slots from cxbase in index
-// order (the chunk's count row is also cleared for the next push)
+// Convert ion j (cell q) into the ENA of slot `slot`: the ion's state at the
+// end of the previous step, its velocity rotated into the frame of the
+// previous step's k4 point (IonNeutralCollisionsSub
+// _8_1_1_1_IonNeutralCollisions.f90:25-58); the ion slot is marked DEAD.
+__device__ __forceinline__ void cx_convert_ion(const CxArgs &a, const TubeD &T,
+                                               int64_t j, int q, int64_t slot) {
+  // ion position and velocity at the end of the previous step
+  double rho, z, vpar, v1, v2, qk4;
+  if (a.mixed) {
+    const double xx = a.ion.x[j];
+    const int cc = x_cell(xx, T.nq);
+    const double oo = xx - (double)cc;
+    const double qq = a.ct.qGL[T.coff + cc] +
+                      oo * (a.ct.qGH[T.coff + cc] - a.ct.qGL[T.coff + cc]);
+    const double ug = a.ct.uL[T.coff + cc] +
+                      oo * (a.ct.uH[T.coff + cc] - a.ct.uL[T.coff + cc]);
+    const double u = quartic_newton(qq, 1.0 / T.pG, ug, 3);
+    const double s2 = u / T.pG;
+    rho = u * RE * sqrt(s2);
+    z = u * RE * qq * u * u;
+    vpar = a.ion.vpar[j];
+    const double2 v = a.ion.v12[j];
+    v1 = v.x;
+    v2 = v.y;
+    qk4 = a.ion.fqk4[j];
+  } else {
+    rho = a.ion.rho[j];
+    z = a.ion.z[j];
+    vpar = a.ion.vpar[j];
+    v1 = a.ion.v1[j];
+    v2 = a.ion.v2[j];
+    qk4 = a.ion.qk4[j];
+  }
+  // geometry of the k4 point of the previous step: stored exactly in
+  // FP64 mode, rebuilt from its q (p = pG) in mixed mode
+  double ctk, stk;
+  if (a.ion.rho4) {
+    const Geo<double> g4 = geo(a.ion.rho4[j], a.ion.z4[j]);
+    ctk = g4.ct;
+    stk = g4.st;
+  } else {
+    const double uk = quartic_newton(qk4, 1.0 / T.pG, sqrt(rho * rho + z * z) / RE, 4);
+    ctk = qk4 * uk * uk;
+    stk = sqrt(uk / T.pG);
+  }
+  const Geo<double> gN = geo(rho, z);
+  double ep[3], epp[3], eph[3], e4[3], e4p[3], e4h[3];
+  dipole_frame(gN.ct, gN.st, T.cphi, T.sphi, ep, epp, eph);
+  dipole_frame(ctk, stk, T.cphi, T.sphi, e4, e4p, e4h);
+  const double VN[3] = {vpar * ep[0], vpar * ep[1], vpar * ep[2]};
+  const double vp4 = e4[0] * VN[0] + e4[1] * VN[1] + e4[2] * VN[2];
+  if (slot < T.ecap) {
+    const int64_t e = T.eoff + slot;
+    a.ena.x[e] = rho * T.cphi;
+    a.ena.y[e] = rho * T.sphi;
+    a.ena.z[e] = z;
+    a.ena.vx[e] = vp4 * e4[0] + v1 * e4p[0] + v2 * e4h[0];
+    a.ena.vy[e] = vp4 * e4[1] + v1 * e4p[1] + v2 * e4h[1];
+    a.ena.vz[e] = vp4 * e4[2] + v1 * e4p[2] + v2 * e4h[2];
+    a.ena.vps[e] = 0.0;  // Vp(j), Vphi(j) still hold the ion zeros
+    a.ena.vphs[e] = 0.0;
+    a.ena.qind[e] = q;
+    a.ena.vb[e] = 0;
+    a.ena.id[e] = a.ion.id[j];
+  } else {
+    atomicOr(a.status, ST_CAP);
+  }
+  a.ion.qind[j] = DEAD;
+  if (a.mixed) a.ion.x[j] = XDEAD;
+}
+
+// In-order conversion of the first need[Q] eligible ions per cell of one
+// chunk, selected in parallel: each of the CX_WARPS warps owns a segment of
+// CX_CHUNK / CX_WARPS consecutive ions.  Pass 1 counts every warp's
+// candidates per cell; the counts become per-cell exclusive prefixes over
+// the warps; pass 2 ranks each candidate among its cell's candidates of the
+// chunk (prefix + running count in the segment), and rank < need converts
+// -- the same ions as a walk in index order.  Each warp lists its
+// conversions in order; they take consecutive ENA slots from cxbase in index
+// order and are converted by all threads at once.
+constexpr int CX_WARPS = 8;  // 256-thread blocks
+static_assert(CX_CHUNK <= (1 << 14), "conversion list packs (cell << 14) | index");
 __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) {
   const TubeD &T = a.tubes[t];
-  unsigned *crow = a.cxc + (int64_t)c * a.nqmax;
   __syncthreads();  // the previous chunk of this block is done with smem
-  const unsigned nconv = a.cxconv[c];
-  if (nconv == 0u) {
-    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) crow[k] = 0u;
-    return;
-  }
   extern __shared__ unsigned sm_[];
-  unsigned *need = sm_;                 // remaining conversions per cell
-  unsigned *wcnt = sm_ + a.nqmax;       // [8 warps][nq] per-tile counts
-  __shared__ unsigned done, wconv[32];
-  if (threadIdx.x == 0) done = 0;
+  unsigned *need = sm_;             // conversions this chunk owes per cell
+  unsigned *wcnt = sm_ + a.nqmax;   // [CX_WARPS][nq]: counts, then ranks
+  int *qs = (int *)(wcnt + CX_WARPS * a.nqmax);  // Qindk1, then the lists
+  __shared__ unsigned wconv[CX_WARPS];
+  const int64_t beg = a.cx_start[c];
+  const int nk = (int)min((int64_t)CX_CHUNK, a.nlive[t] - beg);
+  // owed by this chunk: written by this step's scan for the chunks before
+  // the cell's cxend (0 off the list)
   for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
-    unsigned nd = cx_need(a, a.ct.nuPoi[T.coff + k]);
-    if (nd && c >= a.cxend[T.coff + k]) nd = 0u;  // prefix >= need
-    const unsigned o = nd ? a.cxo[(int64_t)c * a.nqmax + k] : 0u;
-    crow[k] = 0u;
-    need[k] = nd > o ? nd - o : 0u;
+    const int ce = a.cxend[T.coff + k];
+    const unsigned o = a.cxo[(int64_t)c * a.nqmax + k];
+    need[k] = c < ce ? o : 0u;
+  }
+  for (int k = threadIdx.x; k < CX_WARPS * T.nq; k += blockDim.x) wcnt[k] = 0u;
+  if (threadIdx.x == 0) a.cxconv[c] = 0u;  // for the next step's scan
+  __syncthreads();
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const unsigned lt = (1u << l) - 1u;
+  constexpr int SEG = CX_CHUNK / CX_WARPS;  // ions per warp
+  constexpr int GPW = SEG / 32;             // 32-ion groups per warp
+  constexpr int BATCH = 16;                 // loads in flight per lane
+  static_assert(GPW % 32 == 0 && GPW % BATCH == 0, "segment layout");
+  __shared__ unsigned gmask[CX_WARPS * GPW];  // candidate lanes per group
+  const int s0 = w * SEG, s1 = min(s0 + SEG, nk);
+  // each warp stages its own segment: candidates (a cell that still
+  // converts here) keep their cell, others -1; BATCH independent loads per
+  // lane are issued before any is used
+  const int32_t *qsrc = a.ion.qind + T.off + beg;
+  if ((((uintptr_t)qsrc) & 15) == 0 && s1 == s0 + SEG) {
+    // a full, 16-byte aligned segment: SEG / 128 int4 loads per lane, in
+    // two batches of independent loads
+    constexpr int NV = SEG / 256;
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+    int4 v[NV];
+#pragma unroll
+    for (int u = 0; u < NV; ++u)
+      v[u] = *(const int4 *)(qsrc + s0 + 4 * ((b * NV + u) * 32 + l));
+#pragma unroll
+    for (int u = 0; u < NV; ++u) {
+      int4 r;
+      r.x = (v[u].x >= 0 && need[v[u].x] != 0u) ? v[u].x : -1;
+      r.y = (v[u].y >= 0 && need[v[u].y] != 0u) ? v[u].y : -1;
+      r.z = (v[u].z >= 0 && need[v[u].z] != 0u) ? v[u].z : -1;
+      r.w = (v[u].w >= 0 && need[v[u].w] != 0u) ? v[u].w : -1;
+      *(int4 *)(qs + s0 + 4 * ((b * NV + u) * 32 + l)) = r;
+    }
+    }
+  } else {
+    for (int g0 = 0; g0 < GPW; g0 += BATCH) {
+      int v[BATCH];
+#pragma unroll
+      for (int u = 0; u < BATCH; ++u) {
+        const int i = s0 + (g0 + u) * 32 + l;
+        v[u] = i < s1 ? qsrc[i] : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < BATCH; ++u)
+        qs[s0 + (g0 + u) * 32 + l] = (v[u] >= 0 && need[v[u]] != 0u) ? v[u] : -1;
+    }
+  }
+  __syncwarp();
+  for (int g = 0; g < GPW; ++g) {
+    const unsigned m = __ballot_sync(0xffffffffu, qs[s0 + g * 32 + l] >= 0);
+    if (l == 0) gmask[w * GPW + g] = m;
+  }
+  __syncwarp();
+  unsigned *wc = wcnt + w * T.nq;
+  // pass 1: this warp's candidates per cell (one leader per cell adds),
+  // over the groups holding candidates only
+  for (int h = 0; h < GPW; h += 32) {
+    unsigned has = __ballot_sync(0xffffffffu, gmask[w * GPW + h + l] != 0u);
+    while (has) {
+      const int i = s0 + (h + __ffs(has) - 1) * 32 + l;
+      has &= has - 1u;
+      const int q = qs[i];
+      const unsigned peers = __match_any_sync(0xffffffffu, q);
+      if (q >= 0 && (peers & lt) == 0u) wc[q] += __popc(peers);
+      __syncwarp();
+    }
   }
   __syncthreads();
-  if (threadIdx.x == 0) a.cxconv[c] = 0u;  // every thread has read it
+  // per cell: the counts become exclusive prefixes over the warps
+  for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
+    unsigned sum = 0;
+    for (int v = 0; v < CX_WARPS; ++v) {
+      const unsigned x = wcnt[v * T.nq + k];
+      wcnt[v * T.nq + k] = sum;
+      sum += x;
+    }
+  }
+  __syncthreads();
+  // pass 2: ranks; the k-th conversion of the segment is listed at qs[s0 +
+  // k], at or before the entries of its own (already read) group, as
+  // (cell << 14) | index
+  unsigned nwc = 0;
+  for (int h = 0; h < GPW; h += 32) {
+    unsigned has = __ballot_sync(0xffffffffu, gmask[w * GPW + h + l] != 0u);
+    while (has) {
+      const int i = s0 + (h + __ffs(has) - 1) * 32 + l;
+      has &= has - 1u;
+      const int q = qs[i];
+      const unsigned peers = __match_any_sync(0xffffffffu, q);
+      const bool conv = q >= 0 && wc[q] + __popc(peers & lt) < need[q];
+      __syncwarp();  // every lane has read its cell's running rank and entry
+      if (q >= 0 && (peers & lt) == 0u) wc[q] += __popc(peers);
+      const unsigned bal = __ballot_sync(0xffffffffu, conv);
+      if (conv) qs[s0 + nwc + __popc(bal & lt)] = (q << 14) | i;
+      nwc += __popc(bal);
+      __syncwarp();
+    }
+  }
+  if (l == 0) wconv[w] = nwc;
+  __syncthreads();
+  unsigned tot = 0;
+  for (int v = 0; v < CX_WARPS; ++v) tot += wconv[v];
   const int64_t slot0 = a.cxbase[c];
-  const int64_t nl = a.nlive[t];
-  const int64_t beg = a.cx_start[c], end = min(beg + (int64_t)CX_CHUNK, nl);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int64_t r0 = beg; r0 < end; r0 += blockDim.x) {
-    if (done >= nconv) break;  // uniform: read after the tile's last sync
-    const int64_t i = r0 + threadIdx.x;
-    int q = -1;
-    if (i < end) {
-      q = a.ion.qind[T.off + i];
-      if (q < 0 || need[q] == 0) q = -1;
-    }
-    // most tiles hold no candidate: one barrier and on to the next tile
-    if (!__syncthreads_or(q >= 0)) continue;
-    // rank among same-cell candidates of this tile, in index order
-    const unsigned peers = __match_any_sync(0xffffffffu, q);
-    const int wr = __popc(peers & ((1u << l) - 1u));
-    for (int k = threadIdx.x; k < nw * T.nq; k += blockDim.x) wcnt[k] = 0;
-    __syncthreads();
-    if (q >= 0 && wr == 0) wcnt[w * T.nq + q] = __popc(peers);
-    __syncthreads();
-    bool conv = false;
-    if (q >= 0) {
-      unsigned before = 0;
-      for (int v = 0; v < w; ++v) before += wcnt[v * T.nq + q];
-      conv = (before + (unsigned)wr) < need[q];
-    }
-    __syncthreads();
-    // consume: need[q] -= min(need, tile count) (one thread per cell)
-    for (int k = threadIdx.x; k < T.nq; k += blockDim.x) {
-      unsigned tot = 0;
-      for (int v = 0; v < nw; ++v) tot += wcnt[v * T.nq + k];
-      need[k] = need[k] > tot ? need[k] - tot : 0u;
-    }
-    // slot of this conversion: rank among the tile's conversions
-    const unsigned bal = __ballot_sync(0xffffffffu, conv);
-    if (l == 0) wconv[w] = __popc(bal);
-    __syncthreads();
-    unsigned woff = 0, ttot = 0;
-    for (int v = 0; v < nw; ++v) { if (v < w) woff += wconv[v]; ttot += wconv[v]; }
-    const int64_t slot = slot0 + done + woff + __popc(bal & ((1u << l) - 1u));
-    __syncthreads();  // every thread has read done and wconv
-    if (threadIdx.x == 0) done += ttot;
-    if (conv) {
-      const int64_t j = T.off + i;
-      // ion position and velocity at the end of the previous step
-      double rho, z, vpar, v1, v2, qk4;
-      if (a.mixed) {
-        const double xx = a.ion.x[j];
-        const int cc = x_cell(xx, T.nq);
-        const double oo = xx - (double)cc;
-        const double qq = a.ct.qGL[T.coff + cc] +
-                          oo * (a.ct.qGH[T.coff + cc] - a.ct.qGL[T.coff + cc]);
-        const double ug = a.ct.uL[T.coff + cc] +
-                          oo * (a.ct.uH[T.coff + cc] - a.ct.uL[T.coff + cc]);
-        const double u = quartic_newton(qq, 1.0 / T.pG, ug, 3);
-        const double s2 = u / T.pG;
-        rho = u * RE * sqrt(s2);
-        z = u * RE * qq * u * u;
-        vpar = a.ion.vpar[j];
-        const double2 v = a.ion.v12[j];
-        v1 = v.x;
-        v2 = v.y;
-        qk4 = a.ion.fqk4[j];
-      } else {
-        rho = a.ion.rho[j];
-        z = a.ion.z[j];
-        vpar = a.ion.vpar[j];
-        v1 = a.ion.v1[j];
-        v2 = a.ion.v2[j];
-        qk4 = a.ion.qk4[j];
-      }
-      // geometry of the k4 point of the previous step: stored exactly in
-      // FP64 mode, rebuilt from its q (p = pG) in mixed mode
-      double ctk, stk;
-      if (a.ion.rho4) {
-        const Geo<double> g4 = geo(a.ion.rho4[j], a.ion.z4[j]);
-        ctk = g4.ct;
-        stk = g4.st;
-      } else {
-        const double uk = quartic_newton(qk4, 1.0 / T.pG, sqrt(rho * rho + z * z) / RE, 4);
-        ctk = qk4 * uk * uk;
-        stk = sqrt(uk / T.pG);
-      }
-      const Geo<double> gN = geo(rho, z);
-      double ep[3], epp[3], eph[3], e4[3], e4p[3], e4h[3];
-      dipole_frame(gN.ct, gN.st, T.cphi, T.sphi, ep, epp, eph);
-      dipole_frame(ctk, stk, T.cphi, T.sphi, e4, e4p, e4h);
-      const double VN[3] = {vpar * ep[0], vpar * ep[1], vpar * ep[2]};
-      const double vp4 = e4[0] * VN[0] + e4[1] * VN[1] + e4[2] * VN[2];
-      if (slot < T.ecap) {
-        const int64_t e = T.eoff + slot;
-        a.ena.x[e] = rho * T.cphi;
-        a.ena.y[e] = rho * T.sphi;
-        a.ena.z[e] = z;
-        a.ena.vx[e] = vp4 * e4[0] + v1 * e4p[0] + v2 * e4h[0];
-        a.ena.vy[e] = vp4 * e4[1] + v1 * e4p[1] + v2 * e4h[1];
-        a.ena.vz[e] = vp4 * e4[2] + v1 * e4p[2] + v2 * e4h[2];
-        a.ena.vps[e] = 0.0;  // Vp(j), Vphi(j) still hold the ion zeros
-        a.ena.vphs[e] = 0.0;
-        a.ena.qind[e] = q;
-        a.ena.vb[e] = 0;
-        a.ena.id[e] = a.ion.id[j];
-      } else {
-        atomicOr(a.status, ST_CAP);
-      }
-      a.ion.qind[j] = DEAD;
-      if (a.mixed) a.ion.x[j] = XDEAD;
-    }
-    __syncthreads();
+  for (int m = threadIdx.x; m < (int)tot; m += blockDim.x) {
+    int v = 0;
+    unsigned off = 0;
+    while (m >= (int)(off + wconv[v])) off += wconv[v++];
+    const int e = qs[v * SEG + (m - (int)off)];
+    cx_convert_ion(a, T, T.off + beg + (e & ((1 << 14) - 1)), e >> 14, slot0 + m);
   }
 }
 
-// A grid striding over the selection chunks; a chunk without live ions has
-// no counts (the push wrote none since the last clear), and neither has any
-// later chunk of its tube: the block moves on to the next tube.
-__global__ void k_cx_convert(CxArgs a) {
-  int c = blockIdx.x;
-  while (c < a.ncx) {
-    const int t = a.cx_tube[c];
-    if (a.cx_start[c] >= a.nlive[t]) {
-      c = next_own_item(a.tube_cx0[t + 1]);
-      continue;
-    }
-    cx_convert_chunk(a, c, t);
-    c += gridDim.x;
+// One resident wave of blocks; each chunk the scan listed is converted by
+// one block.
+__global__ void __launch_bounds__(256) k_cx_convert(CxArgs a) {
+  const uint32_t par = cx_step(a) & 1u;
+  const int nc = (int)a.nchunk[par];
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.nchunk[par ^ 1u] = 0u;
+  for (int k = blockIdx.x; k < nc; k += gridDim.x) {
+    const int c = a.chunk_list[k];
+    cx_convert_chunk(a, c, a.cx_tube[c]);
   }
 }
 
@@ -355,6 +437,8 @@ struct EnaArgs {
   const int *tube_blk0;  // first work item of each tube (ntubes + 1)
   int nitems;            // work items (tube, chunk of ENA slots)
   int chunk;
+  int sub;               // units per item (a unit: chunk / sub slots, a block's)
+  int ntubes, ct_nqmax;  // tubes; cells of the largest (shared-memory layout)
   const int64_t *nena;
   CellTables ct;
   Enas ena;
@@ -398,29 +482,65 @@ __device__ __forceinline__ void ena_acc(const EnaArgs &a, const double x[3],
   A[0] = g * x[0]; A[1] = g * x[1]; A[2] = g * x[2];
 }
 
-// A grid striding over the (tube, chunk) items; the first idle item of a
-// tube (its ENAs end before it) sends the block on to the next tube.
+// First unit of each tube (UP[0..ntubes], an exclusive prefix of the units
+// holding ENAs this step): each thread a run of consecutive tubes, then one
+// block-wide scan.
+__device__ __forceinline__ void ena_unit_prefix(const EnaArgs &a, int *UP, int usz) {
+  const int n = a.ntubes;
+  const int run = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int r0 = (int)threadIdx.x * run, r1 = min(r0 + run, n);
+  int cnt = 0;
+  for (int t = r0; t < r1; ++t) {
+    const int64_t nl = min(a.nena[t], a.tubes[t].ecap);
+    UP[t] = (int)ceil_div(nl, (int64_t)usz);
+    cnt += UP[t];
+  }
+  __shared__ int wsum[32];
+  const int l = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = cnt;  // inclusive warp scan of the run counts
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (l >= o) x += y;
+  }
+  if (l == 31) wsum[w] = x;
+  __syncthreads();
+  int off = x - cnt;
+  for (int v = 0; v < w; ++v) off += wsum[v];
+  for (int t = r0; t < r1; ++t) {
+    const int c = UP[t];
+    UP[t] = off;
+    off += c;
+  }
+  if (threadIdx.x == blockDim.x - 1) UP[n] = off;
+  __syncthreads();
+}
+
+// A grid striding over the units holding ENAs (one ENA per thread), found
+// through the per-tube unit prefix; a unit's tube by binary search.
 __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
   extern __shared__ double sm[];
   double *E = sm;
+  int *UP = (int *)(sm + a.ct_nqmax + 1);
   // the ENA grid's edges for the bin searches in shared memory (threads
   // read different edges: constant memory would serialise them)
   __shared__ double EE1[MAXV + 1], EE2[MAXV + 1], EEP[MAXV + 1];
   load_vgrid_smem(c_evg.e1, c_evg.e2, c_evg.epar, EE1, EE2, EEP);
-  __syncthreads();
   const double h = a.h, hh = 0.5 * h, h6 = h / 6.0, hsq2 = 0.5 * h * h;
   int tcur = -1;
-  int item = blockIdx.x;
-  while (item < a.nitems) {
-  const int t = a.blk_tube[item];
+  const int usz = a.chunk / a.sub;
+  ena_unit_prefix(a, UP, usz);  // (its barriers order the edges too)
+  const int nunits = UP[a.ntubes];
+  for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
+  int lo = 0, hi = a.ntubes;  // UP[lo] <= unit < UP[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (UP[mid] <= unit) lo = mid; else hi = mid;
+  }
+  const int t = lo;
   const TubeD &T = a.tubes[t];
   const int64_t nl = min(a.nena[t], T.ecap);
-  const int64_t beg = a.blk_start[item];
-  if (beg >= nl) {  // uniform over the block
-    item = next_own_item(a.tube_blk0[t + 1]);
-    continue;
-  }
-  const int64_t end = min(beg + (int64_t)a.chunk, nl);
+  const int64_t beg = (int64_t)(unit - UP[t]) * usz;
+  const int64_t end = min(beg + (int64_t)usz, nl);
   if (t != tcur) {
     __syncthreads();  // the previous tube's edges are no longer read
     for (int k = threadIdx.x; k <= T.nq; k += blockDim.x)
@@ -488,8 +608,7 @@ __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
     a.ena.vphs[e] = vphs;
     a.ena.qind[e] = qi;
   }
-  item += gridDim.x;
-  }  // work items
+  }  // units
 }
 
 // ENA moments of one master step from the ENA counts and (Vp, Vq, Vphi)
