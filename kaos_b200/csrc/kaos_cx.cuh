@@ -284,7 +284,9 @@ __device__ __forceinline__ void cx_convert_ion(const CxArgs &a, const TubeD &T,
 constexpr int CX_WARPS = 8;  // 256-thread blocks
 static_assert(CX_CHUNK <= (1 << 14), "conversion list packs (cell << 14) | index");
 __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) {
-  const TubeD &T = a.tubes[t];
+  // a copy: every barrier below would otherwise reload the fields from
+  // global memory, and the staging traffic evicts them from L1
+  const TubeD T = a.tubes[t];
   __syncthreads();  // the previous chunk of this block is done with smem
   extern __shared__ unsigned sm_[];
   unsigned *need = sm_;             // conversions this chunk owes per cell
@@ -415,7 +417,7 @@ __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) 
 
 // One resident wave of blocks; each chunk the scan listed is converted by
 // one block.
-__global__ void __launch_bounds__(256) k_cx_convert(CxArgs a) {
+__global__ void __launch_bounds__(256, 2) k_cx_convert(CxArgs a) {
   const uint32_t par = cx_step(a) & 1u;
   const int nc = (int)a.nchunk[par];
   if (blockIdx.x == 0 && threadIdx.x == 0) a.nchunk[par ^ 1u] = 0u;
@@ -517,7 +519,7 @@ __device__ __forceinline__ void ena_unit_prefix(const EnaArgs &a, int *UP, int u
 
 // A grid striding over the units holding ENAs (one ENA per thread), found
 // through the per-tube unit prefix; a unit's tube by binary search.
-__global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
+__global__ void __launch_bounds__(256, 3) k_push_ena(EnaArgs a) {
   extern __shared__ double sm[];
   double *E = sm;
   int *UP = (int *)(sm + a.ct_nqmax + 1);
@@ -537,8 +539,16 @@ __global__ void __launch_bounds__(256) k_push_ena(EnaArgs a) {
     if (UP[mid] <= unit) lo = mid; else hi = mid;
   }
   const int t = lo;
-  const TubeD &T = a.tubes[t];
-  const int64_t nl = min(a.nena[t], T.ecap);
+  // the tube's fields in registers: not reloaded after the barriers
+  struct { int nq; double sgn; int64_t coff, eoff; } T;
+  {
+    const TubeD &G = a.tubes[t];
+    T.nq = G.nq;
+    T.sgn = G.sgn;
+    T.coff = G.coff;
+    T.eoff = G.eoff;
+  }
+  const int64_t nl = min(a.nena[t], a.tubes[t].ecap);
   const int64_t beg = (int64_t)(unit - UP[t]) * usz;
   const int64_t end = min(beg + (int64_t)usz, nl);
   if (t != tcur) {
