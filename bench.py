@@ -707,6 +707,7 @@ def main():
                  "mixed_ms_per_step": l32["ms"], "fp64": l64["value"] * world,
                  "fp64_ms_per_step": l64["ms"],
                  "mixed_over_fp64": l32["value"] / l64["value"],
+                 "push_launch": l32["launch"],
                  "note": "both paths replayed from CUDA graphs"}
     batched = None
     if full and args.batched_tubes > 0:

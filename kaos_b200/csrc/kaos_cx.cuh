@@ -526,12 +526,14 @@ __global__ void __launch_bounds__(256, 3) k_push_ena(EnaArgs a) {
   // the ENA grid's edges for the bin searches in shared memory (threads
   // read different edges: constant memory would serialise them)
   __shared__ double EE1[MAXV + 1], EE2[MAXV + 1], EEP[MAXV + 1];
-  load_vgrid_smem(c_evg.e1, c_evg.e2, c_evg.epar, EE1, EE2, EEP);
   const double h = a.h, hh = 0.5 * h, h6 = h / 6.0, hsq2 = 0.5 * h * h;
   int tcur = -1;
   const int usz = a.chunk / a.sub;
-  ena_unit_prefix(a, UP, usz);  // (its barriers order the edges too)
+  ena_unit_prefix(a, UP, usz);
   const int nunits = UP[a.ntubes];
+  if ((int)blockIdx.x >= nunits) return;  // no unit for this block (uniform)
+  load_vgrid_smem(c_evg.e1, c_evg.e2, c_evg.epar, EE1, EE2, EEP);
+  __syncthreads();
   for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
   int lo = 0, hi = a.ntubes;  // UP[lo] <= unit < UP[hi]
   while (hi - lo > 1) {
