@@ -100,6 +100,20 @@ def summarize_clocks(samples):
             "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
 
 
+def with_clocks(fn, *a):
+    """fn(*a) with nvidia-smi clocks sampled while it runs; returns (result,
+    clocks summary)."""
+    stop, samples = threading.Event(), []
+    th = threading.Thread(target=clocks_sampler, args=(stop, samples), daemon=True)
+    th.start()
+    try:
+        r = fn(*a)
+    finally:
+        stop.set()
+        th.join(timeout=5)
+    return r, summarize_clocks(samples)
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -697,7 +711,7 @@ def main():
     large = None
     if full and args.large_particles > 0:
         lsteps = min(args.steps, 100)
-        l32 = run_large(args, KAOS_PREC_MIXED, lsteps)
+        l32, lclk = with_clocks(run_large, args, KAOS_PREC_MIXED, lsteps)
         l64 = run_large(args, KAOS_PREC_FP64, lsteps)
         large = {"workload": "large single tube: L=6, 512 cells 800 km to the equator, "
                              f"3D grid 64x64x96, {int(l32['n'])} O+ (90 % 0.3 eV Maxwellian "
@@ -707,12 +721,12 @@ def main():
                  "mixed_ms_per_step": l32["ms"], "fp64": l64["value"] * world,
                  "fp64_ms_per_step": l64["ms"],
                  "mixed_over_fp64": l32["value"] / l64["value"],
-                 "push_launch": l32["launch"],
+                 "push_launch": l32["launch"], "mixed_clocks": lclk,
                  "note": "both paths replayed from CUDA graphs"}
     batched = None
     if full and args.batched_tubes > 0:
         bsteps = min(args.steps, 100)
-        b32 = run_batched(args, KAOS_PREC_MIXED, bsteps)
+        b32, bclk = with_clocks(run_batched, args, KAOS_PREC_MIXED, bsteps)
         b64 = run_batched(args, KAOS_PREC_FP64, bsteps)
         batched = {"workload": f"{b32['ntubes']} batched uneven tubes: L uniform in [2, 8], "
                                "64-512 cells, 1e4-1e6 O+ each (log-uniform), "
@@ -722,13 +736,13 @@ def main():
                    "mixed_ms_per_step": b32["ms"], "fp64": b64["value"] * world,
                    "fp64_ms_per_step": b64["ms"],
                    "mixed_over_fp64": b32["value"] / b64["value"],
-                   "push_launch": b32["launch"],
+                   "push_launch": b32["launch"], "mixed_clocks": bclk,
                    "note": "one launch per kernel over (tube, chunk) work items; "
                            "both paths replayed from CUDA graphs"}
     species = None
     if full and args.c5:
         try:
-            c32 = run_c5(args, KAOS_PREC_MIXED, min(args.steps, 100))
+            c32, cclk = with_clocks(run_c5, args, KAOS_PREC_MIXED, min(args.steps, 100))
             c64 = run_c5(args, KAOS_PREC_FP64, min(args.steps, 100))
             species = {"workload": "64 tubes (L 3-7, 256 cells), O+ and H+ at 4:1 density as "
                                    f"{c32['entries']} entries, {int(c32['n'])} ions, charge "
@@ -742,6 +756,7 @@ def main():
                        "mixed_ms_per_step": c32["ms"], "fp64": c64["value"] * world,
                        "fp64_ms_per_step": c64["ms"],
                        "mixed_over_fp64": c32["value"] / c64["value"],
+                       "push_launch": c32["launch"], "mixed_clocks": cclk,
                        "note": "ion-steps per second of device time (host table "
                                "regeneration excluded); CUDA graphs except the master "
                                "steps that apply a move"}

@@ -872,8 +872,13 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   // for the comparisons, FP32 lookup tables for the first guess), after the
   // binning window; only the variants that bin are launched with room for
   // them (BINS_SMEM_BYTES)
-  double *VE1 = (double *)(((uintptr_t)(HC + nqmax + bin_win_size()) + 15) &
-                           ~(uintptr_t)15);
+  // (offset arithmetic from the shared array itself: a pointer rebuilt from
+  // an integer would lose its address space and the searches would issue
+  // generic loads)
+  const size_t ve_off =
+      ((size_t)((const char *)(HC + nqmax + bin_win_size()) - (const char *)sm) + 15) &
+      ~(size_t)15;
+  double *VE1 = (double *)((char *)sm + ve_off);
   double *VE2 = VE1 + (MAXV + 1), *VEP = VE2 + (MAXV + 1);
   VBinTab *VTS = (VBinTab *)(VEP + (MAXV + 1));
   VBinTab &VT1 = VTS[0], &VT2 = VTS[1], &VTP = VTS[2];
