@@ -445,6 +445,8 @@ const double *conv_table_ptr(const CellTables &c, int k) {
 // their ions with the old tables and descriptors (k_convect_many), then put
 // the new tables and descriptors in place (k_apply_tables) from one staging
 // copy.
+static int sm_count(kaos_handle *h);
+
 int apply_pending_tubes(kaos_handle *h) {
   static_assert(CONV_TABLES == CONV_NTAB, "table count");
   const int np = (int)h->pending.size();
@@ -490,7 +492,7 @@ int apply_pending_tubes(kaos_handle *h) {
   ca.ion = h->ion[h->cur];
   ca.ct = h->ct;
   ca.mixed = h->mixed;
-  k_convect_many<<<dim3(std::max(1, 148 * 16 / np), np), 256, 0, h->s>>>(ca);
+  k_convect_many<<<dim3(std::max(1, sm_count(h) * 16 / np), np), 256, 0, h->s>>>(ca);
   TableApplyArgs ta{};
   for (int k = 0; k < CONV_TABLES; ++k) ta.dst[k] = (double *)conv_table_ptr(h->ct, k);
   ta.stage = h->d_conv_stage;

@@ -917,13 +917,32 @@ __device__ __forceinline__ void convect_ions(const ConvArgs &a) {
   const TubeD &T = a.T;
   const int64_t nl = a.nlive[a.tube];
   const double ip_old = 1.0 / T.pG, ip_new = 1.0 / a.p_new;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nl;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // the next ion's Qindk1 and position are loaded before the current ion is
+  // moved, so their memory latency overlaps its Newton solves
+  int n_qi = DEAD;
+  double n_a = 0.0, n_b = 0.0;
+  if (i < nl) {
     const int64_t j = T.off + i;
-    if (a.ion.qind[j] == DEAD) continue;
+    n_qi = a.ion.qind[j];
+    if (a.mixed) n_a = a.ion.x[j];
+    else { n_a = a.ion.rho[j]; n_b = a.ion.z[j]; }
+  }
+  for (; i < nl; i += stride) {
+    const int64_t j = T.off + i;
+    const int qd = n_qi;
+    const double pa = n_a, pb = n_b;
+    if (i + stride < nl) {
+      const int64_t jn = j + stride;
+      n_qi = a.ion.qind[jn];
+      if (a.mixed) n_a = a.ion.x[jn];
+      else { n_a = a.ion.rho[jn]; n_b = a.ion.z[jn]; }
+    }
+    if (qd == DEAD) continue;
     double q, u_old;
     if (a.mixed) {
-      const double x = a.ion.x[j];
+      const double x = pa;
       if (x < XDEAD_LIM) continue;
       const int c = x_cell(x, T.nq);
       const int64_t g = T.coff + c;
@@ -931,7 +950,7 @@ __device__ __forceinline__ void convect_ions(const ConvArgs &a) {
       q = a.ct.qGL[g] + o * (a.ct.qGH[g] - a.ct.qGL[g]);
       u_old = quartic_newton_conv(q, ip_old, a.ct.uL[g] + o * (a.ct.uH[g] - a.ct.uL[g]), 8);
     } else {
-      const double rho = a.ion.rho[j], z = a.ion.z[j];
+      const double rho = pa, z = pb;
       const double r2 = rho * rho + z * z, r = sqrt(r2);
       q = (RE * RE) * (z / r) / r2;
       u_old = r / RE;
