@@ -177,7 +177,10 @@ typedef struct kaos_handle kaos_handle;
  * MOMENTFILTERflag = 1 every moving-average window must be odd, >= 3 and at
  * most the tube's cell count (MomentFilterSub reads that many cells around
  * each cell; the reference's guard, NqICT >= (Pt-1)/2, lets shorter tubes
- * read outside the array). */
+ * read outside the array).  With QEXCHANGEflag = 1 at most KAOS_MAX_TUBES_CX
+ * tubes (the ENA push holds a per-tube prefix in shared memory); more
+ * return KAOS_ERR_PARAM. */
+#define KAOS_MAX_TUBES_CX 32768
 int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
                 int32_t ntubes, const kaos_vgrid_c *vg, kaos_handle **out);
 

@@ -1154,6 +1154,7 @@ const char *kaos_last_error(kaos_handle *h) {
 int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
                 int32_t ntubes, const kaos_vgrid_c *vgc, kaos_handle **out) {
   if (!p || !tubes || !vgc || !out || ntubes < 1) return KAOS_ERR_PARAM;
+  if (p->QEXCHANGEflag == 1 && ntubes > KAOS_MAX_TUBES_CX) return KAOS_ERR_PARAM;
   *out = nullptr;
   kaos_handle *h = new kaos_handle();
   h->P = *p;

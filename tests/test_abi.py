@@ -47,3 +47,17 @@ def test_version_and_null_handle(lib):
     # null arguments are rejected before any device work
     assert lib.kaos_create(None, None, 0, None, None) == 1
     assert lib.kaos_step(None, 1) == 1
+
+
+def test_charge_exchange_tube_limit(lib):
+    """With charge exchange on, more than KAOS_MAX_TUBES_CX tubes are
+    rejected before any device work (the ENA push keeps a per-tube prefix in
+    shared memory)."""
+    import ctypes as C
+    from kaos_b200.model_input import KaosTube, KaosVGrid, ModelInput
+    src = open(os.path.join(ROOT, "include", "kaos_gpu.h")).read()
+    limit = int(re.search(r"#define KAOS_MAX_TUBES_CX (\d+)", src).group(1))
+    p = ModelInput(QEXCHANGEflag=1).to_c()
+    tube, vg, out = KaosTube(), KaosVGrid(), C.c_void_p()
+    rc = lib.kaos_create(C.byref(p), C.byref(tube), limit + 1, C.byref(vg), C.byref(out))
+    assert rc == 1 and not out.value

@@ -213,6 +213,51 @@ def test_charge_exchange_and_ena_push(mixed):
         assert np.max(np.abs(a - b)) / scale < TRAJ_TOL, k
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_charge_exchange_many_tubes(mixed):
+    """300 small tubes with a dense exosphere in one solver: most cells
+    convert ions every step (several per cell: the ranked selection), the
+    scan and conversion kernels work on many tubes at once, and the ENA
+    push builds its per-tube unit prefix over more tubes than it has
+    threads (two tubes a thread).  Each tube matches its own oracle run:
+    the ion and ENA counts and the Poisson means exactly, the ENA states to
+    1e-12 (FP64 path)."""
+    from kaos_b200.grids import TubeSpec, make_tube, make_vgrid
+    from kaos_b200.model_input import ModelInput
+    mi = ModelInput(h=0.01, ndatfac=4, ION2VPERPflag=1, QEXCHANGEflag=1)
+    if mixed:
+        mi.precision = KAOS_PREC_MIXED
+    vg = make_vgrid(True, 16, 16, 24, 8e3)
+    nt = 300
+    specs = [TubeSpec(L=3.0 + 3.0 * k / nt, nq=16, n_particles=300, q_ub=0.15,
+                      H=600e3, neut_n0=3e18, neut_H=300e3) for k in range(nt)]
+    tubes = [make_tube(sp, mi) for sp in specs]
+    s = Solver(mi, tubes, vg)
+    inits = []
+    for k, (sp, t) in enumerate(zip(specs, tubes)):
+        init = grids.initial_particles(t, sp, mi, seed=500 + k)
+        inits.append(init)
+        s.load(k, *init)
+    s.step(10)
+    total_enas = 0
+    for k, (sp, t) in enumerate(zip(specs, tubes)):
+        o = Oracle(mi, t, vg)
+        o.load(*inits[k])
+        o.step(10)
+        assert s.count(k) == o.count(), k
+        np.testing.assert_array_equal(s.moments(14, k), o.moments(14))  # nuPoi
+        total_enas += o.count()[1]
+        if mixed:
+            continue
+        eo, es = o.enas(), s.enas(k)
+        io, is_ = np.argsort(eo["z"]), np.argsort(es["z"])
+        for key in ("x", "y", "z", "vx", "vy", "vz"):
+            a, b = es[key][is_], eo[key][io]
+            scale = max(np.max(np.abs(eo["z"])) if key in "xyz" else np.max(np.abs(eo["vz"])), 1.0)
+            assert np.max(np.abs(a - b)) / scale < TRAJ_TOL, (k, key)
+    assert total_enas > 100 * nt
+
+
 def test_batched_uneven_tubes_one_launch():
     """Several tubes of different L-shell, cell count and particle count
     advance together (one launch per kernel over a (tube, chunk) map); each
