@@ -10,8 +10,10 @@
 //
 // Selection on the GPU keeps the index order exactly: the push that writes
 // Qindk1 also counts, per selection chunk of CX_CHUNK ions, the ions of each
-// cell (flush_cx_counts); an exclusive scan over chunks per cell follows,
-// then an in-order walk of only those chunks that hold converted ions.
+// cell (flush_cx_counts); a scan over chunks per cell follows (what each
+// chunk still owes each cell, and the list of chunks that convert), then a
+// parallel selection of the first owed ions per cell in each listed chunk,
+// equal to a walk in index order.
 #pragma once
 #include "kaos_push.cuh"
 
