@@ -134,7 +134,10 @@ def build_workload(precision, n_part=N_PART, heating=True, collisions=True,
 
 
 def bytes_per_particle_step(mixed, heating, collisions):
-    """Algorithmic HBM bytes per ion per ordinary step (reads + writes)."""
+    """Algorithmic HBM bytes per ion per ordinary step (reads + writes).
+    `collisions`: the charge exchange converts ions in this interval (an
+    idle interval -- no converting cell, no ENA -- stores no Qindk1 or k4
+    point at its ordinary steps)."""
     if mixed:  # FP64 state: cell coordinate, V||, (Vperp1, Vperp2); FP32 AEA, AG
         rd, wr = 8 + 8 + 16 + 8, 8 + 8 + (16 if heating else 0)
         if collisions:  # Qindk1 + q at k4 (FP32) written for the charge exchange
@@ -197,13 +200,13 @@ def run_ours(args, precision, graph=False, ndatfac=NDATFAC, steps=None):
     s.step(steps)
     ms, launches = s.timing()
     pms, pl = s.push_timing()  # events around each push launch
-    n1, _ = s.count()
+    n1, ne = s.count()
     nmean = 0.5 * (n0 + n1)
     value = nmean * steps / (ms * 1e-3)
     push_ms = pms / max(pl, 1)
     return dict(value=value, ms=ms, launches=launches, n=nmean, push_ms=push_ms,
                 t_load=t_load, solver=s, init=init, tube=tube, mi=mi,
-                launch=s.launch())
+                launch=s.launch(), enas=ne)
 
 
 def run_large(args, precision, steps):
@@ -701,7 +704,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * r32["n"] * args.steps / (ms * 1e-3)
-    mixed_bytes = bytes_per_particle_step(True, not args.no_heating, args.collisions)
+    # (this tube's exosphere forms no ENA: its intervals are idle)
+    cx_active = args.collisions and r32["enas"] > 0
+    mixed_bytes = bytes_per_particle_step(True, not args.no_heating, cx_active)
     achieved = mixed_bytes * r32["n"] / (r32["push_ms"] * 1e-3) / 1e9
     achieved_frozen = FROZEN_MIXED_BYTES * r32["n"] / (r32["push_ms"] * 1e-3) / 1e9
     peak, peak_kind = peaks()
@@ -814,6 +819,14 @@ def main():
                          "achieved_at_frozen_bytes": achieved_frozen,
                          "frac_at_frozen_bytes": achieved_frozen / peak,
                          "bytes_note": "the mixed state is FP64 (cell coordinate, V||, "
+                                       "Vperp pair: 32 B read + 32 B written) so that every "
+                                       "moment matches the FP64 path; the frozen 48 B "
+                                       "counted the earlier FP32 state; Qindk1 and the k4 "
+                                       "point (8 B) are stored only in intervals whose "
+                                       "charge exchange converts ions (none here: the "
+                                       "exosphere forms no ENA)"
+                                       if not cx_active else
+                                       "the mixed state is FP64 (cell coordinate, V||, "
                                        "Vperp pair: 32 B read + 32 B written) so that every "
                                        "moment matches the FP64 path; the frozen 48 B "
                                        "counted the earlier FP32 state",

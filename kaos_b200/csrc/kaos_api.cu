@@ -137,7 +137,7 @@ struct kaos_handle {
   int *d_tube_done = nullptr;  // per tube: charge-exchange cell scans done
   int *d_cx_list = nullptr, *d_cx_nlist = nullptr, *d_tube_active = nullptr;
   int *d_cx_chunks = nullptr;       // chunks with conversions this step
-  unsigned *d_cx_nchunk = nullptr;  // their count, by step parity
+  unsigned *d_cx_nchunk = nullptr;  // their count, blocks that read it
   int cx_blocks = 0;                // k_cx_convert: one resident wave
   // convection: device staging of the moves of one master step (allocated
   // at the first move) and its host side
@@ -162,6 +162,15 @@ struct kaos_handle {
   uint32_t *d_step = nullptr;
   int capturing = 0;
   int dstep_valid = 0;
+  // charge exchange idle for the current master interval: the last master
+  // step listed no converting cell and left no ENA.  Its ordinary steps
+  // then launch no selection, conversion or ENA push, the pushes count no
+  // Qindk1 for the selection and store no Qindk1 or k4 point for it (master
+  // steps keep all of it: their moments decide the next interval).  Decided
+  // on the host from cx_stat, copied back after every master step.
+  int cx_idle = 0;
+  int cx_stat_pending = 0;
+  int64_t *cx_stat = nullptr;  // pinned: [0] listed cells, [1..ntubes] ENAs
   struct StepGraph {
     cudaGraphExec_t exec = nullptr;
     int64_t launches = 0;
@@ -534,6 +543,11 @@ int launch_moments(kaos_handle *h, uint32_t nn) {
     k_cx_list<<<(int)((h->ncell + 255) / 256), 256, 0, h->s>>>(cx_args(h), h->d_cell_tube,
                                                              h->ncell);
     h->launches += 2;
+    // the next interval's activity (read on the host before its first step)
+    CK(cudaMemcpyAsync(h->cx_stat, h->d_cx_nlist, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaMemcpyAsync(h->cx_stat + 1, h->d_nena, h->ntubes * sizeof(int64_t),
+                       cudaMemcpyDeviceToHost, h->s));
+    h->cx_stat_pending = 1;
     if (nn > 1) {  // ENA statistics from the second master step on
       k_ena_moments<<<(int)((h->ncell + cells_per_block - 1) / cells_per_block), 256, 0, h->s>>>(
           h->d_tubes, h->d_cell_tube, h->ct, h->acc);
@@ -753,8 +767,6 @@ CxArgs cx_args(kaos_handle *h) {
   a.nlist = h->d_cx_nlist;
   a.chunk_list = h->d_cx_chunks;
   a.nchunk = h->d_cx_nchunk;
-  a.step = (uint32_t)(h->n + 1);
-  a.dstep = h->capturing ? h->d_step : nullptr;
   a.tube_active = h->d_tube_active;
   a.rank = h->rank;
   a.nranks = h->nranks;
@@ -914,6 +926,19 @@ __global__ void k_sample_rng(SampleArgs a) {
 __global__ void k_set_step(uint32_t *d, uint32_t v) { *d = v; }
 __global__ void k_next_step(uint32_t *d) { *d += 1u; }
 
+// The charge-exchange activity of the master interval that starts at the
+// next step, from the list length and ENA counts the last master step
+// copied back (one host wait per master interval, outside any capture).
+int resolve_cx_idle(kaos_handle *h) {
+  if (!h->cx_stat_pending) return KAOS_OK;
+  CK(cudaStreamSynchronize(h->s));
+  int64_t enas = 0;
+  for (int t = 0; t < h->ntubes; ++t) enas += h->cx_stat[1 + t];
+  h->cx_idle = (*(const int *)h->cx_stat == 0 && enas == 0) ? 1 : 0;
+  h->cx_stat_pending = 0;
+  return KAOS_OK;
+}
+
 // One computational step n = h->n + 1.
 int step_once(kaos_handle *h) {
   const int64_t n = h->n + 1;
@@ -960,7 +985,12 @@ int step_once(kaos_handle *h) {
     for (auto &pt : h->pending) h->applied.push_back(std::move(pt));
     h->pending.clear();
   }
-  if (qx && (rc = launch_cx(h))) return rc;
+  // an idle interval converts nothing: no selection; its master step still
+  // counts Qindk1 for the next interval, into rows cleared here
+  const bool cx_on = qx && !h->cx_idle;
+  if (cx_on && (rc = launch_cx(h))) return rc;
+  if (qx && !cx_on && master)
+    CK(cudaMemsetAsync(h->d_cxc, 0, (size_t)h->ncx * max_nq(h) * sizeof(unsigned), h->s));
   if (master) {
     const int compact = bc_decide(h, n);
     if ((rc = launch_boundary(h, compact))) return rc;
@@ -973,13 +1003,14 @@ int step_once(kaos_handle *h) {
   p.step = (uint32_t)n;
   p.bin = master;
   p.prologue = master;
-  p.write_qind = (!h->mixed) || next_master || qx || h->export_on;
-  p.write_qk4 = next_master || qx;
-  if (qx) p.cxc = h->d_cxc;
+  const bool cx_rec = cx_on || (qx && master);  // state the selection reads
+  p.write_qind = (!h->mixed) || next_master || cx_rec || h->export_on;
+  p.write_qk4 = next_master || cx_rec;
+  if (cx_rec) p.cxc = h->d_cxc;
   // the ENA push (independent of the ions) runs beside the ion push
-  if (qx && (rc = launch_push_ena(h, master))) return rc;
+  if (cx_on && (rc = launch_push_ena(h, master))) return rc;
   if ((rc = launch_push(h, p))) return rc;
-  if (qx && (rc = join_push_ena(h))) return rc;
+  if (cx_on && (rc = join_push_ena(h))) return rc;
   if (master) {
     if (h->P.LBCONDITIONflag == 1 && (rc = launch_inject(h, 0))) return rc;
     if (h->P.UBCONDITIONflag == 1 && (rc = launch_inject(h, 1))) return rc;
@@ -1092,7 +1123,8 @@ int graph_steps(kaos_handle *h, int g) {
                        ((uint64_t)compact << 21) |
                        ((uint64_t)is_master(h, n + 1) << 17) |
                        ((uint64_t)h->cur << 18) | ((uint64_t)h->ecur << 19) |
-                       ((uint64_t)(h->export_on != 0) << 20);
+                       ((uint64_t)(h->export_on != 0) << 20) |
+                       ((uint64_t)(h->cx_idle != 0) << 22);
   if (!h->dstep_valid) {
     k_set_step<<<1, 1, 0, h->s>>>(h->d_step, (uint32_t)h->n);
     h->launches++;
@@ -1107,7 +1139,10 @@ int graph_steps(kaos_handle *h, int g) {
       const int64_t m = h->n + 1;
       if (is_master(h, m)) {  // launch_boundary / launch_boundary_ena swaps
         bc_after(h, bc_decide(h, m));
-        if (h->P.QEXCHANGEflag == 1) h->ecur = 1 - h->ecur;
+        if (h->P.QEXCHANGEflag == 1) {
+          h->ecur = 1 - h->ecur;
+          h->cx_stat_pending = 1;  // the graph copied the next interval's stat
+        }
       }
       h->n = m;
     }
@@ -1477,6 +1512,8 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
         (rc = dalloc(h, &h->d_cxc, cxt.size() * (size_t)max_nq(h))) ||
         (rc = dalloc(h, &h->d_cxo, cxt.size() * (size_t)max_nq(h))))
       return rc;
+    CK(cudaMallocHost((void **)&h->cx_stat, (size_t)(ntubes + 1) * sizeof(int64_t)));
+    memset(h->cx_stat, 0, (size_t)(ntubes + 1) * sizeof(int64_t));
   }
   // kernels whose per-tube shared tables may exceed the default 48 KB
   {
@@ -1757,6 +1794,7 @@ int kaos_step(kaos_handle *h, int64_t nsteps) {
   for (int64_t k = 0; k < nsteps;) {
     const int64_t n = h->n + 1;
     int rc;
+    if ((rc = resolve_cx_idle(h))) return rc;
     if (h->tune_pending && n >= 2 && (rc = autotune(h))) return rc;
     if (!h->graph || n == 1 || h->reduce_fn ||
         (!h->pending.empty() && is_master(h, n))) {  // host work between kernels
@@ -2078,6 +2116,7 @@ void kaos_destroy(kaos_handle *h) {
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
   if (h->conv_host.stage) cudaFreeHost(h->conv_host.stage);
+  if (h->cx_stat) cudaFreeHost(h->cx_stat);
   if (h->efork) cudaEventDestroy(h->efork);
   if (h->ejoin) cudaEventDestroy(h->ejoin);
   if (h->s2) cudaStreamDestroy(h->s2);

@@ -38,22 +38,17 @@ struct CxArgs {
   int *cxend;                // per cell (all tubes): chunks >= cxend convert none
   int *tube_done;            // per tube: cell scans finished this step
   int *list, *nlist;         // cells with conversions (need > 0), their count
-  // chunks with conversions this step, appended by the scan; their count
-  // by step parity (the conversion kernel of step n resets step n+1's)
+  // chunks with conversions this step, appended by the scan; [0] their
+  // count, [1] conversion blocks that have read it (the last one resets
+  // both for the next step)
   int *chunk_list;
   unsigned *nchunk;
-  uint32_t step;
-  const uint32_t *dstep;     // graph replay: the step number in device memory
   int *tube_active;          // per tube: listed cells
   int nqmax, mixed;
   int ncx;                   // selection chunks (all tubes)
   int rank, nranks;          // this rank's share of a split tube's conversions
   uint32_t *status;
 };
-
-__device__ __forceinline__ uint32_t cx_step(const CxArgs &a) {
-  return a.dstep ? *a.dstep : a.step;
-}
 
 // Ions a cell converts at this step on this rank: its share of
 // nint(nuIonNeutPoiT) when the tube is split over nranks.
@@ -102,7 +97,7 @@ __device__ __forceinline__ void cx_scan_cell(const CxArgs &a, int t, int k,
       a.cxo[(int64_t)c * a.nqmax + k] = s < need ? need - s : 0u;
       // the first cell to give the chunk a conversion lists it
       if (n && s < need && atomicAdd(&a.cxconv[c], min(n, need - s)) == 0u)
-        a.chunk_list[atomicAdd(a.nchunk + (cx_step(a) & 1u), 1u)] = c;
+        a.chunk_list[atomicAdd(a.nchunk, 1u)] = c;
     }
     __syncthreads();
     if (threadIdx.x == 0) base += tot;
@@ -420,9 +415,17 @@ __device__ __forceinline__ void cx_convert_chunk(const CxArgs &a, int c, int t) 
 // One resident wave of blocks; each chunk the scan listed is converted by
 // one block.
 __global__ void __launch_bounds__(256, 2) k_cx_convert(CxArgs a) {
-  const uint32_t par = cx_step(a) & 1u;
-  const int nc = (int)a.nchunk[par];
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.nchunk[par ^ 1u] = 0u;
+  __shared__ int nc_s;
+  if (threadIdx.x == 0) {
+    nc_s = (int)__ldcg(a.nchunk);
+    __threadfence();
+    if (atomicAdd(a.nchunk + 1, 1u) == gridDim.x - 1) {  // every block has read it
+      a.nchunk[0] = 0u;
+      a.nchunk[1] = 0u;
+    }
+  }
+  __syncthreads();
+  const int nc = nc_s;
   for (int k = blockIdx.x; k < nc; k += gridDim.x) {
     const int c = a.chunk_list[k];
     cx_convert_chunk(a, c, a.cx_tube[c]);
