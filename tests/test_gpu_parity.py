@@ -214,6 +214,46 @@ def test_charge_exchange_and_ena_push(mixed):
 
 
 @pytest.mark.parametrize("mixed", [False, True])
+def test_charge_exchange_idle_then_active(mixed):
+    """A thin exosphere: the master steps at 1 and 4 list no converting cell
+    and leave no ENA, so steps 2-8 run idle (no selection, conversion or ENA
+    push; no Qindk1 or k4 stores at the ordinary steps); the master steps
+    still count Qindk1 into cleared rows, and the Poisson draw at 8 lists
+    two cells: conversions start at step 9.  The converted ions, the ENA
+    states and every count match the oracle, which selects at every step."""
+    from kaos_b200.grids import TubeSpec, make_tube, make_vgrid
+    from kaos_b200.model_input import ModelInput
+    mi = ModelInput(h=0.01, ndatfac=4, ION2VPERPflag=1, QEXCHANGEflag=1, ICRflag=1)
+    if mixed:
+        mi.precision = KAOS_PREC_MIXED
+    vg = make_vgrid(True, 16, 16, 24, 8e3)
+    sp = TubeSpec(L=4.0, nq=32, n_particles=3000, q_ub=0.15, H=600e3, neut_n0=3e16,
+                  neut_H=300e3, heat_rate_eV_s=200.0)
+    tube = make_tube(sp, mi)
+    init = grids.initial_particles(tube, sp, mi, seed=9)
+    o = Oracle(mi, tube, vg)
+    o.load(*init)
+    s = Solver(mi, [tube], vg)
+    s.load(0, *init)
+    seen = []
+    for _ in range(6):  # master steps at 4, 8, ..., 24
+        o.step(4)
+        s.step(4)
+        assert s.count() == o.count()
+        np.testing.assert_array_equal(s.moments(14), o.moments(14))  # nuPoi
+        seen.append(o.count()[1])
+    assert seen[:2] == [0, 0] and seen[-1] > 0  # idle first, converting later
+    if mixed:
+        return
+    eo, es = o.enas(), s.enas()
+    io, is_ = np.argsort(eo["z"]), np.argsort(es["z"])
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        a, b = es[k][is_], eo[k][io]
+        scale = max(np.max(np.abs(eo["z"])) if k in "xyz" else np.max(np.abs(eo["vz"])), 1.0)
+        assert np.max(np.abs(a - b)) / scale < TRAJ_TOL, k
+
+
+@pytest.mark.parametrize("mixed", [False, True])
 def test_charge_exchange_many_tubes(mixed):
     """300 small tubes with a dense exosphere in one solver: most cells
     convert ions every step (several per cell: the ranked selection), the
