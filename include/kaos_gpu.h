@@ -267,7 +267,11 @@ int kaos_set_export(kaos_handle *h, int32_t on);
 
 /* Copy the ion state of a tube to host arrays of length n (n must equal the
  * live ion count): field-line q, parallel velocity, Vperp1, Vperp2 and the
- * start-of-step cell index Qindk1 (0-based, -1/-2 escape sentinels).  Any
+ * start-of-step cell index Qindk1 (0-based, -1/-2 escape sentinels).  In
+ * mixed precision Qindk1 is stored only by the pushes whose successor reads
+ * it (the step before a master step, every step of an interval whose charge
+ * exchange converts ions, or every step with export on): elsewhere it is
+ * that of the last such step.  Any
  * pointer may be NULL.  Order is the reference particle order.  The state
  * is gathered on the device into the spare particle buffers (no device
  * allocation) and copied once per array. */
