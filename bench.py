@@ -328,17 +328,19 @@ def moment_errors(a, b):
     return out
 
 
-def error_run(args, heating, collisions, n_part, with_oracle=False):
-    """The mixed path against the FP64 path (and, on a small sample, the
-    FP64 oracle) over the configuration's 500 steps from the same ions and
-    random streams: the error of every moment at every master step from
-    step 100 on (maximum over those steps) and at the last one."""
+def error_run(args, heating, collisions, n_part, with_oracle=False, mixed_prec=None):
+    """The mixed path (KAOS_PREC_MIXED, or the precision mode given) against
+    the FP64 path (and, on a small sample, the FP64 oracle) over the
+    configuration's 500 steps from the same ions and random streams: the
+    error of every moment at every master step from step 100 on (maximum
+    over those steps) and at the last one."""
     from kaos_b200 import grids
     from kaos_b200.lib import Solver
     from kaos_b200.model_input import KAOS_PREC_FP64, KAOS_PREC_MIXED
+    mixed = KAOS_PREC_MIXED if mixed_prec is None else mixed_prec
     runs = {}
     init = None
-    for prec in (KAOS_PREC_FP64, KAOS_PREC_MIXED):
+    for prec in (KAOS_PREC_FP64, mixed):
         mi, spec, tube, vg = grids.config_c2(n_particles=n_part, heating=heating,
                                              collisions=collisions, precision=prec,
                                              ndatfac=NDATFAC)
@@ -367,10 +369,10 @@ def error_run(args, heating, collisions, n_part, with_oracle=False):
         done += k
         if done < 100 or done % NDATFAC:
             continue
-        last = moment_errors(runs[KAOS_PREC_MIXED], runs[KAOS_PREC_FP64])
+        last = moment_errors(runs[mixed], runs[KAOS_PREC_FP64])
         worst = {m: max(worst[m], last[m]) for m in MOMENT_NAMES}
         if orc is not None:
-            last_o = moment_errors(runs[KAOS_PREC_MIXED], orc)
+            last_o = moment_errors(runs[mixed], orc)
             worst_o = {m: max(worst_o[m], last_o[m]) for m in MOMENT_NAMES}
     for s in runs.values():
         s.close()
@@ -387,9 +389,11 @@ def moment_error_block(args):
     """Every moment of the mixed path against the FP64 path on the full
     tube (1e7 ions), with heating and collisions on (the timed workload) and
     off, and against the FP64 oracle on a 2e4-ion sample of the tube."""
+    from kaos_b200.model_input import KAOS_PREC_MIXED_K64
     on = error_run(args, True, True, args.particles)
     off = error_run(args, False, False, args.particles)
     orc = error_run(args, True, True, 20000, with_oracle=True)
+    k64 = error_run(args, True, True, args.particles, mixed_prec=KAOS_PREC_MIXED_K64)
     def mx(d):
         return max(d.values())
     return {"heating_collisions_on": on, "heating_collisions_off": off,
@@ -397,6 +401,8 @@ def moment_error_block(args):
             "max_vs_fp64_on": mx(on["vs_fp64_max_over_master_steps_from_100"]),
             "max_vs_fp64_off": mx(off["vs_fp64_max_over_master_steps_from_100"]),
             "max_vs_oracle_sample": mx(orc["vs_oracle_max_over_master_steps_from_100"]),
+            "kick64_heating_collisions_on": k64,
+            "max_vs_fp64_on_kick64": mx(k64["vs_fp64_max_over_master_steps_from_100"]),
             "definition": "max over cells |m_mixed - m_ref| / max over cells |m_ref|, "
                           "per moment, at every master step from step 100 to 500"}
 
@@ -608,6 +614,9 @@ def main():
     ap.add_argument("--no-heating", action="store_true")
     ap.add_argument("--no-collisions", dest="collisions", action="store_false")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--kick64", action="store_true",
+                    help="with --only mixed: time the mixed path with the heating kick "
+                         "in FP64 (precision mode KAOS_PREC_MIXED_K64)")
     ap.add_argument("--large-particles", type=int, default=100_000_000,
                     help="ions of the large single-tube line (0: skip it)")
     ap.add_argument("--batched-tubes", type=int, default=256,
@@ -669,7 +678,7 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    from kaos_b200.model_input import KAOS_PREC_FP64, KAOS_PREC_MIXED
+    from kaos_b200.model_input import KAOS_PREC_FP64, KAOS_PREC_MIXED, KAOS_PREC_MIXED_K64
     full = args.only == "all"
     # FP64 path first (reported beside the headline)
     r64 = run_ours(args, KAOS_PREC_FP64) if full else None
@@ -680,7 +689,8 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     th.start()
-    r32 = run_ours(args, KAOS_PREC_MIXED)
+    r32 = run_ours(args, KAOS_PREC_MIXED_K64 if (args.kick64 and not full)
+                   else KAOS_PREC_MIXED)
     torch.cuda.synchronize()
     stop.set()
     if full:
@@ -689,6 +699,12 @@ def main():
     # error of every moment of the mixed path against the FP64 path and the
     # FP64 oracle (same ions, same random streams), master steps 100-500
     moment_error = moment_error_block(args) if full else None
+    # the mixed path with the heating kick in FP64 (KAOS_PREC_MIXED_K64: the
+    # variant whose moments keep the FP64 path's bins with heating on)
+    rk = None
+    if full:
+        rk = run_ours(args, KAOS_PREC_MIXED_K64)
+        rk["solver"].close()
     # the same steps replayed from CUDA graphs, and at cadence 1 (every step
     # a master step: removal/injection, fields, counts and moments each step)
     rg = rc1 = None
@@ -795,6 +811,16 @@ def main():
             "mixed_over_fp64": value / (r64["value"] * world) if full else None,
             "fp64_roofline": fp64_pipe_roofline(r64["value"]) if full else None,
             "mixed_push_ms": r32["push_ms"],
+            "kick64": None if not full else {
+                "value": rk["value"] * world, "ms_per_step": rk["ms"] / args.steps,
+                "push_ms": rk["push_ms"],
+                "over_fp64": rk["value"] / r64["value"],
+                "push_launch": rk["launch"],
+                "moment_error_vs_fp64_max": moment_error["max_vs_fp64_on_kick64"],
+                "note": "precision mode KAOS_PREC_MIXED_K64: the mixed path with the "
+                        "heating kick in FP64 (the FP64 path's formula and draw), "
+                        "same workload; its moment error is in "
+                        "moment_error_vs_fp64.kick64_heating_collisions_on"},
             "large": large,
             "batched": batched,
             "species_ena_convection": species,

@@ -47,6 +47,10 @@ extern "C" {
 #define KAOS_PREC_MIXED 1 /* FP32 forces, RK stages and heating kicks on
                              FP64 state (position, V||, Vperp); FP64 quartic,
                              renormalisation and reductions                  */
+#define KAOS_PREC_MIXED_K64 2 /* KAOS_PREC_MIXED with the WaveHeatingSub kick
+                             (_8_1_1_0_WaveHeating.f90:72-312) in FP64: the
+                             FP64 path's formula and random draw on the FP64
+                             state, so heated runs keep the FP64 path's bins */
 
 /* ---- moment selectors for kaos_get_moments ------------------------------ */
 #define KAOS_M0 0        /* M0phRT      density [m^-3]                      */
@@ -440,7 +444,8 @@ void kaos_destroy(kaos_handle *h);
  * loads the library until the process exits.  nq > 512 or more than 128
  * velocity cells per axis return KAOS_ERR_CAPACITY.  The first call on a
  * device looks up that array's device address (cudaGetSymbolAddress) and
- * the device's SM count with the device current.  All calls share the
+ * the device's SM count with the device current; make that first call on
+ * each device before any stream capture begins.  All calls share the
  * array and each clears it first, so calls that overlap on the GPU race:
  * serialise them.
  */

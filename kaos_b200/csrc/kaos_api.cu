@@ -89,6 +89,7 @@ struct kaos_handle {
   kaos_params_c P{};
   int ntubes = 0;
   int mixed = 0;
+  int kick64 = 0;  // mixed push with the FP64 heating kick
   int three_d = 1;
   int nv = 0;
   int64_t ncell = 0;
@@ -371,17 +372,21 @@ int launch_push(kaos_handle *h, const PushArgs &a) {
   // the budgets: 64 registers (4 blocks of 256 threads per SM), 80 (3
   // blocks of 256), 72 (7 blocks of 128)
   using KFn = void (*)(PushArgs);
-#define KAOS_K32(M, D)                                                        \
-  {{k_push32<D, 256, 4, false, M>, k_push32<D, 256, 4, true, M>},            \
-   {k_push32<D, 256, 3, false, M>, k_push32<D, 256, 3, true, M>},            \
-   {k_push32<D, 128, 7, false, M>, k_push32<D, 128, 7, true, M>}}
-  static const KFn k32[2][2][3][2] = {{KAOS_K32(false, false), KAOS_K32(false, true)},
-                                      {KAOS_K32(true, false), KAOS_K32(true, true)}};
+#define KAOS_K32(M, D, K)                                                     \
+  {{k_push32<D, 256, 4, false, M, K>, k_push32<D, 256, 4, true, M, K>},      \
+   {k_push32<D, 256, 3, false, M, K>, k_push32<D, 256, 3, true, M, K>},      \
+   {k_push32<D, 128, 7, false, M, K>, k_push32<D, 128, 7, true, M, K>}}
+  // [FP64 heating kick][master-step work][three_d][register budget][persistent]
+  static const KFn k32[2][2][2][3][2] = {
+      {{KAOS_K32(false, false, false), KAOS_K32(false, true, false)},
+       {KAOS_K32(true, false, false), KAOS_K32(true, true, false)}},
+      {{KAOS_K32(false, false, true), KAOS_K32(false, true, true)},
+       {KAOS_K32(true, false, true), KAOS_K32(true, true, true)}}};
 #undef KAOS_K32
   const int nt = rs == 2 ? 128 : PUSH_THREADS;
   static const KFn k64[2][2] = {{k_push64<false, false>, k_push64<false, true>},
                                 {k_push64<true, false>, k_push64<true, true>}};
-  const KFn fn = h->mixed ? k32[ms][h->three_d][rs][ps] : k64[h->three_d][ps];
+  const KFn fn = h->mixed ? k32[h->kick64][ms][h->three_d][rs][ps] : k64[h->three_d][ps];
   if (smem > 48 * 1024)
     CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int &occ = h->occ[h->mixed ? ms : 0][rs];
@@ -1199,7 +1204,13 @@ int kaos_create(const kaos_params_c *p, const kaos_tube_c *tubes,
     *out = h;
     return rc;
   }
-  h->mixed = p->precision == KAOS_PREC_MIXED;
+  if (p->precision != KAOS_PREC_FP64 && p->precision != KAOS_PREC_MIXED &&
+      p->precision != KAOS_PREC_MIXED_K64) {
+    *out = h;
+    return fail(h, KAOS_ERR_PARAM, "unknown precision mode %d", (int)p->precision);
+  }
+  h->mixed = p->precision == KAOS_PREC_MIXED || p->precision == KAOS_PREC_MIXED_K64;
+  h->kick64 = p->precision == KAOS_PREC_MIXED_K64;
   h->three_d = p->ION2VPERPflag == 1;
   h->ntubes = ntubes;
   h->id_base.assign(ntubes, 0);

@@ -842,8 +842,10 @@ __device__ __forceinline__ void start_bins(const PushArgs &a, const Ions &I,
 // increment added to the FP64 V||.
 // NT threads per block and MINB resident blocks per SM set the register
 // budget (256 x 4: 64 registers, 256 x 3: 80, 128 x 7: 72); the autotuner
-// picks one.
-template <bool THREE_D, int NT, int MINB, bool PERSIST, bool MASTER>
+// picks one.  K64 (precision mode KAOS_PREC_MIXED_K64) computes the heating
+// kick in FP64 from the FP64 state, with the FP64 path's formula and Philox
+// draw; the rest of the step is unchanged.
+template <bool THREE_D, int NT, int MINB, bool PERSIST, bool MASTER, bool K64>
 __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   // master-step work (field re-interpolation, binning) only in the MASTER
   // variant: the ordinary step carries none of its code or registers
@@ -937,6 +939,9 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   const float qs_ms = (float)(T.qs / T.ms);
   const float c_invOm = (float)(T.ms / (T.qs * MDIP));
   const float ylim = (float)((2.0 * PI / a.h) * (2.0 * PI / a.h));
+  // the FP64 kick's per-tube constants (K64 only)
+  const double qs_ms64 = T.qs / T.ms, c_invOm64 = T.ms / (T.qs * MDIP);
+  const double invsumds64 = 1.0 / T.sumdsICR;
   // the item's ions through per-item base pointers and a 32-bit index
   const int64_t base = T.off + beg;
   const int nk = (int)(end - beg);
@@ -1039,7 +1044,17 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       continue;
     }
     double v1n = v1, v2n = v2;  // after the wave-heating kick
-    if (a.icr && qi >= 0) {
+    if (K64 && a.icr && qi >= 0) {
+      // FP64 kick: Omega = (q/m) MDIP sqrt(ell) / r^3 and 1/Omega from the
+      // FP64 radius and 1/sqrt(ell) (yl), 1/r from the FP32 reciprocal and
+      // one FP64 Newton step (relative error ~1e-14)
+      double ir = (double)rcpa((float)r);
+      ir = ir * fma(-r, ir, 2.0);
+      const double Om = qs_ms64 * MDIP * (ell64 * yl) * (ir * ir * ir);
+      const double invOm = c_invOm64 * (r * r * r) * yl;
+      const HeatC<double> hc = heat_consts<double>(a.ct, (int64_t)T.coff + qi);
+      heat<double>(a, step, hc, pid, invsumds64, Om, invOm, fabs(vpar), v1n, v2n);
+    } else if (a.icr && qi >= 0) {
       const float rr = (float)r;
       const float sl = g1.ell * g1.isl;
       const float ir3 = g1.ir * g1.ir * g1.ir;

@@ -15,7 +15,8 @@ module kaos_gpu_iface
   integer(c_int), parameter :: KAOS_OK = 0, KAOS_ERR_PARAM = 1, &
     KAOS_ERR_CAPACITY = 2, KAOS_ERR_NAN = 3, KAOS_ERR_CUDA = 4, &
     KAOS_ERR_TIMEOUT = 5, KAOS_ERR_STATE = 6
-  integer(c_int), parameter :: KAOS_PREC_FP64 = 0, KAOS_PREC_MIXED = 1
+  integer(c_int), parameter :: KAOS_PREC_FP64 = 0, KAOS_PREC_MIXED = 1, &
+                                KAOS_PREC_MIXED_K64 = 2
   integer(c_int), parameter :: KAOS_M0 = 0, KAOS_M1PERP1 = 1, &
     KAOS_M1PERP2 = 2, KAOS_M1PAR = 3, KAOS_M2 = 4, KAOS_M2PERP1 = 5, &
     KAOS_M2PERP2 = 6, KAOS_M2PAR = 7, KAOS_M1PERP = 8, KAOS_M2PERP = 9, &

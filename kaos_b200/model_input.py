@@ -28,6 +28,7 @@ MH = 1.0 * 1.66054e-27    # H+ / H mass [kg]
 
 KAOS_PREC_FP64 = 0
 KAOS_PREC_MIXED = 1
+KAOS_PREC_MIXED_K64 = 2  # mixed push, heating kick in FP64
 
 (KAOS_M0, KAOS_M1PERP1, KAOS_M1PERP2, KAOS_M1PAR, KAOS_M2, KAOS_M2PERP1,
  KAOS_M2PERP2, KAOS_M2PAR, KAOS_M1PERP, KAOS_M2PERP, KAOS_NQ, KAOS_EAMAG,

@@ -85,14 +85,17 @@ class _DeviceCounters:
 
 def nccl_reduce_hook(group=None):
     """A Solver.set_reduce hook: in-place sum of the accumulator block over
-    the process group (NCCL on GPUs), then wait for it."""
+    the process group (NCCL on GPUs), ordered on the library's stream (the
+    hook's `stream` argument), then wait for it."""
     import torch
     import torch.distributed as dist
 
     def hook(buf: int, count: int, stream: int) -> int:
         t = torch.as_tensor(_DeviceCounters(buf, count), device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-        torch.cuda.current_stream().synchronize()
+        s = torch.cuda.ExternalStream(int(stream)) if stream else torch.cuda.current_stream()
+        with torch.cuda.stream(s):
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        s.synchronize()
         return 0
 
     return hook

@@ -61,3 +61,20 @@ def test_charge_exchange_tube_limit(lib):
     tube, vg, out = KaosTube(), KaosVGrid(), C.c_void_p()
     rc = lib.kaos_create(C.byref(p), C.byref(tube), limit + 1, C.byref(vg), C.byref(out))
     assert rc == 1 and not out.value
+
+
+def test_unknown_precision_mode_rejected(lib):
+    """A precision mode other than KAOS_PREC_FP64, KAOS_PREC_MIXED and
+    KAOS_PREC_MIXED_K64 is rejected before any device work, with a message."""
+    import ctypes as C
+    from kaos_b200.model_input import (KAOS_PREC_MIXED_K64, KaosTube, KaosVGrid,
+                                       ModelInput)
+    src = open(os.path.join(ROOT, "include", "kaos_gpu.h")).read()
+    assert int(re.search(r"#define KAOS_PREC_MIXED_K64 (\d+)", src).group(1)) == \
+        KAOS_PREC_MIXED_K64
+    p = ModelInput(precision=7).to_c()
+    tube, vg, out = KaosTube(), KaosVGrid(), C.c_void_p()
+    rc = lib.kaos_create(C.byref(p), C.byref(tube), 1, C.byref(vg), C.byref(out))
+    assert rc == 1
+    assert b"precision" in lib.kaos_last_error(out)
+    lib.kaos_destroy(out)

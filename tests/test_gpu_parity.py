@@ -154,6 +154,38 @@ def test_mixed_precision_every_moment_vs_oracle(heat):
         assert err < MIXED_MOM_TOL, (m, err)
 
 
+def test_mixed_kick64_heating_matches_fp64():
+    """KAOS_PREC_MIXED_K64 -- the mixed path with the WaveHeatingSub kick in
+    FP64 (the FP64 path's formula and Philox draw on the FP64 state) --
+    against the FP64 oracle on the precision A/B geometry, 2e4 ions, heating
+    and collisions on, three master steps: Vperp within 1e-9 (measured
+    5e-11: the kick's inputs differ from the oracle's only by the mixed
+    path's position and V|| rounding) and a thousand times closer than with
+    the FP32 kick of KAOS_PREC_MIXED (measured 2e-6), counts bit-exact,
+    every moment within 1e-6."""
+    from kaos_b200.model_input import KAOS_PREC_MIXED_K64
+    import dataclasses
+    mi, spec, tube, vg = grids.config_c2(n_particles=20000, heating=True,
+                                         collisions=True, precision=KAOS_PREC_MIXED_K64,
+                                         ndatfac=10)
+    o, s = run_pair(mi, spec, tube, vg, 31)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=3)
+    f = Solver(dataclasses.replace(mi, precision=KAOS_PREC_MIXED), [tube], vg)
+    f.load(0, q, vpar, v1, v2)
+    f.step(31)
+    assert s.count() == o.count() == f.count()
+    po, ps, pf = o.particles(), s.particles(), f.particles()
+    e64 = max(rel_norm(ps[k], po[k]) for k in ("vperp1", "vperp2"))
+    e32 = max(rel_norm(pf[k], po[k]) for k in ("vperp1", "vperp2"))
+    assert e64 < 1e-9 and e64 < 1e-3 * e32, (e64, e32)
+    assert rel_norm(ps["vpar"], po["vpar"]) < 1e-6
+    np.testing.assert_array_equal(s.counts(), o.counts())
+    for m in ALL_ION_MOMENTS:
+        err = rel_norm(s.moments(m), o.moments(m))
+        assert err < MIXED_MOM_TOL, (m, err)
+    f.close()
+
+
 ENA_MOMENTS = list(range(15, 24))  # KAOS_ENA_NQ .. KAOS_ENA_M2PHI
 
 

@@ -91,3 +91,42 @@ def test_split_tube_matches_unsplit():
         for m in (KAOS_M0, KAOS_M2, KAOS_M2PAR, KAOS_EAMAG):
             np.testing.assert_array_equal(s.moments(m), ref.moments(m), err_msg=f"{r} {m}")
         np.testing.assert_array_equal(s.counts(), ref.counts())
+
+
+def test_nccl_hook_on_a_one_rank_group(tmp_path):
+    """shard.nccl_reduce_hook as a Solver.set_reduce hook on a one-rank NCCL
+    process group: the all-reduce runs on the library's stream at every
+    statistics step (here the identity) and the run equals the unhooked one
+    bit for bit.  (The two-rank sum is checked by the host-barrier hook
+    above and, over gloo on host memory, by the CPU tests.)"""
+    import torch.distributed as dist
+    from kaos_b200.shard import nccl_reduce_hook
+    mi, spec, tube, vg = grids.config_small(n_particles=3000, three_d=True,
+                                            steps_per_master=4, heating=True)
+    q, vpar, v1, v2 = grids.initial_particles(tube, spec, mi, seed=22)
+    ref = Solver(mi, [tube], vg)
+    ref.load(0, q, vpar, v1, v2)
+    ref.step(9)
+    store = dist.FileStore(str(tmp_path / "pg"), 1)
+    dist.init_process_group("nccl", store=store, rank=0, world_size=1)
+    try:
+        inner = nccl_reduce_hook()
+        calls = []
+
+        def hook(buf, count, stream):
+            calls.append(stream)
+            return inner(buf, count, stream)
+
+        s = Solver(mi, [tube], vg)
+        s.set_rank(0, 1)
+        s.set_reduce(hook)
+        s.load(0, q, vpar, v1, v2)
+        s.step(9)
+        assert len(calls) >= 3 and all(calls)  # step 1, master steps 4 and 8
+        np.testing.assert_array_equal(s.counts(), ref.counts())
+        for m in (KAOS_M0, KAOS_M2, KAOS_M2PAR, KAOS_EAMAG):
+            np.testing.assert_array_equal(s.moments(m), ref.moments(m))
+        s.close()
+    finally:
+        dist.destroy_process_group()
+    ref.close()
