@@ -326,12 +326,16 @@ int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches);
  *   KAOS_SAMPLE_GAUSS64 2 values: the FP64 Gaussian pair of the FP64 push's
  *                       heating kick for particle id0 + i at step;
  *   KAOS_SAMPLE_POISSON 1 value: the collision-count draw with mean
- *                       `lambda` for cell id0 + i at master step `step`.
- * out holds 4, 2, 2 or 1 doubles per draw; n <= 2^26. */
+ *                       `lambda` for cell id0 + i at master step `step`;
+ *   KAOS_SAMPLE_GAUSS64T 2 values: the same pair as KAOS_SAMPLE_GAUSS64 as
+ *                       the KAOS_PREC_MIXED_K64 push evaluates it (table-
+ *                       reduced FP64 logarithm and sine/cosine).
+ * out holds 4, 2, 2, 1 or 2 doubles per draw; n <= 2^26. */
 #define KAOS_SAMPLE_PHILOX 0
 #define KAOS_SAMPLE_GAUSS32 1
 #define KAOS_SAMPLE_GAUSS64 2
 #define KAOS_SAMPLE_POISSON 3
+#define KAOS_SAMPLE_GAUSS64T 4
 int kaos_sample_rng(int32_t kind, uint64_t seed, uint64_t id0, uint32_t step,
                     uint32_t c3, double lambda, int64_t n, double *out);
 

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libkaos_gpu.so")
 SOURCES = ["kaos_api.cu"]
-DEPS = ["kaos_api.cu", "kaos_common.cuh", "kaos_push.cuh", "kaos_tube.cuh",
+DEPS = ["kaos_api.cu", "kaos_common.cuh", "kaos_push.cuh", "kaos_tube.cuh", "kaos_f64.cuh",
         "kaos_cx.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo",

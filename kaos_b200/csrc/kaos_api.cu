@@ -906,6 +906,9 @@ int sample_width(int kind) {
 }
 
 __global__ void k_sample_rng(SampleArgs a) {
+  double *kt = kf_tables();
+  if (a.kind == KAOS_SAMPLE_GAUSS64T) kf_tables_fill(kt);
+  __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t id = a.id0 + (uint64_t)i;
@@ -920,6 +923,11 @@ __global__ void k_sample_rng(SampleArgs a) {
     } else if (a.kind == KAOS_SAMPLE_GAUSS64) {
       double g1, g2;
       gauss2_64(a.seed, id, a.step, KAOS_RNG_HEAT, g1, g2);
+      a.out[2 * i] = g1;
+      a.out[2 * i + 1] = g2;
+    } else if (a.kind == KAOS_SAMPLE_GAUSS64T) {
+      double g1, g2;
+      gauss2_64t(a.rk, kt, id, a.step, g1, g2);
       a.out[2 * i] = g1;
       a.out[2 * i + 1] = g2;
     } else {
@@ -2087,7 +2095,7 @@ int kaos_get_push_timing(kaos_handle *h, double *ms, int64_t *launches) {
 
 int kaos_sample_rng(int32_t kind, uint64_t seed, uint64_t id0, uint32_t step,
                     uint32_t c3, double lambda, int64_t n, double *out) {
-  if (kind < KAOS_SAMPLE_PHILOX || kind > KAOS_SAMPLE_POISSON || n < 0 ||
+  if (kind < KAOS_SAMPLE_PHILOX || kind > KAOS_SAMPLE_GAUSS64T || n < 0 ||
       n > ((int64_t)1 << 26) || (n > 0 && !out) ||
       (kind == KAOS_SAMPLE_POISSON && !(lambda >= 0.0 && lambda <= 700.0)))
     return KAOS_ERR_PARAM;

@@ -11,6 +11,7 @@
 // WaveHeatingSub _8_1_1_0_WaveHeating.f90:32-312.
 #pragma once
 #include "kaos_common.cuh"
+#include "kaos_f64.cuh"
 
 namespace kaos {
 
@@ -536,6 +537,76 @@ __device__ __forceinline__ void heat32(const PushArgs &a, uint32_t step,
   dv2 = h0.y * e2 * G2;
 }
 
+// The tables of kaos_f64.cuh in shared memory (allocated only in the
+// kernels that call this): 2^(i/128), i = 0..128, then the (cos, sin) pairs
+// of 2 pi i/128.  Filled by kf_tables_fill before the block's first barrier.
+__device__ __forceinline__ double *kf_tables() {
+  __shared__ double t[3 * (KF_N + 1)];
+  return t;
+}
+__device__ __forceinline__ void kf_tables_fill(double *t) {
+  for (int i = threadIdx.x; i <= KF_N; i += blockDim.x) {
+    double sn, cs;
+    t[i] = exp2((double)i / KF_N);
+    sincospi((double)i / (KF_N / 2), &sn, &cs);
+    t[KF_N + 1 + 2 * i] = cs;
+    t[KF_N + 2 + 2 * i] = sn;
+  }
+}
+
+// gauss2_64's Gaussian pair (the same Philox words, 53-bit uniforms) through
+// the table-reduced logarithm and sine/cosine; kt = kf_tables().  Also
+// evaluated by the diagnostic sampler kaos_sample_rng.
+__device__ __forceinline__ void gauss2_64t(const uint32_t (&rk)[20], const double *kt,
+                                           uint64_t id, uint32_t step, double &g1,
+                                           double &g2) {
+  const kaos_u32x4 w = philox_rk(rk, (uint32_t)id, (uint32_t)(id >> 32), step,
+                                 KAOS_RNG_HEAT << 24);
+  const double R = sqrt(-2.0 * kf_ln(kt, kaos_u01(w.v[0], w.v[1])));
+  double sn, cn;
+  kf_sincos2pi(kt + KF_N + 1, kaos_u01(w.v[2], w.v[3]), sn, cn);
+  g1 = R * cn;
+  g2 = R * sn;
+}
+
+// The stochastic WaveHeatingSub kick of heat<double> (the FP64 path's kick)
+// for the mixed push in precision mode KAOS_PREC_MIXED_K64, every factor in
+// FP64 through the table-reduced functions of kaos_f64.cuh.  In log form,
+// as in heat32,
+//   kick_i = K_i G_i 2^E_i,  E_i = -c_i log2(Om/Om0) + log2(y Sig^-6)/4,
+// y = Om |V||| / sum ds = (Om s)^2, the Sig^-6 factor (Sig = 2 pi Vperp /
+// (Om lambda)) only for lambda != 0 and Sig >= 1; applied while
+// y <= (2 pi/h)^2 (h Om s <= 2 pi).  The Gaussians are gauss2_64's pair
+// from the same Philox words (53-bit uniforms); the kicks agree with
+// heat<double>'s to a few units in the last place.  A kick below 1e-75 of
+// its scale (y Sig^-6 < 1e-300) is left out: added to an FP64 velocity it
+// changes nothing.
+__device__ __forceinline__ void heat64t(const PushArgs &a, uint32_t step,
+                                        const double *kt, const CellTables &ct,
+                                        int64_t g, uint64_t id, double invsumds,
+                                        double ylim, double Om, double invOm,
+                                        double vabs, double &v1, double &v2) {
+  double arg = Om * vabs * invsumds;  // y
+  if (!(arg <= ylim)) return;         // beyond the stochastic regime
+  const double lam = ct.lambdaPerp[g];
+  if (lam != 0.0) {
+    const double sk = (2.0 * PI) * invOm / lam;
+    const double S2 = sk * sk * fma(v1, v1, v2 * v2);  // Sig^2
+    if (S2 >= 1.0) arg = arg / (S2 * S2 * S2);
+  }
+  if (!(arg > 1e-300)) return;
+  double G1, G2;
+  gauss2_64t(a.rk, kt, id, step, G1, G2);
+  const double *p2 = kt;
+  const double c1 = ct.hc1[g], c2 = ct.hc2[g];
+  const double lx = kf_log2(p2, Om * ct.hiom0[g]);
+  const double b = 0.25 * kf_log2(p2, arg);
+  const double e1 = kf_exp2(p2, fma(-c1, lx, b));
+  const double e2 = (c2 == c1) ? e1 : kf_exp2(p2, fma(-c2, lx, b));
+  v1 = fma(ct.hK1[g] * e1, G1, v1);
+  v2 = fma(ct.hK2[g] * e2, G2, v2);
+}
+
 // Positive root u = r/RE of q^2 u^4 + u/p - 1 = 0 by Newton from u0 (the
 // function is increasing and convex for u > 0: the root is unique).  The
 // derivative is inverted in FP32 (correctly rounded); each step still
@@ -884,6 +955,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   double *VE2 = VE1 + (MAXV + 1), *VEP = VE2 + (MAXV + 1);
   VBinTab *VTS = (VBinTab *)(VEP + (MAXV + 1));
   VBinTab &VT1 = VTS[0], &VT2 = VTS[1], &VTP = VTS[2];
+  if (K64) kf_tables_fill(kf_tables());  // ordered by the item loop's barrier
   if (bin || !THREE_D) {
     load_vgrid_smem(c_vg.e1, c_vg.e2, c_vg.epar, VE1, VE2, VEP);
     build_vbin_tab(VTP, c_vg.epar, c_vg.npar);
@@ -942,6 +1014,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
   // the FP64 kick's per-tube constants (K64 only)
   const double qs_ms64 = T.qs / T.ms, c_invOm64 = T.ms / (T.qs * MDIP);
   const double invsumds64 = 1.0 / T.sumdsICR;
+  const double ylim64 = (2.0 * PI / a.h) * (2.0 * PI / a.h);
   // the item's ions through per-item base pointers and a 32-bit index
   const int64_t base = T.off + beg;
   const int nk = (int)(end - beg);
@@ -1052,8 +1125,13 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       ir = ir * fma(-r, ir, 2.0);
       const double Om = qs_ms64 * MDIP * (ell64 * yl) * (ir * ir * ir);
       const double invOm = c_invOm64 * (r * r * r) * yl;
-      const HeatC<double> hc = heat_consts<double>(a.ct, (int64_t)T.coff + qi);
-      heat<double>(a, step, hc, pid, invsumds64, Om, invOm, fabs(vpar), v1n, v2n);
+      if (!a.icrcoh) {
+        heat64t(a, step, kf_tables(), a.ct, (int64_t)T.coff + qi, pid, invsumds64,
+                ylim64, Om, invOm, fabs(vpar), v1n, v2n);
+      } else {  // coherent branch: the FP64 path's own code
+        const HeatC<double> hc = heat_consts<double>(a.ct, (int64_t)T.coff + qi);
+        heat<double>(a, step, hc, pid, invsumds64, Om, invOm, fabs(vpar), v1n, v2n);
+      }
     } else if (a.icr && qi >= 0) {
       const float rr = (float)r;
       const float sl = g1.ell * g1.isl;

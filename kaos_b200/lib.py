@@ -34,8 +34,8 @@ EXPORTS = [
 ]
 
 # kaos_sample_rng kinds and values per draw
-SAMPLE_PHILOX, SAMPLE_GAUSS32, SAMPLE_GAUSS64, SAMPLE_POISSON = 0, 1, 2, 3
-_SAMPLE_WIDTH = {0: 4, 1: 2, 2: 2, 3: 1}
+SAMPLE_PHILOX, SAMPLE_GAUSS32, SAMPLE_GAUSS64, SAMPLE_POISSON, SAMPLE_GAUSS64T = 0, 1, 2, 3, 4
+_SAMPLE_WIDTH = {0: 4, 1: 2, 2: 2, 3: 1, 4: 2}
 
 # int fn(void *ctx, uint32_t *buf, int64_t count, void *stream)
 REDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)

@@ -9,11 +9,15 @@ defaults, each against the oracle on the same seeded ions:
   redrawn;
 * the unsigned ambipolar field (EAMBSIGNflag = 0,
   _8_1_1_KineticUpdateA.f90:656-658): the field magnitude pointed away from
-  the Earth in both hemispheres.
+  the Earth in both hemispheres;
+* a finite perpendicular wavelength lambdaPerp (_8_1_1_0_WaveHeating.f90:
+  91-97): the diffusion coefficient divided by Sig^3 where Sig = 2 pi
+  |Vperp| / (lambdaPerp Omega) >= 1 (lambdaPerp = 5 m: most ions, not all).
 
 FP64 path: states within 1e-12, counts bit-exact, moments within 1e-10;
-mixed path: every moment within 1e-6.  Each case also checks that the
-branch changes the run (against the default flag).
+mixed path (FP32 kick) and KAOS_PREC_MIXED_K64 (FP64 kick): every moment
+within 1e-6, and for K64 with heating on Vperp within 1e-9.  Each case also
+checks that the branch changes the run (against the default flag).
 """
 import dataclasses
 
@@ -25,7 +29,8 @@ from kaos_b200 import grids
 from kaos_b200.lib import Solver
 from kaos_b200.model_input import (KAOS_EAMAG, KAOS_M0, KAOS_M1PAR, KAOS_M1PERP1,
                                    KAOS_M1PERP2, KAOS_M2, KAOS_M2PAR, KAOS_M2PERP1,
-                                   KAOS_M2PERP2, KAOS_NQ, KAOS_PREC_MIXED)
+                                   KAOS_M2PERP2, KAOS_NQ, KAOS_PREC_MIXED,
+                                   KAOS_PREC_MIXED_K64)
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -45,9 +50,11 @@ def rel_norm(a, b):
 
 def case(name):
     """ModelInput changes of a branch, and the run length."""
-    heating = name == "coherent"
+    heating = name in ("coherent", "lambda")
     mi, spec, tube, vg = grids.config_small(n_particles=4000, three_d=True,
                                             steps_per_master=5, heating=heating)
+    if name == "lambda":
+        tube.lambdaPerp = np.full(tube.nq, 5.0)
     if name == "te_ramp":
         mi.dNTe, mi.dNTeEND = 400.0, 5000.0   # K per master step, cap
     elif name == "coherent":
@@ -67,21 +74,25 @@ def run(mi, tube, vg, init, steps, gpu):
     return r
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-@pytest.mark.parametrize("name", ["te_ramp", "coherent", "eamb_unsigned"])
-def test_branch_matches_oracle(name, mixed):
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "k64"])
+@pytest.mark.parametrize("name", ["te_ramp", "coherent", "eamb_unsigned", "lambda"])
+def test_branch_matches_oracle(name, prec):
     mi, spec, tube, vg = case(name)
     init = grids.initial_particles(tube, spec, mi, seed=31)
     steps = 23  # master steps at 5, 10, 15, 20
     o = run(mi, tube, vg, init, steps, gpu=False)
-    mg = dataclasses.replace(mi, precision=KAOS_PREC_MIXED) if mixed else mi
+    mg = mi if prec == "fp64" else dataclasses.replace(
+        mi, precision=KAOS_PREC_MIXED if prec == "mixed" else KAOS_PREC_MIXED_K64)
     s = run(mg, tube, vg, init, steps, gpu=True)
     assert s.count() == o.count()
     po, ps = o.particles(), s.particles()
-    if mixed:
+    if prec != "fp64":
         for m in MOMENTS:
             err = rel_norm(s.moments(m), o.moments(m))
             assert err < MIXED_MOM_TOL, (name, m, err)
+        if prec == "k64" and mi.ICRflag:
+            for k in ("vperp1", "vperp2"):
+                assert rel_norm(ps[k], po[k]) < 1e-9, (name, k, rel_norm(ps[k], po[k]))
         return
     for k in ("rho", "z", "vpar", "vperp1", "vperp2"):
         assert rel_norm(ps[k], po[k]) < TRAJ_TOL, (name, k)
@@ -90,7 +101,8 @@ def test_branch_matches_oracle(name, mixed):
         assert rel_norm(s.moments(m), o.moments(m)) < MOM_TOL, (name, m)
     # the branch is live: the default flag gives a different run
     base = dataclasses.replace(mi, dNTe=0.0, ICRCOHERENCEflag=0, EAMBSIGNflag=1)
-    b = run(base, tube, vg, init, steps, gpu=True)
+    tb = dataclasses.replace(tube, lambdaPerp=np.zeros(tube.nq))
+    b = run(base, tb, vg, init, steps, gpu=True)
     pb = b.particles()
-    key = "vperp1" if name == "coherent" else "vpar"
+    key = "vperp1" if name in ("coherent", "lambda") else "vpar"
     assert rel_norm(pb[key], ps[key]) > 1e-9, name

@@ -79,6 +79,15 @@ def gauss():
     return g32, g64
 
 
+def test_table_reduced_gaussian_pair_equals_fp64_pair(gauss):
+    """The Gaussian pair of the KAOS_PREC_MIXED_K64 kick (table-reduced FP64
+    logarithm and sine/cosine, kaos_f64.cuh) against the FP64 push's pair
+    from the same Philox words: equal to a few units of 2^-52."""
+    n = len(gauss[1])
+    g64t = klib.sample_rng(klib.SAMPLE_GAUSS64T, n, seed=20261203, id0=1 << 20, step=77)
+    assert np.max(np.abs(g64t - gauss[1])) < 1e-14
+
+
 @pytest.mark.parametrize("which", [0, 1])
 def test_gaussian_moments_tails_ks(gauss, which):
     g = gauss[which]
