@@ -1117,22 +1117,9 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       continue;
     }
     double v1n = v1, v2n = v2;  // after the wave-heating kick
-    if (K64 && a.icr && qi >= 0) {
-      // FP64 kick: Omega = (q/m) MDIP sqrt(ell) / r^3 and 1/Omega from the
-      // FP64 radius and 1/sqrt(ell) (yl), 1/r from the FP32 reciprocal and
-      // one FP64 Newton step (relative error ~1e-14)
-      double ir = (double)rcpa((float)r);
-      ir = ir * fma(-r, ir, 2.0);
-      const double Om = qs_ms64 * MDIP * (ell64 * yl) * (ir * ir * ir);
-      const double invOm = c_invOm64 * (r * r * r) * yl;
-      if (!a.icrcoh) {
-        heat64t(a, step, kf_tables(), a.ct, (int64_t)T.coff + qi, pid, invsumds64,
-                ylim64, Om, invOm, fabs(vpar), v1n, v2n);
-      } else {  // coherent branch: the FP64 path's own code
-        const HeatC<double> hc = heat_consts<double>(a.ct, (int64_t)T.coff + qi);
-        heat<double>(a, step, hc, pid, invsumds64, Om, invOm, fabs(vpar), v1n, v2n);
-      }
-    } else if (a.icr && qi >= 0) {
+    // (the FP64 kick of K64 runs after the position and V|| stores below:
+    // nothing before them reads the kicked pair)
+    if (!K64 && a.icr && qi >= 0) {
       const float rr = (float)r;
       const float sl = g1.ell * g1.isl;
       const float ir3 = g1.ir * g1.ir * g1.ir;
@@ -1153,7 +1140,7 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
       }
     }
     // stored at once: the kicked pair holds no registers through the RK
-    if (a.icr) V12[k] = make_double2(v1n, v2n);
+    if (!K64 && a.icr) V12[k] = make_double2(v1n, v2n);
     // ---- the stage accelerations ----------------------------------------
     // a|| = M + s C0 + ce1 AEA with the signed mirror term M (cos(theta) in
     // place of s |cos|: smooth through the equator), the hemisphere sign s
@@ -1222,6 +1209,26 @@ __global__ void __launch_bounds__(NT, MINB) k_push32(PushArgs a) {
     if (prologue) FF[k] = make_float2(aea, ag);
     if (a.write_qind) QI[k] = qi;
     if (a.cxc && qi >= 0) atomicAdd(&HC[qi], 1u);
+    if (K64 && a.icr) {
+      if (qi >= 0) {
+        // FP64 kick at the start-of-step point: Omega = (q/m) MDIP sqrt(ell)
+        // / r^3 and 1/Omega from the FP64 radius and 1/sqrt(ell) (yl), 1/r
+        // from the FP32 reciprocal and one FP64 Newton step (relative error
+        // ~1e-14); the RK above used the pre-kick Vperp, as heat() does
+        double ir = (double)rcpa((float)r);
+        ir = ir * fma(-r, ir, 2.0);
+        const double Om = qs_ms64 * MDIP * (ell64 * yl) * (ir * ir * ir);
+        const double invOm = c_invOm64 * (r * r * r) * yl;
+        if (!a.icrcoh) {
+          heat64t(a, step, kf_tables(), a.ct, (int64_t)T.coff + qi, pid, invsumds64,
+                  ylim64, Om, invOm, fabs(vpar), v1n, v2n);
+        } else {  // coherent branch: the FP64 path's own code
+          const HeatC<double> hc = heat_consts<double>(a.ct, (int64_t)T.coff + qi);
+          heat<double>(a, step, hc, pid, invsumds64, Om, invOm, fabs(vpar), v1n, v2n);
+        }
+      }
+      V12[k] = make_double2(v1n, v2n);
+    }
   }
   if (bin) bin_win_flush(a.acc, T, W);
   if (a.cxc) flush_cx_counts(a, t, beg, T.nq, HC);
