@@ -1,5 +1,5 @@
 """Parity of the CUDA path against the CPU oracle on identical seeded
-initial particles.  Tolerances (BASELINE north star): FP64 trajectories
+initial particles.  Tolerances: FP64 trajectories
 1e-12 relative (norm-wise over the particle set), per-cell integer counts
 bit-exact, moments 1e-10 relative; mixed precision: moments 1e-6 relative
 to the FP64 oracle's scale (stated per moment)."""
@@ -130,7 +130,7 @@ def test_fp64_escape_and_injection_order(tight):
 ALL_ION_MOMENTS = [KAOS_M0, KAOS_M1PERP1, KAOS_M1PERP2, KAOS_M1PAR, KAOS_M2,
                    KAOS_M2PERP1, KAOS_M2PERP2, KAOS_M2PAR, KAOS_NQ, KAOS_EAMAG,
                    KAOS_M0FILT]
-MIXED_MOM_TOL = 1e-6  # north star: every moment within 1e-6 of the FP64 oracle
+MIXED_MOM_TOL = 1e-6  # every moment within 1e-6 of the FP64 oracle's scale
 
 
 @pytest.mark.parametrize("heat", [False, True])

@@ -5,7 +5,7 @@ The reference draws from gfortran's unseeded random_number
 _3_2_PoissonRNG.f90:27-42, used by WaveHeatingSub
 _8_1_1_0_WaveHeating.f90:141-150 and IonNeutralCollisionFrequencyASub
 _8_6_6_1_...:275-301), which cannot be reproduced, so the stochastic terms
-are judged by their distributions:
+are checked by their distributions:
 
 * the device Philox4x32-10 against the published known-answer vectors;
 * the FP32 Gaussian pair of the mixed push's heating kick and the FP64 pair
