@@ -8,7 +8,10 @@ import pytest
 from kaos_b200 import build as kbuild
 from kaos_b200 import grids
 from kaos_b200.lib import Solver
-from kaos_b200.model_input import KAOS_M0, KAOS_M2PAR, KAOS_NUPOI, KAOS_PREC_MIXED
+from kaos_b200.model_input import (KAOS_M0, KAOS_M2PAR, KAOS_NUPOI, KAOS_PREC_FP64,
+                                   KAOS_PREC_MIXED, KAOS_PREC_MIXED_K64)
+
+PRECISIONS = [KAOS_PREC_FP64, KAOS_PREC_MIXED, KAOS_PREC_MIXED_K64]
 
 pytestmark = pytest.mark.gpu
 
@@ -18,12 +21,11 @@ def _build():
     kbuild.build()
 
 
-def _run(mixed, graph, export, chunks):
+def _run(prec, graph, export, chunks):
     mi, spec, tube, vg = grids.config_small(n_particles=6000, three_d=True,
                                             steps_per_master=4, heating=True,
                                             collisions=True)
-    if mixed:
-        mi.precision = KAOS_PREC_MIXED
+    mi.precision = prec
     tube.nsnormCLB = 30.0
     init = grids.initial_particles(tube, spec, mi, seed=11)
     s = Solver(mi, [tube], vg)
@@ -42,11 +44,11 @@ def _run(mixed, graph, export, chunks):
     return out
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-def test_graph_replay_bit_identical(mixed):
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_graph_replay_bit_identical(prec):
     chunks = (1, 6, 19, 3, 12)  # 41 steps: ten master steps, uneven calls
-    a = _run(mixed, False, False, chunks)
-    b = _run(mixed, True, False, chunks)
+    a = _run(prec, False, False, chunks)
+    b = _run(prec, True, False, chunks)
     assert a["n"] == b["n"]
     assert a["n"][1] > 0  # charge exchange produced ENAs
     for k in a["p"]:
@@ -61,19 +63,18 @@ def test_graph_replay_bit_identical(mixed):
 
 def test_graph_replay_with_export():
     chunks = (9, 8)
-    a = _run(False, False, True, chunks)
-    b = _run(False, True, True, chunks)
+    a = _run(KAOS_PREC_FP64, False, True, chunks)
+    b = _run(KAOS_PREC_FP64, True, True, chunks)
     np.testing.assert_array_equal(a["h"], b["h"])
     for k in a["p"]:
         np.testing.assert_array_equal(a["p"][k], b["p"][k], err_msg=k)
 
 
-def _run_shape(mixed, shape):
+def _run_shape(prec, shape):
     mi, spec, tube, vg = grids.config_small(n_particles=9000, three_d=True,
                                             steps_per_master=4, heating=True,
                                             collisions=True)
-    if mixed:
-        mi.precision = KAOS_PREC_MIXED
+    mi.precision = prec
     tube.nsnormCLB = 30.0
     init = grids.initial_particles(tube, spec, mi, seed=5)
     s = Solver(mi, [tube], vg)
@@ -87,18 +88,19 @@ def _run_shape(mixed, shape):
     return out
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-def test_launch_shapes_bit_identical(mixed):
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_launch_shapes_bit_identical(prec):
     """Every push launch shape (ions per work item, one block per item or a
     persistent grid, register budget and block size) and the autotuner's
-    choice give the same particles, ENAs and counts."""
-    ref = _run_shape(mixed, (2048, 0))
+    choice give the same particles, ENAs and counts, in every precision
+    mode."""
+    ref = _run_shape(prec, (2048, 0))
     shapes = [(1024, 1), (4096, 0), None]
-    if mixed:
+    if prec != KAOS_PREC_FP64:
         # bits 3-4: the master-step variant's budget + 1 (64 with 80, 72 with 64)
         shapes += [(1024, 2), (4096, 3), (2048, 4), (1024, 5), (2048, 2 | 8), (4096, 24)]
     for sh in shapes:
-        o = _run_shape(mixed, sh)
+        o = _run_shape(prec, sh)
         if sh is not None:
             assert o["launch"] == sh
         else:

@@ -186,6 +186,37 @@ def test_mixed_kick64_heating_matches_fp64():
     f.close()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "k64"])
+def test_heated_2d_grid_every_precision(prec):
+    """Wave heating on a 2D (V||, |Vperp|) velocity grid, where an ion whose
+    speed leaves the grid keeps its previous bins, in every precision mode
+    against the oracle (23 steps, four master steps, charge exchange on):
+    FP64 states 1e-12, counts and escapes exact, moments 1e-10;
+    KAOS_PREC_MIXED_K64 Vperp 1e-9, counts exact, moments 1e-6; the FP32
+    kick of KAOS_PREC_MIXED moments 1e-6."""
+    from kaos_b200.model_input import KAOS_PREC_MIXED_K64
+    mi, spec, tube, vg = grids.config_small(n_particles=4000, three_d=False,
+                                            steps_per_master=5, heating=True,
+                                            collisions=True)
+    if prec != "fp64":
+        mi.precision = KAOS_PREC_MIXED if prec == "mixed" else KAOS_PREC_MIXED_K64
+    o, s = run_pair(mi, spec, tube, vg, 23, seed=13)
+    assert s.count() == o.count()
+    po, ps = o.particles(), s.particles()
+    if prec == "fp64":
+        for k in ("z", "rho", "vpar", "vperp1", "vperp2"):
+            assert rel_norm(ps[k], po[k]) < TRAJ_TOL, k
+    elif prec == "k64":
+        for k in ("vperp1", "vperp2"):
+            assert rel_norm(ps[k], po[k]) < 1e-9, (k, rel_norm(ps[k], po[k]))
+    if prec != "mixed":
+        np.testing.assert_array_equal(s.counts(), o.counts())
+    tol = MOM_TOL if prec == "fp64" else MIXED_MOM_TOL
+    for m in moment_list(False):
+        err = rel_norm(s.moments(m), o.moments(m))
+        assert err < tol, (m, err)
+
+
 ENA_MOMENTS = list(range(15, 24))  # KAOS_ENA_NQ .. KAOS_ENA_M2PHI
 
 
