@@ -78,3 +78,14 @@ def test_unknown_precision_mode_rejected(lib):
     assert rc == 1
     assert b"precision" in lib.kaos_last_error(out)
     lib.kaos_destroy(out)
+
+
+def test_sample_kinds_match_header():
+    """The sampler kinds of kaos_b200.lib equal the header's KAOS_SAMPLE_*."""
+    from kaos_b200 import lib as klib
+    src = open(os.path.join(ROOT, "include", "kaos_gpu.h")).read()
+    kinds = {m.group(1): int(m.group(2))
+             for m in re.finditer(r"#define KAOS_SAMPLE_([A-Z0-9]+) (\d+)", src)}
+    assert kinds == {"PHILOX": klib.SAMPLE_PHILOX, "GAUSS32": klib.SAMPLE_GAUSS32,
+                     "GAUSS64": klib.SAMPLE_GAUSS64, "POISSON": klib.SAMPLE_POISSON,
+                     "GAUSS64T": klib.SAMPLE_GAUSS64T}
