@@ -474,7 +474,7 @@ def cpu_baseline(args, sample_particles=20000, sample_steps=NDATFAC):
     binning) on a bounded sample of the same workload, one host thread, over
     one whole master interval; beside it the literal reference algorithm
     (O(Nq Nv Np) counting, IonParticleCountsSub _8_3_1_...:311-357) on the
-    plain FP64 configuration, all host cores."""
+    plain FP64 configuration, on all host cores and on one."""
     from oracle.oracle import Oracle
     from kaos_b200 import grids
     from kaos_b200.model_input import KAOS_PREC_FP64
@@ -495,6 +495,7 @@ def cpu_baseline(args, sample_particles=20000, sample_steps=NDATFAC):
                sample=f"{n} O+ of the same tube x {sample_steps} steps holding one "
                       "master step (oracle, direct binning, 1 thread)")
     out["literal_c1"] = literal_baseline()
+    out["literal_c1_1core"] = literal_baseline(cores=1)
     return out
 
 
@@ -538,8 +539,9 @@ def parallel_oracle(worker, jobs):
     return work / span, span
 
 
-def literal_baseline(npart=10000, steps=20):
-    cores = len(os.sched_getaffinity(0))
+def literal_baseline(npart=10000, steps=20, cores=None):
+    """The literal reference algorithm on `cores` host cores (default all)."""
+    cores = len(os.sched_getaffinity(0)) if cores is None else cores
     jobs = [(20261203 + k, npart, steps) for k in range(cores)]
     v, span = parallel_oracle(_literal_worker, jobs)
     return {"value": v, "unit": "particle-steps/s", "cores": cores,
