@@ -102,3 +102,32 @@ def test_table_reduced_functions_accuracy(tmp_path):
     assert e_log2 < 2 * eps, e_log2    # log2 (absolute below 1)
     assert e_exp2 < 2 * eps, e_exp2    # exp2, relative
     assert e_sc < 2 * eps, e_sc        # sin, cos of 2 pi u, absolute
+
+
+def test_log_form_kick_equals_the_reference_form():
+    """The log form of the FP64 kick (heat64t: K G 2^E, E = -c log2(Om/Om0) +
+    log2(y Sig^-6)/4, y = Om |V||| / sum ds, applied while y <= (2 pi/h)^2)
+    equals heat()'s form K x^-c sqrt(Om s) Sig^-3/2 G, x = Om/Om0,
+    s = sqrt(|V||| / (Om sum ds)), applied while h Om s <= 2 pi (the
+    reference's (h/tau) sqrt(2 D tau) G, _8_1_1_0_WaveHeating.f90:141-150,
+    with D's Sig^-3 factor), over random arguments of the kick's ranges."""
+    import numpy as np
+    rng = np.random.default_rng(3)
+    n = 20000
+    Om = 10.0 ** rng.uniform(0.5, 3.0, n)
+    Om0 = 10.0 ** rng.uniform(1.5, 2.5, n)
+    vabs = 10.0 ** rng.uniform(-2.0, 4.5, n)
+    sumds = 10.0 ** rng.uniform(5.0, 7.5, n)
+    c = rng.uniform(0.2, 1.2, n)
+    sig = np.where(rng.uniform(size=n) < 0.5, 1.0, 10.0 ** rng.uniform(0.0, 2.0, n))
+    h = 0.005
+    s = np.sqrt(vabs / (Om * sumds))
+    ref = (Om / Om0) ** (-c) * np.sqrt(Om * s) * sig ** -1.5
+    on_ref = h * Om * s <= 2.0 * np.pi
+    y = Om * vabs / sumds
+    E = -c * np.log2(Om / Om0) + 0.25 * np.log2(y * sig ** -6.0)
+    on_log = y <= (2.0 * np.pi / h) ** 2
+    # the branch agrees except within rounding of its threshold
+    edge = np.abs(h * Om * s / (2.0 * np.pi) - 1.0) < 1e-12
+    assert np.array_equal(on_ref[~edge], on_log[~edge])
+    np.testing.assert_allclose(2.0 ** E, ref, rtol=1e-12)
