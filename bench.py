@@ -830,8 +830,10 @@ def main():
             "graph": None if not full else {
                 "value": rg["value"] * world, "ms_per_step": rg["ms"] / args.steps,
                 "push_launch": rg["launch"],
-                "note": "mixed path, steps replayed from CUDA graphs (warm-up of two "
-                        "master intervals captures every step graph before timing)"},
+                "warmup_steps": graph_warmup(args, NDATFAC),
+                "note": "mixed path, steps replayed from CUDA graphs (a warm-up through "
+                        "two compactions and three more master intervals captures every "
+                        "step graph before timing)"},
             "cadence1": None if not full else {
                 "value": rc1["value"] * world,
                 "ms_per_step": rc1["ms"] / min(args.steps, 50),
